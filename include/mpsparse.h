@@ -1,0 +1,210 @@
+/*
+ * mpsparse.h -- C ABI of the B200 (sm_100a) sparse iterative-solver library.
+ *
+ * Drop-in boundary for SparseForge/mpsparse's PyTorch extension modules
+ * `spmv` (class csr_tensor), `bcsr` (class bcsr_tensor) and `coo_csr`.  Each
+ * entry point names the reference interface it replaces (path:line in the
+ * reference project).
+ *
+ * Conventions
+ *  - Every pointer argument named d_* is device memory on the current device;
+ *    h_* is host memory.  Sizes are element counts.
+ *  - Calls are stream-ordered on the given stream (0 = legacy default stream).
+ *    Solvers synchronise that stream once, at the end, to fill *info.
+ *  - A handle owns its device memory and is released by its destroy call.  A
+ *    handle may not be used from two host threads at once.
+ *  - Errors are returned as mps_status; nothing calls exit().  The message of
+ *    the last error on the calling thread is mps_last_error_string().
+ */
+#ifndef MPSPARSE_H
+#define MPSPARSE_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MPS_OK = 0,
+    MPS_ERR_ARG = 1,        /* bad argument: null pointer, size, block size */
+    MPS_ERR_CUDA = 2,       /* a CUDA runtime call failed */
+    MPS_ERR_OOM = 3,        /* device allocation failed */
+    MPS_ERR_TIMEOUT = 4,    /* a bounded device-side wait gave up */
+    MPS_ERR_BREAKDOWN = 5,  /* solver breakdown (see mps_solve_info) */
+    MPS_ERR_RANGE = 6,      /* a COO key lies outside [0,n_rows) x [0,n_cols) */
+    MPS_ERR_NOT_FINITE = 7  /* right-hand side holds NaN or Inf */
+} mps_status;
+
+typedef struct mps_csr mps_csr;
+typedef struct mps_bcsr mps_bcsr;
+
+/* Preconditioners for mps_csr_cg. */
+enum { MPS_PRECOND_NONE = 0, MPS_PRECOND_JACOBI = 1, MPS_PRECOND_FSAI = 2 };
+
+typedef struct {
+    int32_t reference_compat; /* 1: reproduce the reference's stop rules and
+                                 guards (iteration caps min(1000,n) / min(5000,n),
+                                 absolute ||r||^2 < 1e-5 every 50 iterations,
+                                 BiCGSTAB rho0 = 1 + b.b, Richardson w=0.01 x1000) */
+    int32_t max_iter;         /* iteration cap (0: 2000) */
+    double tol;               /* relative residual ||r||/||b|| target (0: 1e-6) */
+    double omega;             /* Richardson weight (0: 0.01) */
+    int32_t precond;          /* MPS_PRECOND_* (CG only) */
+    int32_t stall_window;     /* FSAI: fall back to Jacobi when ||r|| has not
+                                 dropped by 2x over this many iterations (0: 200) */
+    int32_t host_loop;        /* 0: the whole iteration loop is one CUDA-graph
+                                 launch with a device-side WHILE condition;
+                                 1: the host launches the same kernels and polls
+                                 the device-side stop flag */
+    int32_t reserved;
+} mps_solve_opts;
+
+typedef struct {
+    int32_t iters;
+    int32_t converged;
+    int32_t breakdown;
+    int32_t stalled;          /* FSAI-PCG switched to Jacobi */
+    int32_t compat_snapshot;  /* reference_compat BiCGSTAB returned its last checkpoint */
+    int32_t reserved;
+    double rel_resid;         /* recurrence residual ||r||/||b|| at exit */
+} mps_solve_info;
+
+/* Fill opts with the defaults (tol 1e-6, max_iter 2000, graphs on). */
+void mps_solve_opts_default(mps_solve_opts* opts);
+const char* mps_last_error_string(void);
+const char* mps_status_string(mps_status s);
+int32_t mps_abi_version(void);
+
+/* ---- COO -> CSR ------------------------------------------------------- */
+
+/* GPU LSD radix sort of packed (row<<32|col) keys with their values, then the
+ * row_ptr count-and-scan.  Bit-exact against a stable sort by key.
+ * Replaces csr_tensor::csr_tensor + coo_to_csr_internal
+ * (iterative/BiCGSTAB/spmv.cpp:230-268, 62-228). */
+mps_status mps_csr_create_from_keys(const uint64_t* d_keys, const float* d_vals, uint64_t nnz,
+                                    uint32_t n_rows, uint32_t n_cols, mps_csr** out,
+                                    cudaStream_t stream);
+
+/* Wrap an existing CSR (copied into the handle). */
+mps_status mps_csr_create_from_csr(const int32_t* d_row_ptr, const int32_t* d_col_ind,
+                                   const float* d_vals, uint32_t n_rows, uint32_t n_cols,
+                                   uint64_t nnz, mps_csr** out, cudaStream_t stream);
+
+/* Release a handle (csr_tensor::~csr_tensor, iterative/BiCGSTAB/spmv.cpp:354-366). */
+mps_status mps_csr_destroy(mps_csr* A);
+
+mps_status mps_csr_shape(const mps_csr* A, uint32_t* n_rows, uint32_t* n_cols, uint64_t* nnz);
+
+/* Copy the CSR arrays out (the standalone converter's output tensors,
+ * spmv_kernel/coo_csr/coo_csr/coo_csr/coo_to_csr.cpp:225-236). */
+mps_status mps_csr_export(const mps_csr* A, int32_t* d_row_ptr, int32_t* d_col_ind,
+                          float* d_vals, cudaStream_t stream);
+
+/* Standalone converter: sort and write row_ptr/col_ind/out_vals
+ * (coo_csr.coo_csr, spmv_kernel/coo_csr/coo_csr/coo_csr/coo_to_csr.cpp:259-288). */
+mps_status mps_coo_to_csr(const uint64_t* d_keys, const float* d_vals, uint64_t nnz,
+                          uint32_t n_rows, uint32_t n_cols, int32_t* d_row_ptr,
+                          int32_t* d_col_ind, float* d_out_vals, cudaStream_t stream);
+
+/* ---- SpMV ------------------------------------------------------------- */
+
+/* y = A x (csr_tensor::mv / mv_internal, iterative/BiCGSTAB/spmv.cpp:421-501;
+ * kernel spmv_op, spmv.metal:11-49). */
+mps_status mps_csr_spmv(const mps_csr* A, const float* d_x, float* d_y, cudaStream_t stream);
+
+/* y = A x and *d_dot = w . y in FP64 (fused_spvmv, spmv.metal:70-132;
+ * deterministic). */
+mps_status mps_csr_spmv_dot(const mps_csr* A, const float* d_x, const float* d_w, float* d_y,
+                            double* d_dot, cudaStream_t stream);
+
+/* ---- Solvers on CSR --------------------------------------------------- */
+
+/* CG / Jacobi-PCG / learned-FSAI-PCG, x written in place
+ * (csr_tensor::cgd / cgd_op, iterative/BiCGSTAB/spmv.cpp:515-659;
+ *  iter_solve, iterative/cgd/spmv.cpp:607-747). */
+mps_status mps_csr_cg(mps_csr* A, const float* d_b, float* d_x, const mps_solve_opts* opts,
+                      mps_solve_info* info, cudaStream_t stream);
+
+/* BiCGSTAB (csr_tensor::bicgstab / bicgstab_op, iterative/BiCGSTAB/spmv.cpp:661-888). */
+mps_status mps_csr_bicgstab(mps_csr* A, const float* d_b, float* d_x, const mps_solve_opts* opts,
+                            mps_solve_info* info, cudaStream_t stream);
+
+/* Richardson x += w (b - A x) for max_iter iterations
+ * (iter_solve / iterative_op, iterative/richardson/spmv.cpp:376-438). */
+mps_status mps_csr_richardson(mps_csr* A, const float* d_b, float* d_x,
+                              const mps_solve_opts* opts, mps_solve_info* info,
+                              cudaStream_t stream);
+
+/* Mixed-precision CG: FP64 outer iterative refinement (residual b - A x and
+ * solution in FP64 on the GPU) around FP32 inner CG sweeps whose matrix values
+ * are FP32 (value_bits = 32) or BF16 (value_bits = 16).  No reference
+ * counterpart (the reference solves in FP32 only). */
+typedef struct {
+    double tol;               /* outer relative residual target (0: 1e-10) */
+    double inner_tol;         /* inner relative reduction per sweep (0: 1e-3) */
+    int32_t max_outer;        /* 0: 50 */
+    int32_t max_inner;        /* 0: 2000 */
+    int32_t value_bits;       /* 32 or 16 */
+    int32_t precond;          /* MPS_PRECOND_NONE / JACOBI / FSAI for the inner CG */
+} mps_ir_opts;
+
+typedef struct {
+    int32_t outer_iters;
+    int32_t inner_iters;      /* total inner CG iterations */
+    int32_t converged;
+    int32_t reserved;
+    double rel_resid;         /* FP64 true residual at exit */
+} mps_ir_info;
+
+mps_status mps_csr_cg_mixed(mps_csr* A, const double* d_b, double* d_x, const mps_ir_opts* opts,
+                            mps_ir_info* info, cudaStream_t stream);
+
+/* ---- Learned FSAI preconditioner ------------------------------------- */
+
+/* Attach a lower-triangular factor G (CSR on tril(A)) so that PCG applies
+ * z = G^T (G r).  G's values are copied; its transpose is built on the GPU.
+ * No reference counterpart. */
+mps_status mps_csr_set_fsai(mps_csr* A, const int32_t* d_g_row_ptr, const int32_t* d_g_col_ind,
+                            const float* d_g_vals, uint64_t g_nnz, cudaStream_t stream);
+
+/* ---- BCSR --------------------------------------------------------------- */
+
+/* BCSR from pre-built block arrays: row-major B x B blocks (B = 4 or 8),
+ * block row_ptr/col_ind; n_rows/n_cols are the logical sizes, padded up to a
+ * multiple of B (bcsr_tensor::bcsr_tensor, iterative/BiCGSTAB/bcsr.cpp:357-422). */
+mps_status mps_bcsr_create(const float* d_vals, const int32_t* d_row_ptr,
+                           const int32_t* d_col_ind, uint64_t n_blocks, uint32_t n_rows,
+                           uint32_t n_cols, uint32_t block, mps_bcsr** out,
+                           cudaStream_t stream);
+
+/* BCSR built on the GPU from packed COO keys: radix sort on block keys, then
+ * block densification (replaces the scipy path coo_to_metal_bcsr,
+ * iterative/BiCGSTAB/bcsr_benchmark.py:36-66). */
+mps_status mps_bcsr_create_from_keys(const uint64_t* d_keys, const float* d_vals, uint64_t nnz,
+                                     uint32_t n_rows, uint32_t n_cols, uint32_t block,
+                                     mps_bcsr** out, cudaStream_t stream);
+
+mps_status mps_bcsr_destroy(mps_bcsr* A);
+mps_status mps_bcsr_shape(const mps_bcsr* A, uint32_t* n_block_rows, uint64_t* n_blocks,
+                          uint32_t* block, uint32_t* padded_n);
+mps_status mps_bcsr_export(const mps_bcsr* A, int32_t* d_row_ptr, int32_t* d_col_ind,
+                           float* d_vals, cudaStream_t stream);
+
+/* y = A x on padded vectors (spmv_op, iterative/BiCGSTAB/bcsr_spmv.metal:30-69). */
+mps_status mps_bcsr_spmv(const mps_bcsr* A, const float* d_x, float* d_y, cudaStream_t stream);
+
+/* CG and BiCGSTAB on BCSR; b and x are padded vectors
+ * (bcsr_tensor::cgd_op / bicgstab_op, iterative/BiCGSTAB/bcsr.cpp:590-721, 761-949). */
+mps_status mps_bcsr_cg(mps_bcsr* A, const float* d_b, float* d_x, const mps_solve_opts* opts,
+                       mps_solve_info* info, cudaStream_t stream);
+mps_status mps_bcsr_bicgstab(mps_bcsr* A, const float* d_b, float* d_x,
+                             const mps_solve_opts* opts, mps_solve_info* info,
+                             cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPSPARSE_H */

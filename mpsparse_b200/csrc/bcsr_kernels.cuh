@@ -1,0 +1,195 @@
+// bcsr_kernels.cuh -- BCSR SpMV (4x4 / 8x8 row-major blocks) for sm_100a.
+//
+// Replaces spmv_op / fused_spvmv of iterative/BiCGSTAB/bcsr_spmv.metal:30-138,
+// which gives one thread to a whole block row and reads the block values with
+// uncoalesced float4 loads.  Here a persistent CTA walks tiles of consecutive
+// block rows.  A tile's block values are one contiguous byte range, so one
+// thread stages it into shared memory with a bulk async copy
+// (cp.async.bulk, completion on an mbarrier; no multicast), double-buffered so
+// the next tile streams in while this one is multiplied.  One thread then owns
+// one scalar row: it reads its B-wide row of every block from shared memory
+// and the matching x segment (float4 gathers, L2-resident), and hands the sum
+// to the same epilogues as the CSR kernel.  All mbarrier waits are bounded.
+#pragma once
+#include "common.cuh"
+#include "internal.hpp"
+
+namespace mps {
+
+struct BcsrDev {
+    const int* rp;          // block row_ptr [nbr + 1]
+    const int* ci;          // block col_ind [nb]
+    const float* v;         // nb * B * B
+    const int* tile_brow;   // ntiles + 1 block-row boundaries
+    int nbr;
+    int ntiles;
+    int cap_blocks;         // staged blocks per buffer
+    unsigned* err;
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: false if the limit ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    for (unsigned i = 0; i < kSpinLimit; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (i > 16) __nanosleep(32);
+    }
+    return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+                                         unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Row k of block j times the x segment: B-wide dot product.
+template <int B>
+__device__ __forceinline__ float block_row_dot(const float* __restrict__ row,
+                                               const float* __restrict__ x, int bc) {
+    const float4* r4 = reinterpret_cast<const float4*>(row);
+    const float4* x4 = reinterpret_cast<const float4*>(x + (size_t)bc * B);
+    float s = 0.f;
+#pragma unroll
+    for (int q = 0; q < B / 4; ++q) {
+        const float4 a = r4[q];
+        const float4 b = __ldg(x4 + q);
+        s = fmaf(a.x, b.x, s);
+        s = fmaf(a.y, b.y, s);
+        s = fmaf(a.z, b.z, s);
+        s = fmaf(a.w, b.w, s);
+    }
+    return s;
+}
+
+template <int B, class Epi, int NT = kNT>
+__global__ void __launch_bounds__(NT)
+bcsr_tiles(BcsrDev A, const float* __restrict__ x, Epi epi) {
+    extern __shared__ __align__(128) unsigned char bcsr_smem[];
+    __shared__ unsigned long long bar[2];
+    __shared__ double red[NT / 32];
+    __shared__ int last_flag;
+    __shared__ int timed_out;
+    if (blockIdx.x == 0 && threadIdx.x == 0) epi.tick();
+    if (!epi.active()) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) epi.on_skip();
+        return;
+    }
+    constexpr int BB = B * B;
+    float* buf[2] = {reinterpret_cast<float*>(bcsr_smem),
+                     reinterpret_cast<float*>(bcsr_smem) + (size_t)A.cap_blocks * BB};
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        timed_out = 0;
+        fence_mbar_init();
+    }
+    __syncthreads();
+    double acc[Epi::NS > 0 ? Epi::NS : 1];
+#pragma unroll
+    for (int i = 0; i < (Epi::NS > 0 ? Epi::NS : 1); ++i) acc[i] = 0.0;
+
+    unsigned uses[2] = {0u, 0u};   // completed phases per buffer (uniform)
+    auto staged = [&](int t) {
+        const int j0 = A.rp[A.tile_brow[t]], j1 = A.rp[A.tile_brow[t + 1]];
+        return j1 - j0 <= A.cap_blocks && j1 > j0;
+    };
+    auto issue = [&](int t, int b) {   // thread 0 only
+        const int j0 = A.rp[A.tile_brow[t]], j1 = A.rp[A.tile_brow[t + 1]];
+        const unsigned bytes = (unsigned)(j1 - j0) * BB * sizeof(float);
+        fence_proxy_async();
+        mbar_expect_tx(&bar[b], bytes);
+        bulk_g2s(buf[b], A.v + (size_t)j0 * BB, bytes, &bar[b]);
+    };
+    int it = 0;
+    int t = blockIdx.x;
+    if (t < A.ntiles && threadIdx.x == 0 && staged(t)) issue(t, 0);
+    for (; t < A.ntiles; t += gridDim.x, ++it) {
+        const int b = it & 1;
+        const int tn = t + gridDim.x;
+        // prefetch the next tile into the other buffer (freed at the end of
+        // the previous iteration)
+        if (tn < A.ntiles && threadIdx.x == 0 && staged(tn)) issue(tn, b ^ 1);
+        const int bs = A.tile_brow[t], be = A.tile_brow[t + 1];
+        const int j0 = A.rp[bs], j1 = A.rp[be];
+        const bool use_smem = j1 - j0 <= A.cap_blocks && j1 > j0;
+        if (use_smem) {
+            const bool ok = mbar_wait_bounded(&bar[b], uses[b] & 1u);
+            if (!ok) {
+                // record the phase that never completed; it is waited on
+                // once more (bounded) before the CTA exits
+                atomicOr(A.err, kErrTimeout);
+                timed_out = 1 + (b << 1) + ((uses[b] & 1u) << 2);
+            }
+            ++uses[b];
+        }
+        const int nrows = (be - bs) * B;
+        for (int lr = threadIdx.x; lr < nrows; lr += NT) {
+            const int br = bs + lr / B, k = lr % B;
+            const int jb = A.rp[br], je = A.rp[br + 1];
+            float s = 0.f;
+            if (use_smem) {
+                const float* base = buf[b] + (size_t)(jb - j0) * BB + k * B;
+                for (int j = jb; j < je; ++j, base += BB) s += block_row_dot<B>(base, x, A.ci[j]);
+            } else {
+                for (int j = jb; j < je; ++j)
+                    s += block_row_dot<B>(A.v + (size_t)j * BB + k * B, x, A.ci[j]);
+            }
+            epi.row(br * B + k, s, acc);
+        }
+        __syncthreads();   // buffer b may be refilled by the next iteration
+    }
+    // Drain: a prefetch is only issued for a tile this CTA processes and every
+    // staged tile was waited on above, so a copy can only still be in flight
+    // if its wait ran out; wait for that one again (bounded) before exiting.
+    if (threadIdx.x == 0 && timed_out) {
+        const int tb = (timed_out >> 1) & 1;
+        const unsigned par = (unsigned)(timed_out >> 2) & 1u;
+        mbar_wait_bounded(&bar[tb], par);
+    }
+    if constexpr (Epi::NS > 0) {
+#pragma unroll
+        for (int i = 0; i < Epi::NS; ++i) {
+            const double v = block_sum<NT>(acc[i], red);
+            if (threadIdx.x == 0) epi.partials[i * kMaxPartials + blockIdx.x] = v;
+        }
+        if (arrive_last(epi.counter, &last_flag)) {
+            double tot[Epi::NS];
+#pragma unroll
+            for (int i = 0; i < Epi::NS; ++i)
+                tot[i] = sum_partials<NT>(epi.partials + i * kMaxPartials, gridDim.x, red);
+            if (threadIdx.x == 0) epi.finalize(tot);
+        }
+    }
+}
+
+}  // namespace mps

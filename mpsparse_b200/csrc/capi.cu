@@ -1,0 +1,436 @@
+// capi.cu -- extern "C" entry points (include/mpsparse.h) for CSR handles.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "driver.hpp"
+
+namespace mps {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+mps_status fail(mps_status s, const std::string& msg) {
+    g_last_error = msg;
+    return s;
+}
+mps_status cuda_fail(cudaError_t e, const char* what) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? MPS_ERR_OOM : MPS_ERR_CUDA;
+}
+int num_sms() {
+    static int sms = 0;
+    if (!sms) {
+        int d = 0, v = 0;
+        cudaGetDevice(&d);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
+        sms = v > 0 ? v : 148;
+    }
+    return sms;
+}
+
+static mps_status device_error(unsigned err, const char* what) {
+    if (err & kErrRange) return fail(MPS_ERR_RANGE, std::string(what) + ": a key lies outside [0, num_rows) x [0, num_cols)");
+    if (err & kErrTimeout) return fail(MPS_ERR_TIMEOUT, std::string(what) + ": a bounded device wait gave up");
+    return MPS_OK;
+}
+
+}  // namespace mps
+
+using namespace mps;
+
+struct mps_csr {
+    CsrMat A;
+    __nv_bfloat16* vb = nullptr;
+    CsrMat G, Gt;
+    bool has_fsai = false;
+    SolverHost H;
+    unsigned* d_err = nullptr;
+};
+
+static void csr_free(CsrMat& m) {
+    if (m.rp) cudaFree(m.rp);
+    if (m.ci) cudaFree(m.ci);
+    if (m.v) cudaFree(m.v);
+    spmv_plan_free(m.plan);
+    m = CsrMat{};
+}
+
+static mps_status alloc_csr(CsrMat& m, uint32_t n_rows, uint32_t n_cols, uint64_t nnz) {
+    m.n_rows = n_rows;
+    m.n_cols = n_cols;
+    m.nnz = nnz;
+    const size_t nz = nnz ? nnz : 1;
+    MPS_CUDA(cudaMalloc(&m.rp, ((size_t)n_rows + 1) * sizeof(int32_t)));
+    MPS_CUDA(cudaMalloc(&m.ci, nz * sizeof(int32_t)));
+    MPS_CUDA(cudaMalloc(&m.v, nz * sizeof(float)));
+    return MPS_OK;
+}
+
+static mps_status check_shape(uint64_t nnz, uint32_t n_rows, uint32_t n_cols) {
+    if (n_rows == 0 || n_cols == 0) return fail(MPS_ERR_ARG, "num_rows and num_cols must be positive");
+    if (n_rows >= 0x7fffffffu || n_cols >= 0x7fffffffu) return fail(MPS_ERR_ARG, "num_rows / num_cols must be < 2^31 - 1");
+    if (nnz >= 0x7fffff00ull) return fail(MPS_ERR_ARG, "nnz must be < 2^31 (int32 row_ptr)");
+    return MPS_OK;
+}
+
+// Sort + CSR + tile plan into a fresh CsrMat.
+static mps_status build_from_keys(CsrMat& m, const uint64_t* keys, const uint32_t* payload,
+                                  uint64_t nnz, uint32_t n_rows, uint32_t n_cols, unsigned* d_err,
+                                  cudaStream_t s) {
+    mps_status st = alloc_csr(m, n_rows, n_cols, nnz);
+    if (st != MPS_OK) return st;
+    MPS_CUDA(cudaMemsetAsync(d_err, 0, sizeof(unsigned), s));
+    MPS_CUDA(sort_to_csr(keys, payload, nnz, n_rows, n_cols, m.rp, m.ci, (uint32_t*)m.v, d_err, s));
+    MPS_CUDA(spmv_plan_build(m, 0, s));
+    unsigned err = 0;
+    MPS_CUDA(cudaMemcpyAsync(&err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    MPS_CUDA(cudaStreamSynchronize(s));
+    return device_error(err, "COO->CSR");
+}
+
+extern "C" {
+
+int32_t mps_abi_version(void) { return 1; }
+
+void mps_solve_opts_default(mps_solve_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->tol = 1e-6;
+    o->max_iter = 2000;
+    o->omega = 0.01;
+    o->stall_window = 200;
+}
+
+const char* mps_last_error_string(void) { return g_last_error.c_str(); }
+
+const char* mps_status_string(mps_status s) {
+    switch (s) {
+        case MPS_OK: return "ok";
+        case MPS_ERR_ARG: return "invalid argument";
+        case MPS_ERR_CUDA: return "CUDA error";
+        case MPS_ERR_OOM: return "out of device memory";
+        case MPS_ERR_TIMEOUT: return "device wait timed out";
+        case MPS_ERR_BREAKDOWN: return "solver breakdown";
+        case MPS_ERR_RANGE: return "key out of range";
+        case MPS_ERR_NOT_FINITE: return "non-finite input";
+    }
+    return "unknown status";
+}
+
+mps_status mps_csr_create_from_keys(const uint64_t* d_keys, const float* d_vals, uint64_t nnz,
+                                    uint32_t n_rows, uint32_t n_cols, mps_csr** out,
+                                    cudaStream_t stream) {
+    if (!out) return fail(MPS_ERR_ARG, "out is null");
+    *out = nullptr;
+    mps_status st = check_shape(nnz, n_rows, n_cols);
+    if (st != MPS_OK) return st;
+    if (nnz && (!d_keys || !d_vals)) return fail(MPS_ERR_ARG, "keys / values are null");
+    mps_csr* h = new mps_csr();
+    MPS_CUDA(cudaMalloc(&h->d_err, sizeof(unsigned)));
+    st = build_from_keys(h->A, d_keys, reinterpret_cast<const uint32_t*>(d_vals), nnz, n_rows,
+                         n_cols, h->d_err, stream);
+    if (st != MPS_OK) {
+        mps_csr_destroy(h);
+        return st;
+    }
+    *out = h;
+    return MPS_OK;
+}
+
+mps_status mps_csr_create_from_csr(const int32_t* d_row_ptr, const int32_t* d_col_ind,
+                                   const float* d_vals, uint32_t n_rows, uint32_t n_cols,
+                                   uint64_t nnz, mps_csr** out, cudaStream_t stream) {
+    if (!out) return fail(MPS_ERR_ARG, "out is null");
+    *out = nullptr;
+    mps_status st = check_shape(nnz, n_rows, n_cols);
+    if (st != MPS_OK) return st;
+    if (!d_row_ptr || (nnz && (!d_col_ind || !d_vals))) return fail(MPS_ERR_ARG, "null CSR array");
+    mps_csr* h = new mps_csr();
+    MPS_CUDA(cudaMalloc(&h->d_err, sizeof(unsigned)));
+    st = alloc_csr(h->A, n_rows, n_cols, nnz);
+    if (st != MPS_OK) {
+        mps_csr_destroy(h);
+        return st;
+    }
+    MPS_CUDA(cudaMemcpyAsync(h->A.rp, d_row_ptr, ((size_t)n_rows + 1) * 4, cudaMemcpyDeviceToDevice, stream));
+    if (nnz) {
+        MPS_CUDA(cudaMemcpyAsync(h->A.ci, d_col_ind, nnz * 4, cudaMemcpyDeviceToDevice, stream));
+        MPS_CUDA(cudaMemcpyAsync(h->A.v, d_vals, nnz * 4, cudaMemcpyDeviceToDevice, stream));
+    }
+    cudaError_t e = spmv_plan_build(h->A, 0, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        mps_csr_destroy(h);
+        return cuda_fail(e, "create_from_csr");
+    }
+    *out = h;
+    return MPS_OK;
+}
+
+mps_status mps_csr_destroy(mps_csr* h) {
+    if (!h) return MPS_OK;
+    csr_free(h->A);
+    csr_free(h->G);
+    csr_free(h->Gt);
+    if (h->vb) cudaFree(h->vb);
+    if (h->d_err) cudaFree(h->d_err);
+    h->H.destroy();
+    delete h;
+    return MPS_OK;
+}
+
+mps_status mps_csr_shape(const mps_csr* h, uint32_t* n_rows, uint32_t* n_cols, uint64_t* nnz) {
+    if (!h) return fail(MPS_ERR_ARG, "null handle");
+    if (n_rows) *n_rows = h->A.n_rows;
+    if (n_cols) *n_cols = h->A.n_cols;
+    if (nnz) *nnz = h->A.nnz;
+    return MPS_OK;
+}
+
+mps_status mps_csr_export(const mps_csr* h, int32_t* d_row_ptr, int32_t* d_col_ind, float* d_vals,
+                          cudaStream_t s) {
+    if (!h) return fail(MPS_ERR_ARG, "null handle");
+    if (d_row_ptr)
+        MPS_CUDA(cudaMemcpyAsync(d_row_ptr, h->A.rp, ((size_t)h->A.n_rows + 1) * 4, cudaMemcpyDefault, s));
+    if (d_col_ind && h->A.nnz)
+        MPS_CUDA(cudaMemcpyAsync(d_col_ind, h->A.ci, h->A.nnz * 4, cudaMemcpyDefault, s));
+    if (d_vals && h->A.nnz)
+        MPS_CUDA(cudaMemcpyAsync(d_vals, h->A.v, h->A.nnz * 4, cudaMemcpyDefault, s));
+    return MPS_OK;
+}
+
+mps_status mps_coo_to_csr(const uint64_t* d_keys, const float* d_vals, uint64_t nnz,
+                          uint32_t n_rows, uint32_t n_cols, int32_t* d_row_ptr, int32_t* d_col_ind,
+                          float* d_out_vals, cudaStream_t s) {
+    mps_status st = check_shape(nnz, n_rows, n_cols);
+    if (st != MPS_OK) return st;
+    if (!d_row_ptr || (nnz && (!d_keys || !d_vals || !d_col_ind || !d_out_vals)))
+        return fail(MPS_ERR_ARG, "null pointer");
+    unsigned* d_err = nullptr;
+    MPS_CUDA(cudaMallocAsync(&d_err, sizeof(unsigned), s));
+    MPS_CUDA(cudaMemsetAsync(d_err, 0, sizeof(unsigned), s));
+    cudaError_t e = sort_to_csr(d_keys, reinterpret_cast<const uint32_t*>(d_vals), nnz, n_rows,
+                                n_cols, d_row_ptr, d_col_ind, reinterpret_cast<uint32_t*>(d_out_vals),
+                                d_err, s);
+    unsigned err = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(d_err, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "coo_to_csr");
+    return device_error(err, "COO->CSR");
+}
+
+mps_status mps_csr_spmv(const mps_csr* h, const float* d_x, float* d_y, cudaStream_t s) {
+    if (!h || !d_x || !d_y) return fail(MPS_ERR_ARG, "null argument");
+    MPS_CUDA(spmv_launch(h->A, d_x, d_y, s));
+    return MPS_OK;
+}
+
+mps_status mps_csr_spmv_dot(const mps_csr* hc, const float* d_x, const float* d_w, float* d_y,
+                            double* d_dot, cudaStream_t s) {
+    mps_csr* h = const_cast<mps_csr*>(hc);
+    if (!h || !d_x || !d_w || !d_y || !d_dot) return fail(MPS_ERR_ARG, "null argument");
+    MPS_CUDA(h->H.ensure(h->A.n_rows));
+    MPS_CUDA(spmv_dot_launch(h->A, d_x, d_w, d_y, d_dot, h->H.ws.partials, h->H.ws.counters + 12, s));
+    return MPS_OK;
+}
+
+static mps_status prepare_precond(mps_csr* h, const mps_solve_opts* o, cudaStream_t s) {
+    MPS_CUDA(h->H.ensure(h->A.n_rows));
+    const int pc = o ? o->precond : 0;
+    if (pc != MPS_PRECOND_NONE && !(o && o->reference_compat)) {
+        if (pc == MPS_PRECOND_FSAI && !h->has_fsai)
+            return fail(MPS_ERR_ARG, "FSAI preconditioner requested but no factor was attached");
+        if (pc != MPS_PRECOND_JACOBI && pc != MPS_PRECOND_FSAI)
+            return fail(MPS_ERR_ARG, "unknown preconditioner");
+        if (!h->H.dinv) {
+            MPS_CUDA(cudaMalloc(&h->H.dinv, h->H.ws.n_pad * sizeof(float)));
+            MPS_CUDA(cudaMemsetAsync(h->H.dinv, 0, h->H.ws.n_pad * sizeof(float), s));
+            MPS_CUDA(diag_inv_launch(h->A, h->H.dinv, s));
+            h->H.drop_graphs();   // graphs captured the previous (null) diagonal
+        }
+    }
+    return MPS_OK;
+}
+
+static mps_status csr_solve(SolverKind kind, mps_csr* h, const float* b, float* x,
+                            const mps_solve_opts* o, mps_solve_info* info, cudaStream_t s) {
+    if (!h || !b || !x) return fail(MPS_ERR_ARG, "null argument");
+    if (h->A.n_rows != h->A.n_cols) return fail(MPS_ERR_ARG, "solvers need a square matrix");
+    mps_status st = prepare_precond(h, kind == kCG ? o : nullptr, s);
+    if (st != MPS_OK) return st;
+    CsrOp op{&h->A, nullptr};
+    CsrOp g{&h->G, nullptr}, gt{&h->Gt, nullptr};
+    PrecondOps<CsrOp> pc{h->has_fsai ? &g : nullptr, h->has_fsai ? &gt : nullptr};
+    return run_solve(kind, op, pc, h->H, b, x, o, info, s);
+}
+
+mps_status mps_csr_cg(mps_csr* h, const float* b, float* x, const mps_solve_opts* o,
+                      mps_solve_info* info, cudaStream_t s) {
+    return csr_solve(kCG, h, b, x, o, info, s);
+}
+
+mps_status mps_csr_bicgstab(mps_csr* h, const float* b, float* x, const mps_solve_opts* o,
+                            mps_solve_info* info, cudaStream_t s) {
+    return csr_solve(kBiCG, h, b, x, o, info, s);
+}
+
+mps_status mps_csr_richardson(mps_csr* h, const float* b, float* x, const mps_solve_opts* o,
+                              mps_solve_info* info, cudaStream_t s) {
+    return csr_solve(kRich, h, b, x, o, info, s);
+}
+
+mps_status mps_csr_set_fsai(mps_csr* h, const int32_t* d_g_row_ptr, const int32_t* d_g_col_ind,
+                            const float* d_g_vals, uint64_t g_nnz, cudaStream_t s) {
+    if (!h || !d_g_row_ptr || !d_g_col_ind || !d_g_vals) return fail(MPS_ERR_ARG, "null argument");
+    const uint32_t n = h->A.n_rows;
+    csr_free(h->G);
+    csr_free(h->Gt);
+    h->has_fsai = false;
+    h->H.drop_graphs();
+    mps_status st = alloc_csr(h->G, n, n, g_nnz);
+    if (st != MPS_OK) return st;
+    MPS_CUDA(cudaMemcpyAsync(h->G.rp, d_g_row_ptr, ((size_t)n + 1) * 4, cudaMemcpyDeviceToDevice, s));
+    MPS_CUDA(cudaMemcpyAsync(h->G.ci, d_g_col_ind, g_nnz * 4, cudaMemcpyDeviceToDevice, s));
+    MPS_CUDA(cudaMemcpyAsync(h->G.v, d_g_vals, g_nnz * 4, cudaMemcpyDeviceToDevice, s));
+    MPS_CUDA(spmv_plan_build(h->G, 0, s));
+    // G^T through the same radix sort on (col<<32 | row) keys.
+    unsigned long long* keys = nullptr;
+    MPS_CUDA(cudaMallocAsync(&keys, (g_nnz ? g_nnz : 1) * 8, s));
+    MPS_CUDA(transpose_keys_launch(h->G, keys, s));
+    st = build_from_keys(h->Gt, reinterpret_cast<const uint64_t*>(keys),
+                         reinterpret_cast<const uint32_t*>(h->G.v), g_nnz, n, n, h->d_err, s);
+    cudaFreeAsync(keys, s);
+    if (st != MPS_OK) return st;
+    h->has_fsai = true;
+    return MPS_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Mixed-precision CG with FP64 iterative refinement.
+// ---------------------------------------------------------------------------
+namespace mps {
+
+// r32 = (float)(b - A x) with FP64 gathers of x and FP64 accumulation over the
+// FP32 matrix values; ||b - A x||^2 in FP64.
+struct EpiResid64 {
+    static constexpr int NS = 1;
+    const double* b;
+    float* r32;
+    double* out;
+    unsigned* counter;
+    double* partials;
+    __device__ bool active() const { return true; }
+    __device__ void tick() const {}
+    __device__ void on_skip() const {}
+    __device__ void row(int r, double s, double* acc) const {
+        const double rv = b[r] - s;
+        r32[r] = (float)rv;
+        acc[0] += rv * rv;
+    }
+    __device__ void finalize(const double* tot) const { *out = tot[0]; }
+};
+
+__global__ void ir_accumulate(double* __restrict__ x, const float* __restrict__ d, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        x[i] += (double)d[i];
+}
+
+__global__ void sumsq64(const double* __restrict__ b, int n, double* out, double* part,
+                        unsigned* ctr) {
+    __shared__ double red[kNT / 32];
+    __shared__ int last;
+    double a = 0.0;
+    for (int i = blockIdx.x * kNT + threadIdx.x; i < n; i += gridDim.x * kNT) a += b[i] * b[i];
+    const double v = block_sum<kNT>(a, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = v;
+    if (!arrive_last(ctr, &last)) return;
+    const double t = sum_partials<kNT>(part, gridDim.x, red);
+    if (threadIdx.x == 0) *out = t;
+}
+
+}  // namespace mps
+
+extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_x,
+                                       const mps_ir_opts* o_in, mps_ir_info* info,
+                                       cudaStream_t s) {
+    if (!h || !d_b || !d_x) return fail(MPS_ERR_ARG, "null argument");
+    if (h->A.n_rows != h->A.n_cols) return fail(MPS_ERR_ARG, "solvers need a square matrix");
+    mps_ir_opts o{};
+    if (o_in) o = *o_in;
+    const double tol = o.tol > 0 ? o.tol : 1e-10;
+    const double inner_tol = o.inner_tol > 0 ? o.inner_tol : 1e-3;
+    const int max_outer = o.max_outer > 0 ? o.max_outer : 50;
+    const int max_inner = o.max_inner > 0 ? o.max_inner : 2000;
+    const bool bf16 = o.value_bits == 16;
+    if (o.value_bits != 0 && o.value_bits != 16 && o.value_bits != 32)
+        return fail(MPS_ERR_ARG, "value_bits must be 16 or 32");
+    mps_solve_opts io;
+    mps_solve_opts_default(&io);
+    io.tol = inner_tol;
+    io.max_iter = max_inner;
+    io.precond = o.precond;
+    mps_status st = prepare_precond(h, &io, s);
+    if (st != MPS_OK) return st;
+    SolverHost& H = h->H;
+    const int n = (int)h->A.n_rows;
+    if (bf16 && !h->vb) {
+        MPS_CUDA(cudaMalloc(&h->vb, (h->A.nnz ? h->A.nnz : 1) * sizeof(__nv_bfloat16)));
+        MPS_CUDA(to_bf16_launch(h->A.v, h->vb, h->A.nnz, s));
+    }
+    double* scal = nullptr;   // [0] = ||b||^2, [1] = ||r||^2
+    MPS_CUDA(cudaMallocAsync(&scal, 2 * sizeof(double), s));
+    float* r32 = H.v(vTmp0);
+    float* d32 = H.v(vTmp1);
+    const int g = H.vgrid();
+    sumsq64<<<g, kNT, 0, s>>>(d_b, n, scal, H.ws.partials, H.ws.counters + 13);
+    MPS_CUDA(cudaMemsetAsync(d_x, 0, (size_t)n * sizeof(double), s));
+    double hs[2] = {0, 0};
+    MPS_CUDA(cudaMemcpyAsync(hs, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+    MPS_CUDA(cudaStreamSynchronize(s));
+    const double bnorm = std::sqrt(hs[0]);
+    CsrOp inner{&h->A, bf16 ? h->vb : nullptr};
+    CsrOp gop{&h->G, nullptr}, gtop{&h->Gt, nullptr};
+    PrecondOps<CsrOp> pc{h->has_fsai ? &gop : nullptr, h->has_fsai ? &gtop : nullptr};
+    const CsrDev view = h->A.view();
+    const size_t smem = spmv_smem_bytes<double>(view);
+    smem_optin_k(spmv_tiles<double, double, false, EpiResid64>, smem);
+    int outer = 0, inner_total = 0;
+    bool converged = false;
+    double rel = 1.0;
+    for (;; ++outer) {
+        // FP64 outer residual r = b - A x (FP32 copy feeds the inner solve)
+        spmv_tiles<double, double, false, EpiResid64><<<h->A.plan.grid, kNT, smem, s>>>(
+            view, d_x, EpiResid64{d_b, r32, scal + 1, H.ws.counters + 14, H.ws.partials});
+        MPS_CUDA(cudaGetLastError());
+        MPS_CUDA(cudaMemcpyAsync(hs + 1, scal + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+        MPS_CUDA(cudaStreamSynchronize(s));
+        rel = bnorm > 0 ? std::sqrt(hs[1]) / bnorm : std::sqrt(hs[1]);
+        if (!std::isfinite(rel)) break;
+        if (rel <= tol || bnorm == 0.0) {
+            converged = true;
+            break;
+        }
+        if (outer >= max_outer) break;
+        mps_solve_info ii{};
+        st = run_solve(kCG, inner, pc, H, r32, d32, &io, &ii, s, bf16 ? 1 : 0);
+        if (st != MPS_OK) break;
+        inner_total += ii.iters;
+        ir_accumulate<<<g, kNT, 0, s>>>(d_x, d32, n);
+        MPS_CUDA(cudaGetLastError());
+        if (ii.iters == 0) break;
+    }
+    cudaFreeAsync(scal, s);
+    if (info) {
+        info->outer_iters = outer;
+        info->inner_iters = inner_total;
+        info->converged = converged;
+        info->reserved = 0;
+        info->rel_resid = rel;
+    }
+    return st;
+}

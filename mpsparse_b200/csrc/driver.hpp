@@ -1,0 +1,314 @@
+// driver.hpp -- host driver shared by the CSR and BCSR solvers: workspace,
+// graph capture with a device-side WHILE loop, result and info read-back.
+#pragma once
+#include "solvers.cuh"
+
+namespace mps {
+
+cudaError_t diag_inv_launch(const CsrMat& A, float* dinv, cudaStream_t s);
+cudaError_t transpose_keys_launch(const CsrMat& A, unsigned long long* keys, cudaStream_t s);
+cudaError_t to_bf16_launch(const float* v, __nv_bfloat16* o, uint64_t n, cudaStream_t s);
+int default_tile_nnz(uint64_t nnz, uint32_t n_rows);
+
+template <class K>
+inline void smem_optin_k(K kernel, size_t smem) {
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+// CSR operator: A x through the tile kernel with a given epilogue.
+struct CsrOp {
+    const CsrMat* A;
+    const __nv_bfloat16* vb = nullptr;
+    template <class Epi>
+    cudaError_t apply(const float* x, const Epi& e, cudaStream_t s) const {
+        const CsrDev v = A->view(vb);
+        const size_t smem = spmv_smem_bytes<float>(v);
+        if (vb) {
+            smem_optin_k(spmv_tiles<float, float, true, Epi>, smem);
+            spmv_tiles<float, float, true, Epi><<<A->plan.grid, kNT, smem, s>>>(v, x, e);
+        } else {
+            smem_optin_k(spmv_tiles<float, float, false, Epi>, smem);
+            spmv_tiles<float, float, false, Epi><<<A->plan.grid, kNT, smem, s>>>(v, x, e);
+        }
+        return cudaGetLastError();
+    }
+};
+
+enum SolverKind { kCG = 0, kBiCG = 1, kRich = 2 };
+enum VecSlot { vB = 0, vX, vR, vP, vQ, vR0, vS, vT, vXAlt, vW, vTmp0, vTmp1 };
+
+// State a handle keeps for its solvers.
+struct SolverHost {
+    Workspace ws;
+    GraphCache graphs[32];
+    cudaStream_t cap = nullptr;
+    SolveParams* h_params = nullptr;   // pinned
+    float* dinv = nullptr;             // padded
+    int n = 0;
+
+    float* v(int slot) const { return ws.vec[slot]; }
+    float4* v4(int slot) const { return reinterpret_cast<float4*>(ws.vec[slot]); }
+    int n4() const { return (int)(ws.n_pad / 4); }
+    int vgrid() const {
+        int g = (n4() + kNT - 1) / kNT;
+        const int cap_g = num_sms() * 4;
+        if (g > cap_g) g = cap_g;
+        return g < 1 ? 1 : g;
+    }
+    Ctx ctx(cudaGraphConditionalHandle h, int use) const {
+        return Ctx{ws.sc, ws.partials, ws.counters, h, use};
+    }
+
+    cudaError_t ensure(size_t n_rows) {
+        n = (int)n_rows;
+        const size_t n_pad = (n_rows + 3) & ~size_t(3);
+        if (ws.sc && ws.n_pad >= n_pad) return cudaSuccess;
+        release();
+        cudaError_t e;
+        float* block = nullptr;
+        const size_t nv = sizeof(ws.vec) / sizeof(ws.vec[0]);
+        if ((e = cudaMalloc(&block, nv * (n_pad ? n_pad : 4) * sizeof(float))) != cudaSuccess) return e;
+        if ((e = cudaMemset(block, 0, nv * (n_pad ? n_pad : 4) * sizeof(float))) != cudaSuccess) return e;
+        for (size_t i = 0; i < nv; ++i) ws.vec[i] = block + i * (n_pad ? n_pad : 4);
+        if ((e = cudaMalloc(&ws.partials, 4 * kMaxPartials * sizeof(double))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&ws.counters, 16 * sizeof(unsigned))) != cudaSuccess) return e;
+        if ((e = cudaMemset(ws.counters, 0, 16 * sizeof(unsigned))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&ws.sc, sizeof(DevScalars))) != cudaSuccess) return e;
+        if ((e = cudaMemset(ws.sc, 0, sizeof(DevScalars))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&ws.d_params, sizeof(SolveParams))) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&ws.h_sc, sizeof(DevScalars))) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&h_params, sizeof(SolveParams))) != cudaSuccess) return e;
+        if (!cap && (e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        ws.n_pad = n_pad ? n_pad : 4;
+        return cudaSuccess;
+    }
+    void drop_graphs() {
+        for (auto& g : graphs) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            if (g.graph) cudaGraphDestroy(g.graph);
+            g = GraphCache{};
+        }
+    }
+    void release() {
+        drop_graphs();
+        if (ws.vec[0]) cudaFree(ws.vec[0]);
+        if (ws.partials) cudaFree(ws.partials);
+        if (ws.counters) cudaFree(ws.counters);
+        if (ws.sc) cudaFree(ws.sc);
+        if (ws.d_params) cudaFree(ws.d_params);
+        if (ws.h_sc) cudaFreeHost(ws.h_sc);
+        if (h_params) cudaFreeHost(h_params);
+        if (dinv) cudaFree(dinv);
+        ws = Workspace{};
+        h_params = nullptr;
+        dinv = nullptr;
+    }
+    void destroy() {
+        release();
+        if (cap) cudaStreamDestroy(cap);
+        cap = nullptr;
+    }
+};
+
+// Preconditioner operators for PCG (FSAI: G and G^T as CSR).
+template <class Op>
+struct PrecondOps {
+    const CsrOp* G = nullptr;
+    const CsrOp* Gt = nullptr;
+};
+
+template <class Op>
+cudaError_t launch_init(SolverKind kind, int precond, const Op& op, const PrecondOps<Op>& pc,
+                        SolverHost& H, const Ctx& c, cudaStream_t s) {
+    const int n4 = H.n4(), g = H.vgrid();
+    DevScalars* sc = H.ws.sc;
+    switch (kind) {
+        case kCG:
+            cg_init<<<g, kNT, 0, s>>>(H.v4(vB), H.v4(vX), H.v4(vR), H.v4(vP),
+                                      reinterpret_cast<const float4*>(H.dinv), n4, H.n,
+                                      H.ws.d_params, c);
+            if (precond == MPS_PRECOND_FSAI) {
+                cudaError_t e = pc.G->apply(H.v(vR), EpiFsai1{H.v(vW), sc, c.ctr + 3, c.part}, s);
+                if (e != cudaSuccess) return e;
+                e = pc.Gt->apply(H.v(vW), EpiFsai2{H.v(vP), sc}, s);
+                if (e != cudaSuccess) return e;
+            }
+            break;
+        case kBiCG:
+            bicg_init<<<g, kNT, 0, s>>>(H.v4(vB), H.v4(vX), H.v4(vR), H.v4(vR0), H.v4(vP),
+                                        H.v4(vQ), n4, H.n, H.ws.d_params, c);
+            break;
+        case kRich:
+            rich_init<<<g, kNT, 0, s>>>(H.v4(vB), H.v4(vX), n4, H.n, H.ws.d_params, c);
+            break;
+    }
+    return cudaGetLastError();
+}
+
+template <class Op>
+cudaError_t launch_body(SolverKind kind, int precond, const Op& op, const PrecondOps<Op>& pc,
+                        SolverHost& H, const Ctx& c, cudaStream_t s) {
+    const int n4 = H.n4(), g = H.vgrid();
+    DevScalars* sc = H.ws.sc;
+    cudaError_t e = cudaSuccess;
+    const float4* dinv4 = reinterpret_cast<const float4*>(H.dinv);
+    switch (kind) {
+        case kCG:
+            e = op.apply(H.v(vP), EpiCgPq{H.v(vQ), H.v(vP), sc, c.ctr + 1, c.part}, s);
+            if (e != cudaSuccess) return e;
+            cg_update_xr<<<g, kNT, 0, s>>>(H.v4(vX), H.v4(vR), H.v4(vP), H.v4(vQ),
+                                           precond ? dinv4 : nullptr, n4, c);
+            if (precond == MPS_PRECOND_FSAI) {
+                e = pc.G->apply(H.v(vR), EpiFsai1{H.v(vW), sc, c.ctr + 3, c.part}, s);
+                if (e != cudaSuccess) return e;
+                e = pc.Gt->apply(H.v(vW), EpiFsai2{H.v(vP), sc}, s);
+                if (e != cudaSuccess) return e;
+            }
+            cg_update_p<<<g, kNT, 0, s>>>(H.v4(vP), H.v4(vR), dinv4, n4, c);
+            break;
+        case kBiCG:
+            bicg_update_p<<<g, kNT, 0, s>>>(H.v4(vP), H.v4(vR), H.v4(vQ), n4, c);
+            e = op.apply(H.v(vP), EpiBicgV{H.v(vQ), H.v(vR0), sc, c.ctr + 5, c.part}, s);
+            if (e != cudaSuccess) return e;
+            bicg_update_s<<<g, kNT, 0, s>>>(H.v4(vS), H.v4(vR), H.v4(vQ), n4, c);
+            e = op.apply(H.v(vS), EpiBicgT{H.v(vT), H.v(vS), sc, c.ctr + 6, c.part}, s);
+            if (e != cudaSuccess) return e;
+            bicg_update_xr<<<g, kNT, 0, s>>>(H.v4(vX), H.v4(vR), H.v4(vP), H.v4(vR0), H.v4(vS),
+                                             H.v4(vT), H.v4(vXAlt), n4, c);
+            break;
+        case kRich:
+            e = op.apply(H.v(vX), EpiRich{H.v(vX), H.v(vXAlt), H.v(vB), sc, c.ctr + 9, c.part, c, 0}, s);
+            if (e != cudaSuccess) return e;
+            e = op.apply(H.v(vXAlt), EpiRich{H.v(vXAlt), H.v(vX), H.v(vB), sc, c.ctr + 10, c.part, c, 1}, s);
+            break;
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return e;
+}
+
+// Capture: [init kernels] -> WHILE(cond) { body kernels }.
+template <class Op>
+cudaError_t build_graph(SolverKind kind, int precond, const Op& op, const PrecondOps<Op>& pc,
+                        SolverHost& H, GraphCache& gc) {
+    cudaStream_t cs = H.cap;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaGraphConditionalHandle h{};
+    cudaGraphNode_t cn;
+    cudaGraphNodeParams cp = {};
+    cudaGraph_t body = nullptr;
+    if ((e = cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd)) != cudaSuccess) goto abort;
+    if ((e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault)) != cudaSuccess)
+        goto abort;
+    if ((e = launch_init(kind, precond, op, pc, H, H.ctx(h, 1), cs)) != cudaSuccess) goto abort;
+    if ((e = cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd)) != cudaSuccess) goto abort;
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    if ((e = cudaGraphAddNode(&cn, g, deps, nd, &cp)) != cudaSuccess) goto abort;
+    body = cp.conditional.phGraph_out[0];
+    if ((e = cudaStreamUpdateCaptureDependencies(cs, &cn, 1, cudaStreamSetCaptureDependencies)) !=
+        cudaSuccess)
+        goto abort;
+    if ((e = cudaStreamEndCapture(cs, &g)) != cudaSuccess) return e;
+    if ((e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return e;
+    }
+    e = launch_body(kind, precond, op, pc, H, H.ctx(h, 1), cs);
+    {
+        cudaGraph_t b2 = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(cs, &b2);
+        if (e == cudaSuccess) e = e2;
+    }
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return e;
+    }
+    e = cudaGraphInstantiate(&gc.exec, g, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        gc = GraphCache{};
+        return e;
+    }
+    gc.graph = g;
+    return cudaSuccess;
+abort:
+    {
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(cs, &junk);
+        if (junk) cudaGraphDestroy(junk);
+    }
+    return e;
+}
+
+// Run one solve: b (device, n floats) -> x (device, n floats).
+template <class Op>
+mps_status run_solve(SolverKind kind, const Op& op, const PrecondOps<Op>& pc, SolverHost& H,
+                     const float* d_b, float* d_x, const mps_solve_opts* o_in,
+                     mps_solve_info* info, cudaStream_t s, int variant = 0) {
+    mps_solve_opts o;
+    mps_solve_opts_default(&o);
+    if (o_in) o = *o_in;
+    SolveParams& P = *H.h_params;
+    P.tol = o.tol > 0 ? o.tol : 1e-6;
+    P.omega = o.omega != 0 ? o.omega : 0.01;
+    P.max_iter = o.max_iter > 0 ? o.max_iter : 2000;
+    P.compat = o.reference_compat ? 1 : 0;
+    P.precond = kind == kCG && !P.compat ? o.precond : 0;
+    P.stall_window = o.stall_window > 0 ? o.stall_window : 200;
+    const int precond = P.precond;
+    MPS_CUDA(cudaMemcpyAsync(H.ws.d_params, H.h_params, sizeof(SolveParams), cudaMemcpyHostToDevice, s));
+    MPS_CUDA(cudaMemcpyAsync(H.v(vB), d_b, (size_t)H.n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    if (!o.host_loop) {
+        GraphCache& gc = H.graphs[(kind * 4 + precond) * 2 + (variant & 1)];
+        if (!gc.exec) {
+            // captured once per (solver, preconditioner) on the handle's
+            // private stream; the graph only references handle-owned buffers
+            cudaError_t e = build_graph(kind, precond, op, pc, H, gc);
+            if (e != cudaSuccess) return cuda_fail(e, "solver graph capture");
+        }
+        MPS_CUDA(cudaGraphLaunch(gc.exec, s));
+    } else {
+        MPS_CUDA(launch_init(kind, precond, op, pc, H, H.ctx({}, 0), s));
+        const int per_poll = 16;
+        for (long it = 0;; it += per_poll) {
+            for (int k = 0; k < per_poll; ++k) MPS_CUDA(launch_body(kind, precond, op, pc, H, H.ctx({}, 0), s));
+            MPS_CUDA(cudaMemcpyAsync(H.ws.h_sc, H.ws.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
+            MPS_CUDA(cudaStreamSynchronize(s));
+            if (H.ws.h_sc->done) break;
+            if (it > 100000000L) return fail(MPS_ERR_TIMEOUT, "host loop did not stop");
+        }
+    }
+    {
+        const int nb = (H.n + 255) / 256;
+        copy_result<<<nb < 1184 ? (nb ? nb : 1) : 1184, 256, 0, s>>>(
+            H.v(vX), H.v(vXAlt), H.v(vXAlt), d_x, H.n, kind == kRich ? kResRich : kResX, H.ws.sc);
+        MPS_CUDA(cudaGetLastError());
+    }
+    MPS_CUDA(cudaMemcpyAsync(H.ws.h_sc, H.ws.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
+    MPS_CUDA(cudaStreamSynchronize(s));
+    const DevScalars& r = *H.ws.h_sc;
+    if (info) {
+        info->iters = r.iter;
+        info->converged = r.converged;
+        info->breakdown = r.breakdown;
+        info->stalled = r.stalled;
+        info->compat_snapshot = r.snapshot;
+        info->reserved = 0;
+        const double num = kind == kCG ? r.rr : r.rnorm2;
+        info->rel_resid = r.bnorm2 > 0 ? sqrt(num / r.bnorm2) : sqrt(num);
+    }
+    if (r.err & kErrNotFinite) return fail(MPS_ERR_NOT_FINITE, "right-hand side holds NaN or Inf");
+    if (r.err & kErrTimeout) return fail(MPS_ERR_TIMEOUT, "solver loop stopped by its watchdog");
+    return MPS_OK;
+}
+
+}  // namespace mps

@@ -1,0 +1,126 @@
+// internal.hpp -- host-side structures shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/mpsparse.h"
+
+namespace mps {
+
+// ---- error plumbing -------------------------------------------------------
+void set_error(const std::string& msg);
+mps_status fail(mps_status s, const std::string& msg);
+mps_status cuda_fail(cudaError_t e, const char* what);
+#define MPS_CUDA(call)                                             \
+    do {                                                           \
+        cudaError_t _e = (call);                                   \
+        if (_e != cudaSuccess) return ::mps::cuda_fail(_e, #call); \
+    } while (0)
+
+int num_sms();
+
+// ---- device scalar block of one solve --------------------------------------
+// One instance lives in device memory per handle; the host mirrors it into
+// pinned memory at the end of a solve.
+struct DevScalars {
+    // Krylov scalars (FP64: the alpha/beta/omega reductions run in FP64)
+    double rr, rz, pq, alpha, beta;
+    double rho, rho_old, omega, sigma, phi1, phi2, rnorm2;
+    double bnorm2, tol2, staged, best_rr;
+    double omega_rich;
+    // control
+    int iter, max_iter, done, converged, breakdown, stalled, snapshot, compat;
+    int mode;           // preconditioner in force: 0 none, 1 Jacobi, 2 FSAI
+    int best_iter, stall_window, err;
+    int n;              // rows
+    int restart;        // next direction update restarts (beta = 0)
+    int guard;          // loop bodies executed (watchdog)
+    int guard_limit;    // watchdog bound: a loop never runs more bodies than this
+};
+
+// Parameters copied host->device before each solve.
+struct SolveParams {
+    double tol;
+    double omega;
+    int max_iter;
+    int compat;
+    int precond;
+    int stall_window;
+};
+
+// ---- CSR views ---------------------------------------------------------------
+struct CsrDev {
+    const int* rp;
+    const int* ci;
+    const float* v;
+    const __nv_bfloat16* vb;
+    const int* tile_row;   // ntiles + 1 row boundaries of the SpMV tiles
+    int n_rows;
+    int ntiles;
+    int cap;               // shared-memory product capacity of a tile
+};
+
+struct SpmvPlan {
+    int tile_nnz = 0;      // target nnz per tile
+    int ntiles = 0;
+    int cap = 0;
+    int grid = 0;          // persistent CTAs
+    int* d_tile_row = nullptr;
+};
+
+// Launch geometry of the streaming vector kernels.
+struct VecGeom {
+    int grid;
+    int n4;                // float4 count over the padded length
+};
+
+constexpr int kNT = 256;           // threads per CTA of the solver kernels
+constexpr int kMaxPartials = 4096; // FP64 partial slots per reduction
+
+// Solver workspace owned by a handle (lazily allocated, padded to x4 floats).
+struct Workspace {
+    size_t n_pad = 0;
+    float* vec[12] = {};
+    double* partials = nullptr;    // 4 * kMaxPartials
+    unsigned* counters = nullptr;  // 16
+    DevScalars* sc = nullptr;
+    DevScalars* h_sc = nullptr;    // pinned mirror
+    SolveParams* d_params = nullptr;
+};
+
+struct GraphCache {
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+};
+
+struct CsrMat {
+    int32_t* rp = nullptr;
+    int32_t* ci = nullptr;
+    float* v = nullptr;
+    uint32_t n_rows = 0, n_cols = 0;
+    uint64_t nnz = 0;
+    SpmvPlan plan;
+    CsrDev view(const __nv_bfloat16* vb = nullptr) const {
+        return CsrDev{rp, ci, v, vb, plan.d_tile_row, (int)n_rows, plan.ntiles, plan.cap};
+    }
+};
+
+// ---- internal entry points ---------------------------------------------------
+// Sort packed keys into CSR arrays (caller-allocated outputs).  `payload` is
+// moved as 32-bit words.  Returns a CUDA error; device-side range / timeout
+// errors are OR-ed into *d_err.
+cudaError_t sort_to_csr(const uint64_t* keys, const uint32_t* payload, uint64_t nnz,
+                        uint32_t n_rows, uint32_t n_cols, int32_t* row_ptr, int32_t* col_out,
+                        uint32_t* payload_out, unsigned* d_err, cudaStream_t s);
+
+cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s);
+void spmv_plan_free(SpmvPlan& p);
+cudaError_t spmv_launch(const CsrMat& A, const float* x, float* y, cudaStream_t s);
+cudaError_t spmv_dot_launch(const CsrMat& A, const float* x, const float* w, float* y,
+                            double* d_dot, double* partials, unsigned* counter,
+                            cudaStream_t s);
+
+}  // namespace mps

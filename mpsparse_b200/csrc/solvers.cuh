@@ -1,0 +1,604 @@
+// solvers.cuh -- Krylov solvers with every iteration on the device.
+//
+// The reference drives CG / BiCGSTAB / Richardson from the host with 3-6
+// kernel dispatches per iteration, relaxed float atomics for the dots and a
+// host round-trip every 50 iterations (iterative/BiCGSTAB/spmv.cpp:528-888,
+// iterative/richardson/spmv.cpp:376-425).  Here:
+//   * each dot product is fused into the kernel that produces its operand
+//     (SpMV epilogue or axpy) and reduced deterministically in FP64: per-CTA
+//     partials, then the last CTA sums them in a fixed order and updates the
+//     FP64 scalars (alpha, beta, omega, rho) in device memory;
+//   * stop rules run on the device: the last CTA of the last kernel of an
+//     iteration writes the CUDA-graph WHILE condition, so a whole solve is one
+//     graph launch with no host synchronisation until the end;
+//   * every kernel of an iteration returns immediately once the stop flag is
+//     set, so a solve never overshoots its result.
+#pragma once
+#include "spmv_kernels.cuh"
+
+namespace mps {
+
+struct Ctx {
+    DevScalars* sc;
+    double* part;          // 4 * kMaxPartials doubles
+    unsigned* ctr;         // 16 counters
+    cudaGraphConditionalHandle h;
+    int use_cond;
+};
+
+__device__ __forceinline__ void set_cond(const Ctx& c, bool run) {
+    if (c.use_cond) cudaGraphSetConditional(c.h, run ? 1u : 0u);
+}
+
+// Two-sum block reduction + last-CTA election, shared by the vector kernels.
+template <int NS>
+__device__ __forceinline__ bool reduce_partials(const Ctx& c, int slot, const double* acc,
+                                                double* tot) {
+    __shared__ double red[kNT / 32];
+    __shared__ int last_flag;
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+        const double v = block_sum<kNT>(acc[i], red);
+        if (threadIdx.x == 0) c.part[i * kMaxPartials + blockIdx.x] = v;
+    }
+    if (!arrive_last(c.ctr + slot, &last_flag)) return false;
+#pragma unroll
+    for (int i = 0; i < NS; ++i) tot[i] = sum_partials<kNT>(c.part + i * kMaxPartials, gridDim.x, red);
+    return true;
+}
+
+__device__ __forceinline__ double dot4(float4 a, float4 b) {
+    return (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z + (double)a.w * b.w;
+}
+__device__ __forceinline__ double dot4w(float4 a, float4 w) {   // sum a^2 * w
+    return (double)a.x * a.x * w.x + (double)a.y * a.y * w.y + (double)a.z * a.z * w.z +
+           (double)a.w * a.w * w.w;
+}
+__device__ __forceinline__ float4 axpy4(float a, float4 x, float4 y) {   // y + a x
+    return make_float4(fmaf(a, x.x, y.x), fmaf(a, x.y, y.y), fmaf(a, x.z, y.z), fmaf(a, x.w, y.w));
+}
+__device__ __forceinline__ float4 mul4(float4 a, float4 b) {
+    return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w);
+}
+
+// Watchdog of a device-side loop, run by one thread of the last kernel of each
+// loop body: stops the loop (and flags a timeout) once it has executed more
+// bodies than the iteration cap allows, whatever happened to the reductions.
+__device__ __forceinline__ void loop_watchdog(DevScalars* s) {
+    if (++s->guard > s->guard_limit) {
+        s->done = 1;
+        s->err |= kErrTimeout;
+    }
+}
+
+#define MPS_GRID_STRIDE(i, n) \
+    for (int i = blockIdx.x * kNT + threadIdx.x; i < (n); i += gridDim.x * kNT)
+
+// ============================ CG / PCG =====================================
+// Counter slots: 0 init, 1 pq, 2 xr, 3 G-apply, 4..7 BiCGSTAB, 8 Richardson.
+
+// x = 0, r = b, p = M b; rr = b.b, rz = b.Mb; stop flags reset.
+static __global__ void __launch_bounds__(kNT)
+cg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restrict__ r,
+        float4* __restrict__ p, const float4* __restrict__ dinv, int n4, int n,
+        const SolveParams* __restrict__ prm, Ctx c) {
+    const int mode = prm->precond;
+    double acc[2] = {0.0, 0.0};
+    MPS_GRID_STRIDE(i, n4) {
+        const float4 bv = b[i];
+        x[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        r[i] = bv;
+        float4 z = bv;
+        if (mode == 1) {
+            const float4 d = dinv[i];
+            z = mul4(bv, d);
+            acc[1] += dot4w(bv, d);
+        }
+        if (mode != 2) p[i] = z;
+        acc[0] += dot4(bv, bv);
+    }
+    double tot[2];
+    if (!reduce_partials<2>(c, 0, acc, tot)) return;
+    if (threadIdx.x != 0) return;
+    DevScalars* s = c.sc;
+    const double bb = tot[0];
+    s->n = n;
+    s->compat = prm->compat;
+    s->max_iter = prm->compat ? (n < 1000 ? n : 1000) : prm->max_iter;
+    s->iter = 0;
+    s->done = 0;
+    s->converged = 0;
+    s->breakdown = 0;
+    s->stalled = 0;
+    s->snapshot = 0;
+    s->err = 0;
+    s->mode = prm->compat ? 0 : mode;
+    s->stall_window = prm->stall_window;
+    s->restart = 1;
+    s->bnorm2 = bb;
+    s->rr = bb;
+    s->rz = (mode == 1) ? tot[1] : bb;
+    s->tol2 = prm->tol * prm->tol * bb;
+    s->best_rr = bb;
+    s->best_iter = 0;
+    s->beta = 0.0;
+    s->guard = 0;
+    s->guard_limit = s->max_iter + 8;
+    if (!isfinite(bb)) {
+        s->err = kErrNotFinite;
+        s->done = 1;
+    } else if (!prm->compat && bb == 0.0) {
+        s->done = 1;
+        s->converged = 1;
+    } else if (s->max_iter <= 0) {
+        s->done = 1;
+    }
+    set_cond(c, !s->done);
+}
+
+// q = A p ; pq = p.q ; alpha = rz / pq
+struct EpiCgPq {
+    static constexpr int NS = 1;
+    float* q;
+    const float* p;
+    DevScalars* sc;
+    unsigned* counter;
+    double* partials;
+    __device__ bool active() const { return !sc->done; }
+    __device__ void tick() const {}
+    __device__ void on_skip() const {}
+    __device__ void row(int r, float s, double* acc) const {
+        q[r] = s;
+        acc[0] += (double)p[r] * (double)s;
+    }
+    __device__ void finalize(const double* tot) const {
+        const double pq = tot[0];
+        sc->pq = pq;
+        double alpha;
+        if (sc->compat) {                                    // cgd.metal:38-42
+            alpha = fabs(pq) > 1e-9 ? sc->rz / pq : 0.0;
+        } else if (!(pq > 0.0) || !isfinite(pq)) {
+            sc->breakdown = 1;
+            sc->done = 1;
+            alpha = 0.0;
+        } else {
+            alpha = sc->rz / pq;
+        }
+        sc->alpha = alpha;
+    }
+};
+
+static __device__ void cg_finalize_xr(DevScalars* s, double rr_new, double rz_jac) {
+    const int it = ++s->iter;
+    const double rr_old = s->rr;
+    s->rr = rr_new;
+    if (s->compat) {
+        // spmv.cpp:603-627: every 50 iterations, on the value before this update
+        if ((it - 1) % 50 == 0 && rr_old < 1e-5) {
+            s->done = 1;
+            s->converged = 1;
+        } else if (it >= s->max_iter) {
+            s->done = 1;
+        }
+        s->beta = rr_new / rr_old;                           // cgd.metal:81, unguarded
+        s->rz = rr_new;
+        return;
+    }
+    if (!isfinite(rr_new)) {
+        s->breakdown = 1;
+        s->done = 1;
+        return;
+    }
+    if (rr_new <= s->tol2) {
+        s->converged = 1;
+        s->done = 1;
+        return;
+    }
+    if (it >= s->max_iter) {
+        s->done = 1;
+        return;
+    }
+    if (s->mode == 2) {   // stall watch of the learned preconditioner
+        if (rr_new < 0.25 * s->best_rr) {
+            s->best_rr = rr_new;
+            s->best_iter = it;
+        } else if (it - s->best_iter >= s->stall_window) {
+            s->mode = 1;          // fall back to Jacobi and restart the direction
+            s->stalled = 1;
+            s->restart = 1;
+            s->best_iter = it;
+            s->best_rr = rr_new;
+        }
+    }
+    if (s->mode == 1) {
+        s->beta = s->restart ? 0.0 : rz_jac / s->rz;
+        s->rz = rz_jac;
+        s->restart = 0;
+    } else if (s->mode == 0) {
+        s->beta = rr_new / s->rz;
+        s->rz = rr_new;
+    }
+}
+
+// x += alpha p ; r -= alpha q ; rr = r.r (and r.D^-1 r when a diagonal exists)
+static __global__ void __launch_bounds__(kNT)
+cg_update_xr(float4* __restrict__ x, float4* __restrict__ r, const float4* __restrict__ p,
+             const float4* __restrict__ q, const float4* __restrict__ dinv, int n4, Ctx c) {
+    if (c.sc->done) return;
+    const float a = (float)c.sc->alpha;
+    double acc[2] = {0.0, 0.0};
+    MPS_GRID_STRIDE(i, n4) {
+        const float4 pv = p[i], qv = q[i];
+        x[i] = axpy4(a, pv, x[i]);
+        const float4 rv = axpy4(-a, qv, r[i]);
+        r[i] = rv;
+        acc[0] += dot4(rv, rv);
+        if (dinv) acc[1] += dot4w(rv, dinv[i]);
+    }
+    double tot[2];
+    if (!reduce_partials<2>(c, 2, acc, tot)) return;
+    if (threadIdx.x == 0) cg_finalize_xr(c.sc, tot[0], tot[1]);
+}
+
+// p = z + beta p with z = r (no preconditioner) or D^-1 r (Jacobi).  Last
+// kernel of a CG iteration: writes the WHILE condition.
+static __global__ void __launch_bounds__(kNT)
+cg_update_p(float4* __restrict__ p, const float4* __restrict__ r, const float4* __restrict__ dinv,
+            int n4, Ctx c) {
+    DevScalars* s = c.sc;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        loop_watchdog(s);
+        set_cond(c, !s->done);
+    }
+    if (s->done || s->mode == 2) return;
+    const float beta = (float)s->beta;
+    const bool jac = s->mode == 1;
+    MPS_GRID_STRIDE(i, n4) {
+        float4 z = r[i];
+        if (jac) z = mul4(z, dinv[i]);
+        p[i] = axpy4(beta, p[i], z);
+    }
+}
+
+// FSAI step 1: w = G r ; rz = w.w (= r.G^T G r) ; beta = rz / rz_old
+struct EpiFsai1 {
+    static constexpr int NS = 1;
+    float* w;
+    DevScalars* sc;
+    unsigned* counter;
+    double* partials;
+    __device__ bool active() const { return !sc->done && sc->mode == 2; }
+    __device__ void tick() const {}
+    __device__ void on_skip() const {}
+    __device__ void row(int r, float s, double* acc) const {
+        w[r] = s;
+        acc[0] += (double)s * (double)s;
+    }
+    __device__ void finalize(const double* tot) const {
+        const double rz = tot[0];
+        sc->beta = sc->restart ? 0.0 : rz / sc->rz;
+        sc->rz = rz;
+        sc->restart = 0;
+    }
+};
+
+// FSAI step 2: p = G^T w + beta p
+struct EpiFsai2 {
+    static constexpr int NS = 0;
+    float* p;
+    DevScalars* sc;
+    unsigned* counter = nullptr;
+    double* partials = nullptr;
+    __device__ bool active() const { return !sc->done && sc->mode == 2; }
+    __device__ void tick() const {}
+    __device__ void on_skip() const {}
+    __device__ void row(int r, float s, double*) const {
+        const float beta = (float)__ldcg(&sc->beta);
+        p[r] = fmaf(beta, p[r], s);
+    }
+    __device__ void finalize(const double*) const {}
+};
+
+// ============================ BiCGSTAB =====================================
+
+static __global__ void __launch_bounds__(kNT)
+bicg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restrict__ r,
+          float4* __restrict__ r0, float4* __restrict__ p, float4* __restrict__ v, int n4, int n,
+          const SolveParams* __restrict__ prm, Ctx c) {
+    double acc[1] = {0.0};
+    MPS_GRID_STRIDE(i, n4) {
+        const float4 bv = b[i];
+        x[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        r[i] = bv;
+        r0[i] = bv;
+        p[i] = bv;
+        acc[0] += dot4(bv, bv);
+    }
+    double tot[1];
+    if (!reduce_partials<1>(c, 4, acc, tot)) return;
+    if (threadIdx.x != 0) return;
+    DevScalars* s = c.sc;
+    const double bb = tot[0];
+    s->n = n;
+    s->compat = prm->compat;
+    s->max_iter = prm->compat ? (n < 5000 ? n : 5000) : prm->max_iter;
+    s->iter = 0;
+    s->done = 0;
+    s->converged = 0;
+    s->breakdown = 0;
+    s->stalled = 0;
+    s->snapshot = 0;
+    s->err = 0;
+    s->bnorm2 = bb;
+    s->tol2 = prm->tol * prm->tol * bb;
+    // spmv.cpp:724,744-752: slots start at 1 and r.r is added on top (rho0 = 1 + b.b)
+    s->rho = (prm->compat ? 1.0 : 0.0) + bb;
+    s->rho_old = 1.0;
+    s->alpha = 1.0;
+    s->omega = 1.0;
+    s->rnorm2 = bb;
+    s->staged = 1e9;                                         // spmv.cpp:712
+    s->beta = 0.0;
+    s->guard = 0;
+    s->guard_limit = s->max_iter + 8;
+    if (!isfinite(bb)) {
+        s->err = kErrNotFinite;
+        s->done = 1;
+    } else if (!prm->compat && bb == 0.0) {
+        s->done = 1;
+        s->converged = 1;
+    } else if (s->max_iter <= 0) {
+        s->done = 1;
+    }
+    set_cond(c, !s->done);
+}
+
+// upp (bicgstab.metal:12-68): p = r on the first iteration, else
+// p = r + beta (p - omega v) with beta prepared by the previous iteration.
+static __global__ void __launch_bounds__(kNT)
+bicg_update_p(float4* __restrict__ p, const float4* __restrict__ r, const float4* __restrict__ v,
+              int n4, Ctx c) {
+    DevScalars* s = c.sc;
+    if (s->done) return;
+    if (s->iter == 0) {
+        MPS_GRID_STRIDE(i, n4) p[i] = r[i];
+        return;
+    }
+    const float beta = (float)s->beta, omega = (float)s->omega;
+    MPS_GRID_STRIDE(i, n4) {
+        const float4 pv = p[i], vv = v[i], rv = r[i];
+        const float4 t = axpy4(-omega, vv, pv);
+        p[i] = axpy4(beta, t, rv);
+    }
+}
+
+// v = A p ; sigma = r0.v ; alpha = rho / sigma (fused_spvmv + f_upalpha_ups)
+struct EpiBicgV {
+    static constexpr int NS = 1;
+    float* v;
+    const float* r0;
+    DevScalars* sc;
+    unsigned* counter;
+    double* partials;
+    __device__ bool active() const { return !sc->done; }
+    __device__ void tick() const {}
+    __device__ void on_skip() const {}
+    __device__ void row(int r, float s, double* acc) const {
+        v[r] = s;
+        acc[0] += (double)r0[r] * (double)s;
+    }
+    __device__ void finalize(const double* tot) const {
+        const double sigma = tot[0];
+        sc->sigma = sigma;
+        if (!sc->compat && (sigma == 0.0 || !isfinite(sigma))) {
+            sc->breakdown = 1;
+            sc->done = 1;
+            sc->alpha = 0.0;
+            return;
+        }
+        sc->alpha = sc->rho / sigma;                         // bicgstab.metal:87, unguarded
+    }
+};
+
+// s = r - alpha v
+static __global__ void __launch_bounds__(kNT)
+bicg_update_s(float4* __restrict__ s_, const float4* __restrict__ r, const float4* __restrict__ v,
+              int n4, Ctx c) {
+    if (c.sc->done) return;
+    const float a = (float)c.sc->alpha;
+    MPS_GRID_STRIDE(i, n4) s_[i] = axpy4(-a, v[i], r[i]);
+}
+
+// t = A s ; phi1 = t.s ; phi2 = t.t ; omega (spmv_op + f_dip)
+struct EpiBicgT {
+    static constexpr int NS = 2;
+    float* t;
+    const float* s_;
+    DevScalars* sc;
+    unsigned* counter;
+    double* partials;
+    __device__ bool active() const { return !sc->done; }
+    __device__ void tick() const {}
+    __device__ void on_skip() const {}
+    __device__ void row(int r, float s, double* acc) const {
+        t[r] = s;
+        acc[0] += (double)s * (double)s_[r];
+        acc[1] += (double)s * (double)s;
+    }
+    __device__ void finalize(const double* tot) const {
+        sc->phi1 = tot[0];
+        sc->phi2 = tot[1];
+        sc->omega = fabs(tot[1]) < 1e-20 ? 0.0 : tot[0] / tot[1];   // bicgstab.metal:264-269
+    }
+};
+
+// x += alpha p + omega s ; r = s - omega t ; rho = r0.r ; ||r||^2
+// (f_upomega_upxr_laa, bicgstab.metal:245-326).  Last kernel of an iteration.
+static __global__ void __launch_bounds__(kNT)
+bicg_update_xr(float4* __restrict__ x, float4* __restrict__ r, const float4* __restrict__ p,
+               const float4* __restrict__ r0, const float4* __restrict__ s_,
+               const float4* __restrict__ t, float4* __restrict__ xsnap, int n4, Ctx c) {
+    DevScalars* s = c.sc;
+    if (blockIdx.x == 0 && threadIdx.x == 0) loop_watchdog(s);
+    if (s->done) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(c, false);
+        return;
+    }
+    const int it = s->iter;   // 0-based index of this iteration
+    // Reference-compat delayed stop (spmv.cpp:835-859): at a check index
+    // other than 0, a staged ||r||^2 below 1e-5 returns the checkpoint.
+    const bool check = s->compat && (it % 50 == 0);
+    const bool stop_now = check && it > 0 && s->staged < 1e-5;
+    const bool snap = check && !stop_now;
+    const float a = (float)s->alpha, w = (float)s->omega;
+    double acc[2] = {0.0, 0.0};
+    if (!stop_now) {
+        MPS_GRID_STRIDE(i, n4) {
+            const float4 sv = s_[i], tv = t[i];
+            float4 xv = axpy4(a, p[i], x[i]);
+            xv = axpy4(w, sv, xv);
+            x[i] = xv;
+            if (snap) xsnap[i] = xv;
+            const float4 rv = axpy4(-w, tv, sv);
+            r[i] = rv;
+            acc[0] += dot4(r0[i], rv);
+            acc[1] += dot4(rv, rv);
+        }
+    }
+    double tot[2];
+    if (!reduce_partials<2>(c, 7, acc, tot)) return;
+    if (threadIdx.x != 0) return;
+    if (stop_now) {
+        s->done = 1;
+        s->converged = 1;
+        s->snapshot = 1;
+        s->rnorm2 = s->staged;
+        s->iter = it - 50 + 1;
+        set_cond(c, false);
+        return;
+    }
+    s->iter = it + 1;
+    s->rho_old = s->rho;
+    s->rho = tot[0];
+    s->rnorm2 = tot[1];
+    if (s->compat) {
+        double beta = 0.0;                                   // bicgstab.metal:46-56
+        if (fabs(s->rho_old) > 1e-15 && fabs(s->omega) > 1e-15) {
+            beta = (s->rho / s->rho_old) * (s->alpha / s->omega);
+            if (isinf(beta) || isnan(beta)) beta = 0.0;
+        }
+        s->beta = beta;
+        if (check) s->staged = tot[1];
+        if (s->iter >= s->max_iter) s->done = 1;
+    } else {
+        if (!isfinite(tot[1])) {
+            s->breakdown = 1;
+            s->done = 1;
+        } else if (tot[1] <= s->tol2) {
+            s->converged = 1;
+            s->done = 1;
+        } else if (s->omega == 0.0 || s->rho == 0.0) {
+            s->breakdown = 1;
+            s->done = 1;
+        } else if (s->iter >= s->max_iter) {
+            s->done = 1;
+        }
+        s->beta = (s->rho / s->rho_old) * (s->alpha / s->omega);
+    }
+    set_cond(c, !s->done);
+}
+
+// ============================ Richardson ===================================
+
+static __global__ void __launch_bounds__(kNT)
+rich_init(const float4* __restrict__ b, float4* __restrict__ x0, int n4, int n,
+          const SolveParams* __restrict__ prm, Ctx c) {
+    double acc[1] = {0.0};
+    MPS_GRID_STRIDE(i, n4) {
+        const float4 bv = b[i];
+        x0[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        acc[0] += dot4(bv, bv);
+    }
+    double tot[1];
+    if (!reduce_partials<1>(c, 8, acc, tot)) return;
+    if (threadIdx.x != 0) return;
+    DevScalars* s = c.sc;
+    s->n = n;
+    s->compat = prm->compat;
+    s->max_iter = prm->compat ? 1000 : prm->max_iter;        // richardson/spmv.cpp:402
+    s->omega_rich = prm->compat ? 0.01 : prm->omega;
+    s->iter = 0;
+    s->done = 0;
+    s->converged = 0;
+    s->breakdown = 0;
+    s->snapshot = 0;
+    s->err = 0;
+    s->bnorm2 = tot[0];
+    s->rnorm2 = tot[0];
+    s->tol2 = prm->compat ? 0.0 : prm->tol * prm->tol * tot[0];
+    s->guard = 0;
+    s->guard_limit = s->max_iter / 2 + 8;
+    if (!isfinite(tot[0])) {
+        s->err = kErrNotFinite;
+        s->done = 1;
+    } else if (s->max_iter <= 0) {
+        s->done = 1;
+    }
+    set_cond(c, !s->done);
+}
+
+// x_out = x_in + (w b + (-w) A x_in)  (iterative_step's spmv_op + two
+// weighted_add, fused); ||b - A x_in||^2 for the optional stop test.
+struct EpiRich {
+    static constexpr int NS = 1;
+    const float* xin;
+    float* xout;
+    const float* b;
+    DevScalars* sc;
+    unsigned* counter;
+    double* partials;
+    Ctx ctx;
+    int last_in_body;
+    __device__ void tick() const {
+        if (last_in_body) loop_watchdog(sc);
+    }
+    __device__ bool active() const { return !sc->done; }
+    __device__ void on_skip() const {
+        if (last_in_body) set_cond(ctx, false);
+    }
+    __device__ void row(int r, float s, double* acc) const {
+        const float w = (float)__ldcg(&sc->omega_rich);
+        const float bv = b[r];
+        const float s2 = w * bv + (-w) * s;
+        xout[r] = xin[r] + s2;
+        const double res = (double)bv - (double)s;
+        acc[0] += res * res;
+    }
+    __device__ void finalize(const double* tot) const {
+        const int it = ++sc->iter;
+        sc->rnorm2 = tot[0];
+        if (sc->tol2 > 0.0 && tot[0] <= sc->tol2) {
+            sc->converged = 1;
+            sc->done = 1;
+        }
+        if (it >= sc->max_iter) sc->done = 1;
+        if (last_in_body) set_cond(ctx, !sc->done);
+    }
+};
+
+// Result selection without a host round-trip.
+enum { kResX = 0, kResRich = 1 };
+static __global__ void copy_result(const float* __restrict__ x0, const float* __restrict__ x1,
+                            const float* __restrict__ xsnap, float* __restrict__ out, int n,
+                            int kind, const DevScalars* __restrict__ sc) {
+    const float* src = x0;
+    if (kind == kResRich)
+        src = (sc->iter & 1) ? x1 : x0;
+    else if (sc->snapshot)
+        src = xsnap;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = src[i];
+}
+
+}  // namespace mps

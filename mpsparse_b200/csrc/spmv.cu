@@ -1,0 +1,146 @@
+// spmv.cu -- SpMV tile plans, plain SpMV launches and CSR utilities.
+#include "spmv_kernels.cuh"
+
+namespace mps {
+namespace {
+
+// tile_row[t] = first row whose row_ptr is >= t * T (binary search), with
+// tile_row[0] = 0 and tile_row[ntiles] = n_rows.  Rows whose nonzeros start in
+// the window [tT, (t+1)T) form tile t.
+__global__ void plan_tiles_kernel(const int* __restrict__ rp, int n_rows, int T, int ntiles,
+                                  int* __restrict__ tile_row) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > ntiles) return;
+    if (t == 0) {
+        tile_row[0] = 0;
+        return;
+    }
+    if (t == ntiles) {
+        tile_row[t] = n_rows;
+        return;
+    }
+    const long long target = (long long)t * T;
+    int lo = 0, hi = n_rows;
+    while (lo < hi) {
+        const int mid = lo + ((hi - lo) >> 1);
+        if (rp[mid] < target)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    tile_row[t] = lo;
+}
+
+__global__ void diag_inv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
+                                const float* __restrict__ v, int n, float* __restrict__ dinv) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        float d = 0.f;
+        for (int k = rp[r]; k < rp[r + 1]; ++k)
+            if (ci[k] == r) d += v[k];
+        dinv[r] = d != 0.f ? 1.0f / d : 1.0f;
+    }
+}
+
+// (col << 32 | row) keys of every nonzero: sorting them yields the transpose.
+__global__ void transpose_keys_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
+                                      int n_rows, unsigned long long* __restrict__ keys) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += gridDim.x * blockDim.x)
+        for (int k = rp[r]; k < rp[r + 1]; ++k)
+            keys[k] = ((unsigned long long)(unsigned)ci[k] << 32) | (unsigned)r;
+}
+
+__global__ void f32_to_bf16_kernel(const float* __restrict__ v, __nv_bfloat16* __restrict__ o,
+                                   uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        o[i] = __float2bfloat16_rn(v[i]);
+}
+
+int grid_for(uint64_t n, int nt) {
+    uint64_t g = (n + nt - 1) / nt;
+    const uint64_t cap = (uint64_t)num_sms() * 8;
+    if (g > cap) g = cap;
+    return g ? (int)g : 1;
+}
+
+}  // namespace
+
+int default_tile_nnz(uint64_t nnz, uint32_t n_rows) {
+    const double avg = n_rows ? (double)nnz / n_rows : 1.0;
+    int t = (int)(kNT * (avg < 1.0 ? 1.0 : avg + 0.999));
+    t = (t + 3) & ~3;
+    if (t < 512) t = 512;
+    if (t > 4096) t = 4096;
+    return t;
+}
+
+void spmv_plan_free(SpmvPlan& p) {
+    if (p.d_tile_row) cudaFree(p.d_tile_row);
+    p = SpmvPlan{};
+}
+
+cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s) {
+    if (tile_nnz <= 0) tile_nnz = default_tile_nnz(A.nnz, A.n_rows);
+    tile_nnz = (tile_nnz + 3) & ~3;
+    const uint64_t nt = A.nnz ? (A.nnz + tile_nnz - 1) / tile_nnz : 1;
+    SpmvPlan p;
+    p.tile_nnz = tile_nnz;
+    p.ntiles = (int)nt;
+    p.cap = 2 * tile_nnz + 64;
+    const int cap_grid = num_sms() * 8;
+    p.grid = p.ntiles < cap_grid ? p.ntiles : cap_grid;
+    if (p.grid < 1) p.grid = 1;
+    cudaError_t e = cudaMalloc(&p.d_tile_row, (size_t)(p.ntiles + 1) * sizeof(int));
+    if (e != cudaSuccess) return e;
+    plan_tiles_kernel<<<(p.ntiles + 1 + 255) / 256, 256, 0, s>>>(A.rp, (int)A.n_rows, tile_nnz,
+                                                                 p.ntiles, p.d_tile_row);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cudaFree(p.d_tile_row);
+        return e;
+    }
+    spmv_plan_free(A.plan);
+    A.plan = p;
+    return cudaSuccess;
+}
+
+template <class K>
+static void smem_optin(K kernel, size_t smem) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+cudaError_t spmv_launch(const CsrMat& A, const float* x, float* y, cudaStream_t s) {
+    const CsrDev v = A.view();
+    const size_t smem = spmv_smem_bytes<float>(v);
+    EpiStore e{y};
+    smem_optin(spmv_tiles<float, float, false, EpiStore>, smem);
+    spmv_tiles<float, float, false, EpiStore><<<A.plan.grid, kNT, smem, s>>>(v, x, e);
+    return cudaGetLastError();
+}
+
+cudaError_t spmv_dot_launch(const CsrMat& A, const float* x, const float* w, float* y,
+                            double* d_dot, double* partials, unsigned* counter, cudaStream_t s) {
+    const CsrDev v = A.view();
+    const size_t smem = spmv_smem_bytes<float>(v);
+    EpiStoreDot e{y, w, d_dot, counter, partials};
+    smem_optin(spmv_tiles<float, float, false, EpiStoreDot>, smem);
+    spmv_tiles<float, float, false, EpiStoreDot><<<A.plan.grid, kNT, smem, s>>>(v, x, e);
+    return cudaGetLastError();
+}
+
+cudaError_t diag_inv_launch(const CsrMat& A, float* dinv, cudaStream_t s) {
+    diag_inv_kernel<<<grid_for(A.n_rows, 256), 256, 0, s>>>(A.rp, A.ci, A.v, (int)A.n_rows, dinv);
+    return cudaGetLastError();
+}
+
+cudaError_t transpose_keys_launch(const CsrMat& A, unsigned long long* keys, cudaStream_t s) {
+    transpose_keys_kernel<<<grid_for(A.n_rows, 256), 256, 0, s>>>(A.rp, A.ci, (int)A.n_rows, keys);
+    return cudaGetLastError();
+}
+
+cudaError_t to_bf16_launch(const float* v, __nv_bfloat16* o, uint64_t n, cudaStream_t s) {
+    f32_to_bf16_kernel<<<grid_for(n, 256), 256, 0, s>>>(v, o, n);
+    return cudaGetLastError();
+}
+
+}  // namespace mps

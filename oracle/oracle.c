@@ -1,0 +1,391 @@
+/*
+ * oracle.c -- CPU restatement of SparseForge/mpsparse's solver path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker the CUDA path is compared
+ * against (tests/, __graft_entry__.smoke(), bench.py's CPU-baseline leg).  The
+ * product path never links or loads it.
+ *
+ * Every function restates the reference algorithm from its source; the
+ * reference file:line each one follows is given beside it.  Arithmetic is
+ * FP64 throughout (the "FP64 host transcription"); matrix values are the FP32
+ * values the caller stored.  The sort is bit-exact integer work.
+ */
+#include "oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* COO -> CSR                                                                */
+/* ------------------------------------------------------------------------ */
+
+static int bit_width_u32(uint32_t v) { return v ? 32 - __builtin_clz(v) : 0; }
+
+/* iterative/BiCGSTAB/spmv.cpp:62-228.  The reference masks the 64-bit key to
+ * bits(n_cols) column bits and bits(n_rows) row bits (spmv.cpp:73-77) and
+ * runs one stable counting-sort pass per 4-bit digit that overlaps the mask
+ * (spmv.cpp:110-170; radix_frequencies/vertical_scan/scan_histogram/reorder,
+ * coo_csr.metal:17-142).  It then writes col_ind = low word, row starts where
+ * the row changes, row_ptr[n] = nnz (coo_to_csr_compress, coo_csr.metal:144-178)
+ * and fills empty rows backward (row_fixer, coo_csr.metal:180-193).
+ * Keys outside [0,n_rows) x [0,n_cols) are undefined in the reference; here
+ * they are rejected (-1).  nnz == 0 yields an all-zero row_ptr. */
+int orc_coo_to_csr(const uint64_t* keys, const float* vals, uint64_t nnz,
+                   uint32_t n_rows, uint32_t n_cols,
+                   int32_t* row_ptr, int32_t* col_ind, float* out_vals) {
+    for (uint64_t i = 0; i < nnz; ++i) {
+        uint64_t r = keys[i] >> 32, c = keys[i] & 0xFFFFFFFFull;
+        if (r >= n_rows || c >= n_cols) return -1;
+    }
+    if (nnz == 0) {
+        for (uint64_t i = 0; i <= n_rows; ++i) row_ptr[i] = 0;
+        return 0;
+    }
+    uint64_t mask = ((1ull << bit_width_u32(n_cols)) - 1) |
+                    (((1ull << bit_width_u32(n_rows)) - 1) << 32);
+    uint64_t* ka = (uint64_t*)malloc(nnz * sizeof(uint64_t));
+    uint64_t* kb = (uint64_t*)malloc(nnz * sizeof(uint64_t));
+    float* va = (float*)malloc(nnz * sizeof(float));
+    float* vb = (float*)malloc(nnz * sizeof(float));
+    if (!ka || !kb || !va || !vb) { free(ka); free(kb); free(va); free(vb); return -2; }
+    memcpy(ka, keys, nnz * sizeof(uint64_t));
+    memcpy(va, vals, nnz * sizeof(float));
+    for (int shift = 0; shift < 64; shift += 4) {
+        if (((0xFull << shift) & mask) == 0) continue;      /* spmv.cpp:117-122 */
+        uint64_t cnt[16] = {0}, off[16];
+        for (uint64_t i = 0; i < nnz; ++i) cnt[(ka[i] >> shift) & 0xF]++;
+        uint64_t run = 0;
+        for (int d = 0; d < 16; ++d) { off[d] = run; run += cnt[d]; }
+        for (uint64_t i = 0; i < nnz; ++i) {                /* stable scatter */
+            unsigned d = (unsigned)((ka[i] >> shift) & 0xF);
+            kb[off[d]] = ka[i];
+            vb[off[d]] = va[i];
+            off[d]++;
+        }
+        uint64_t* tk = ka; ka = kb; kb = tk;
+        float* tv = va; va = vb; vb = tv;
+    }
+    /* coo_to_csr_compress (coo_csr.metal:144-178) after the 0xFF fill
+     * (spmv.cpp:187-191). */
+    for (uint64_t i = 0; i <= n_rows; ++i) row_ptr[i] = (int32_t)0xFFFFFFFF;
+    for (uint64_t g = 0; g < nnz; ++g) {
+        uint32_t row = (uint32_t)(ka[g] >> 32);
+        col_ind[g] = (int32_t)(uint32_t)(ka[g] & 0xFFFFFFFFull);
+        if (g == 0) {
+            row_ptr[0] = 0;
+            row_ptr[row] = 0;
+        } else if (row != (uint32_t)(ka[g - 1] >> 32)) {
+            row_ptr[row] = (int32_t)g;
+        }
+        if (g == nnz - 1) row_ptr[n_rows] = (int32_t)nnz;
+    }
+    /* row_fixer (coo_csr.metal:180-193). */
+    for (int64_t i = (int64_t)n_rows - 1; i >= 0; --i)
+        if ((uint32_t)row_ptr[i] == 0xFFFFFFFFu) row_ptr[i] = row_ptr[i + 1];
+    memcpy(out_vals, va, nnz * sizeof(float));
+    free(ka); free(kb); free(va); free(vb);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* SpMV                                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* spmv_op, iterative/BiCGSTAB/spmv.metal:11-49: one row, sum of val*x[col]. */
+void orc_csr_spmv(const int32_t* rp, const int32_t* ci, const float* v,
+                  int64_t n, const double* x, double* y, int threads) {
+    (void)threads;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(threads > 0 ? threads : 1)
+#endif
+    for (int64_t i = 0; i < n; ++i) {
+        double s = 0.0;
+        for (int32_t k = rp[i]; k < rp[i + 1]; ++k) s += (double)v[k] * x[ci[k]];
+        y[i] = s;
+    }
+}
+
+/* spmv_op, iterative/BiCGSTAB/bcsr_spmv.metal:30-69: block row br produces
+ * y[B*br + k] = sum over blocks of dot(block row k, x[B*bc .. B*bc+B-1]);
+ * blocks are row-major B x B (scipy bsr.data.flatten(), bcsr_benchmark.py:52). */
+void orc_bcsr_spmv(const int32_t* rp, const int32_t* ci, const float* v,
+                   int64_t nbr, int B, const double* x, double* y) {
+    for (int64_t br = 0; br < nbr; ++br) {
+        for (int k = 0; k < B; ++k) y[br * B + k] = 0.0;
+        for (int32_t j = rp[br]; j < rp[br + 1]; ++j) {
+            const float* blk = v + (int64_t)j * B * B;
+            const double* xs = x + (int64_t)ci[j] * B;
+            for (int k = 0; k < B; ++k) {
+                double s = 0.0;
+                for (int c = 0; c < B; ++c) s += (double)blk[k * B + c] * xs[c];
+                y[br * B + k] += s;
+            }
+        }
+    }
+}
+
+static void apply(const orc_op* A, const double* x, double* y, int threads) {
+    if (A->block == 0)
+        orc_csr_spmv(A->row_ptr, A->col_ind, A->val, A->n, x, y, threads);
+    else
+        orc_bcsr_spmv(A->row_ptr, A->col_ind, A->val, A->n / A->block, A->block, x, y);
+}
+
+/* Deterministic dot: fixed static chunks summed in chunk order. */
+static double dot(const double* a, const double* b, int64_t n, int threads) {
+    int t = threads > 0 ? threads : 1;
+    if (t == 1) {
+        double s = 0.0;
+        for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+        return s;
+    }
+    double part[256] = {0};
+    if (t > 256) t = 256;
+    int64_t chunk = (n + t - 1) / t;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static, 1) num_threads(t)
+#endif
+    for (int c = 0; c < t; ++c) {
+        int64_t lo = (int64_t)c * chunk, hi = lo + chunk < n ? lo + chunk : n;
+        double s = 0.0;
+        for (int64_t i = lo; i < hi; ++i) s += a[i] * b[i];
+        part[c] = s;
+    }
+    double s = 0.0;
+    for (int c = 0; c < t; ++c) s += part[c];
+    return s;
+}
+
+static void diag_of(const orc_op* A, double* d) {
+    for (int64_t i = 0; i < A->n; ++i) d[i] = 0.0;
+    if (A->block == 0) {
+        for (int64_t i = 0; i < A->n; ++i)
+            for (int32_t k = A->row_ptr[i]; k < A->row_ptr[i + 1]; ++k)
+                if (A->col_ind[k] == i) d[i] += A->val[k];
+    } else {
+        int B = A->block;
+        for (int64_t br = 0; br < A->n / B; ++br)
+            for (int32_t j = A->row_ptr[br]; j < A->row_ptr[br + 1]; ++j)
+                if (A->col_ind[j] == br)
+                    for (int k = 0; k < B; ++k) d[br * B + k] += A->val[(int64_t)j * B * B + k * B + k];
+    }
+}
+
+double orc_true_residual(const orc_op* A, const double* b, const double* x) {
+    double* ax = (double*)malloc(A->n * sizeof(double));
+    apply(A, x, ax, 1);
+    double rr = 0.0, bb = 0.0;
+    for (int64_t i = 0; i < A->n; ++i) {
+        double r = b[i] - ax[i];
+        rr += r * r;
+        bb += b[i] * b[i];
+    }
+    free(ax);
+    return bb > 0 ? sqrt(rr / bb) : sqrt(rr);
+}
+
+/* ------------------------------------------------------------------------ */
+/* CG                                                                        */
+/* ------------------------------------------------------------------------ */
+
+/* csr_tensor::cgd_op, iterative/BiCGSTAB/spmv.cpp:528-659, kernels
+ * update_xr / update_p (cgd.metal:11-82):
+ *   x = 0, r = p = b, rr = r.r                       (spmv.cpp:542-565)
+ *   loop i < min(1000, n)                             (spmv.cpp:572-573)
+ *     Ap = A p, pAp = p.Ap                            (fused_spvmv)
+ *     alpha = |pAp| > 1e-9 ? rr/pAp : 0               (cgd.metal:38-42)
+ *     x += alpha p, r -= alpha Ap, rr' = r.r          (cgd.metal:44-46)
+ *     p = r + (rr'/rr) p                              (cgd.metal:81)
+ *     every 50 iterations stop if rr (the value before this update) < 1e-5
+ *     (spmv.cpp:603-627; the curr/next swap happens after the check).
+ * compat = 0: x0 = 0, relative test ||r|| <= tol ||b|| after every update,
+ * optional Jacobi preconditioner (z = r / diag(A)). */
+int orc_cg(const orc_op* A, const double* b, double* x, const orc_opts* o, orc_info* info) {
+    int64_t n = A->n;
+    int th = o->threads;
+    double *r = malloc(n * 8), *p = malloc(n * 8), *q = malloc(n * 8), *z = malloc(n * 8),
+           *dinv = NULL;
+    if (o->precond == 1 && !o->compat) {
+        dinv = malloc(n * 8);
+        diag_of(A, dinv);
+        for (int64_t i = 0; i < n; ++i) dinv[i] = dinv[i] != 0.0 ? 1.0 / dinv[i] : 1.0;
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        x[i] = 0.0;
+        r[i] = b[i];
+        z[i] = dinv ? dinv[i] * b[i] : b[i];
+        p[i] = z[i];
+    }
+    double bnorm = sqrt(dot(b, b, n, th));
+    double rr = dot(r, r, n, th);
+    double rz = dinv ? dot(r, z, n, th) : rr;
+    int cap = o->compat ? (n < 1000 ? (int)n : 1000) : o->max_iter;
+    info->iters = 0;
+    info->converged = 0;
+    info->breakdown = 0;
+    if (!o->compat && bnorm == 0.0) {
+        info->converged = 1;
+        info->rel_resid = 0.0;
+        goto done;
+    }
+    for (int i = 0; i < cap; ++i) {
+        apply(A, p, q, th);
+        double pq = dot(p, q, n, th);
+        double alpha;
+        if (o->compat) {
+            alpha = fabs(pq) > 1e-9 ? rz / pq : 0.0;
+        } else {
+            if (!(pq > 0.0)) { info->breakdown = 1; break; }
+            alpha = rz / pq;
+        }
+        for (int64_t k = 0; k < n; ++k) {
+            x[k] += alpha * p[k];
+            r[k] -= alpha * q[k];
+        }
+        double rr_new = dot(r, r, n, th);
+        double rz_new = rr_new;
+        if (dinv) {
+            for (int64_t k = 0; k < n; ++k) z[k] = dinv[k] * r[k];
+            rz_new = dot(r, z, n, th);
+        }
+        double beta = rz_new / rz;
+        const double* zz = dinv ? z : r;
+        for (int64_t k = 0; k < n; ++k) p[k] = zz[k] + beta * p[k];
+        info->iters = i + 1;
+        if (o->compat) {
+            if (i % 50 == 0 && rr < 1e-5) { rr = rr_new; info->converged = 1; break; }
+        } else if (sqrt(rr_new) <= o->tol * bnorm) {
+            rr = rr_new;
+            info->converged = 1;
+            break;
+        }
+        rr = rr_new;
+        rz = rz_new;
+    }
+    info->rel_resid = bnorm > 0 ? sqrt(rr) / bnorm : sqrt(rr);
+done:
+    free(r); free(p); free(q); free(z); free(dinv);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* BiCGSTAB                                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* csr_tensor::bicgstab_op, iterative/BiCGSTAB/spmv.cpp:699-888, kernels upp,
+ * fused_spvmv, f_upalpha_ups, spmv_op, f_dip, f_upomega_upxr_laa
+ * (bicgstab.metal:12-326).  Scalar slots {rho_prev, rho_curr, alpha, omega,
+ * sigma, phi1, phi2, ||r||^2} start at {1,1,1,1,0,0,0,0} (spmv.cpp:724) and
+ * the first r.r is added on top of slot 1 (spmv.cpp:744-752), so compat mode
+ * starts from rho0 = 1 + b.b.  Guards: beta = 0 unless |rho_old| > 1e-15 and
+ * |omega| > 1e-15, and beta = 0 if it is inf/NaN (bicgstab.metal:46-56);
+ * omega = 0 if |phi2| < 1e-20 (bicgstab.metal:264-269).  The compat stop rule
+ * models the reference's delayed check (spmv.cpp:835-859) without its host
+ * race: the first check index j (a multiple of 50, j + 50 < cap) whose
+ * ||r_j||^2 < 1e-5 returns the iterate after iteration j; the cap is
+ * min(5000, n).  compat = 0 is the plain van der Vorst recurrence with
+ * rho0 = b.b and the relative test every iteration. */
+int orc_bicgstab(const orc_op* A, const double* b, double* x, const orc_opts* o, orc_info* info) {
+    int64_t n = A->n;
+    int th = o->threads;
+    double *r = malloc(n * 8), *r0 = malloc(n * 8), *p = malloc(n * 8), *v = malloc(n * 8),
+           *s = malloc(n * 8), *t = malloc(n * 8), *xs = NULL;
+    for (int64_t i = 0; i < n; ++i) {
+        x[i] = 0.0;
+        r[i] = r0[i] = p[i] = b[i];
+        v[i] = 0.0;
+    }
+    double bnorm = sqrt(dot(b, b, n, th));
+    double rho_old = 1.0, alpha = 1.0, omega = 1.0;
+    double rho = (o->compat ? 1.0 : 0.0) + dot(r, r, n, th);
+    double rnorm2 = rho - (o->compat ? 1.0 : 0.0);
+    int cap = o->compat ? (n < 5000 ? (int)n : 5000) : o->max_iter;
+    double staged = 1e9;          /* host copy of ||r||^2 from the last check */
+    if (o->compat) xs = malloc(n * 8);
+    info->iters = 0;
+    info->converged = 0;
+    info->breakdown = 0;
+    if (!o->compat && bnorm == 0.0) {
+        info->converged = 1;
+        info->rel_resid = 0.0;
+        goto done;
+    }
+    for (int i = 0; i < cap; ++i) {
+        if (i > 0) {                                          /* upp */
+            double beta = 0.0;
+            if (fabs(rho_old) > 1e-15 && fabs(omega) > 1e-15) {
+                beta = (rho / rho_old) * (alpha / omega);
+                if (isinf(beta) || isnan(beta)) beta = 0.0;
+            }
+            for (int64_t k = 0; k < n; ++k) p[k] = r[k] + beta * (p[k] - omega * v[k]);
+        } else {
+            for (int64_t k = 0; k < n; ++k) p[k] = r[k];
+        }
+        apply(A, p, v, th);                                   /* fused_spvmv */
+        double sigma = dot(r0, v, n, th);
+        if (!o->compat && sigma == 0.0) { info->breakdown = 1; break; }
+        alpha = rho / sigma;                                  /* f_upalpha_ups */
+        for (int64_t k = 0; k < n; ++k) s[k] = r[k] - alpha * v[k];
+        apply(A, s, t, th);                                   /* spmv_op */
+        double phi1 = dot(t, s, n, th), phi2 = dot(t, t, n, th);   /* f_dip */
+        omega = fabs(phi2) < 1e-20 ? 0.0 : phi1 / phi2;       /* f_upomega_upxr_laa */
+        for (int64_t k = 0; k < n; ++k) {
+            x[k] += alpha * p[k] + omega * s[k];
+            r[k] = s[k] - omega * t[k];
+        }
+        rho_old = rho;
+        rho = dot(r0, r, n, th);
+        rnorm2 = dot(r, r, n, th);
+        info->iters = i + 1;
+        if (o->compat) {
+            if (i % 50 == 0) {
+                if (i > 0 && staged < 1e-5) {
+                    /* the batch after the previous check is discarded */
+                    memcpy(x, xs, n * 8);
+                    info->iters = i - 50 + 1;
+                    info->converged = 1;
+                    rnorm2 = staged;
+                    break;
+                }
+                staged = rnorm2;
+                memcpy(xs, x, n * 8);
+            }
+        } else {
+            if (sqrt(rnorm2) <= o->tol * bnorm) { info->converged = 1; break; }
+            if (omega == 0.0 || rho == 0.0) { info->breakdown = 1; break; }
+        }
+    }
+    info->rel_resid = bnorm > 0 ? sqrt(rnorm2) / bnorm : sqrt(rnorm2);
+done:
+    free(r); free(r0); free(p); free(v); free(s); free(t); free(xs);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Richardson                                                                */
+/* ------------------------------------------------------------------------ */
+
+/* csr_tensor::iterative_op / iterative_step, iterative/richardson/spmv.cpp:
+ * 376-425 and 441-495: x = 0, then for a fixed count s1 = A x,
+ * s2 = w b + (-w) s1, x = x + s2 (weighted_add, richardson/spmv.metal:50-63).
+ * compat = 1 fixes w = 0.01 and 1000 iterations (spmv.cpp:402-404). */
+int orc_richardson(const orc_op* A, const double* b, double* x, const orc_opts* o, orc_info* info) {
+    int64_t n = A->n;
+    double w = o->compat ? 0.01 : o->omega;
+    int iters = o->compat ? 1000 : o->max_iter;
+    double* s1 = malloc(n * 8);
+    for (int64_t i = 0; i < n; ++i) x[i] = 0.0;
+    for (int it = 0; it < iters; ++it) {
+        apply(A, x, s1, o->threads);
+        for (int64_t i = 0; i < n; ++i) x[i] = x[i] + (w * b[i] + (-w) * s1[i]);
+    }
+    info->iters = iters;
+    info->converged = 0;
+    info->breakdown = 0;
+    info->rel_resid = orc_true_residual(A, b, x);
+    free(s1);
+    return 0;
+}
