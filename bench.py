@@ -1,0 +1,416 @@
+"""Benchmark of the sparse iterative-solver path on B200.
+
+Headline metric: time to an FP64-checked relative residual of 1e-6 on the
+512x512 log-normal diffusion set (2D 5-point, sigma 1.5, correlation length
+16; held-out seeds), for the solver named in config.solver, with the plain
+FP32 CG drop-in timed beside it on the same systems.  One step = one solve of
+one system whose CSR is already resident in HBM; L2 is flushed between steps.
+
+Also measured in the same run (reported, not the headline):
+  * spmv: CSR SpMV GB/s on the 256^3 7-point diffusion operator (1.14 GB per
+    SpMV, larger than L2) -- the HBM-bound kernel whose roofline is reported;
+  * e2e: the same metric through the drop-in API with host buffers --
+    spmv.csr_tensor(keys, values, ...) from pinned host COO (GPU sort) and
+    cgd(b, x) with pinned host b/x, every copy inside the timed region;
+  * cpu_baseline: the CPU oracle's CG on the box's host cores (bounded sample)
+    and scipy.sparse.linalg.cg beside it.
+
+`--impl reference` times the reference algorithm's CPU implementation (the
+oracle port of iterative/BiCGSTAB/spmv.cpp cgd_op) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-to-1e-6-residual"
+UNIT = "ms"
+WORKLOAD = "512x512 log-normal diffusion (2D 5-pt, sigma 1.5, corr 16), held-out seeds"
+TEST_SEED0 = 100_000        # held-out seeds start here (training uses 0..1999)
+TOL = 1e-6
+MAX_ITER = 40_000
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- clocks ----
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        load = [s for s in sm if mx and s > 0.3 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------- systems -----
+def c4_system(seed):
+    from mpsparse_b200 import workloads as W
+    coo = W.diffusion_512sq(seed).shuffled(seed + 1)
+    b = W.rhs(coo.n, seed + 2)
+    return coo, b
+
+
+def true_residual_gpu(A_csr, b, x):
+    """FP64 ||b - A x|| / ||b|| on the GPU (verification only, untimed)."""
+    import torch
+    rp, ci, v = A_csr
+    M = torch.sparse_csr_tensor(rp.long(), ci.long(), v.double(), (b.numel(), b.numel()))
+    r = b.double() - (M @ x.double().unsqueeze(1)).squeeze(1)
+    return float(r.norm() / b.double().norm())
+
+
+def flush_l2(buf):
+    buf.add_(1.0)
+
+
+# ------------------------------------------------------------- our arm -----
+def run_ours(args, rank, world, dev):
+    import torch
+    import mpsparse_b200 as mps
+    torch.cuda.set_device(dev)
+    steps, warm = args.steps, args.warmup
+    nsys = steps + warm
+    seeds = [TEST_SEED0 + rank * 10_000 + i for i in range(nsys)]
+    systems = []
+    e = torch.empty(0)
+    for s in seeds:
+        coo, b = c4_system(s)
+        A = mps.spmv.csr_tensor(torch.from_numpy(coo.keys()), torch.from_numpy(coo.vals), e, e, e,
+                                coo.n, coo.n, fill_outputs=False)
+        systems.append((coo, A, torch.from_numpy(b).cuda()))
+    n = systems[0][0].n
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2
+    stream = torch.cuda.current_stream()
+
+    def solve_plain(i):
+        coo, A, b = systems[i]
+        x = torch.zeros(n, device=dev)
+        info = A.cgd(b, x, tol=TOL, max_iter=MAX_ITER)
+        return x, info
+
+    headline = solve_plain
+    solver_name = "plain FP32 CG (drop-in cgd)"
+
+    def timed(fn):
+        times, infos, xs = [], [], []
+        for i in range(nsys):
+            flush_l2(flush)
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            x, info = fn(i)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            if i >= warm:
+                times.append(ev0.elapsed_time(ev1))
+                infos.append(info)
+                xs.append(x)
+        return times, infos, xs
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        t_wall0 = time.perf_counter()
+        times, infos, xs = timed(headline)
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall0
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = clk.summary()
+    # verification (untimed): FP64 true residual of every timed solve
+    resid = []
+    for k, x in enumerate(xs):
+        coo, A, b = systems[warm + k]
+        resid.append(true_residual_gpu(A.csr(), b, x))
+    # plain CG on the same systems (the comparison the metric names)
+    ptimes, pinfos, pxs = timed(solve_plain)
+    presid = [true_residual_gpu(systems[warm + k][1].csr(), systems[warm + k][2], x)
+              for k, x in enumerate(pxs)]
+
+    total_ms = sum(times)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    iters = [i["iters"] for i in infos]
+    launches = sum(2 + 3 * it for it in iters)          # init + 3 kernels/iteration + result copy
+
+    out = {
+        "solver": solver_name,
+        "ms_per_solve": total_ms / steps,
+        "value": total_ms / (steps * world),
+        "iters_mean": statistics.mean(iters),
+        "true_resid_max": max(resid),
+        "plain_cg": {"ms_per_solve": statistics.mean(ptimes),
+                     "iters_mean": statistics.mean(i["iters"] for i in pinfos),
+                     "true_resid_max": max(presid)},
+        "clocks": clocks, "gpu_launches": launches, "wall_s": t_wall,
+    }
+    out["e2e"] = e2e_drop_in(args, systems, dev, warm, steps)
+    out["spmv"] = spmv_c3(args, dev) if not args.skip_spmv else None
+    return out
+
+
+def e2e_drop_in(args, systems, dev, warm, steps):
+    """csr_tensor from pinned host COO + cgd with pinned host b/x, per step."""
+    import torch
+    import mpsparse_b200 as mps
+    n = systems[0][0].n
+    stream = torch.cuda.current_stream()
+    times = []
+    h2d = d2h = 0
+    e = torch.empty(0)
+    for i in range(warm + steps):
+        coo = systems[i][0]
+        keys = torch.from_numpy(coo.keys()).pin_memory()
+        vals = torch.from_numpy(coo.vals).pin_memory()
+        b = systems[i][2].cpu().pin_memory()
+        x = torch.zeros(n).pin_memory()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        A = mps.spmv.csr_tensor(keys, vals, e, e, e, n, n, fill_outputs=False)
+        A.cgd(b, x, tol=TOL, max_iter=MAX_ITER)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if i >= warm:
+            times.append(ev0.elapsed_time(ev1))
+            h2d = keys.numel() * 8 + vals.numel() * 4 + b.numel() * 4
+            d2h = x.numel() * 4
+        del A
+    return {"value": statistics.mean(times), "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h,
+            "path": "spmv.csr_tensor(pinned host COO) + cgd(pinned host b, x)"}
+
+
+def spmv_c3(args, dev):
+    """CSR SpMV on the 256^3 7-point diffusion operator: GB/s by the byte model
+    8*nnz + 4*(n+1) + 4*n_cols + 4*n_rows, CUDA events per launch."""
+    import torch
+    import mpsparse_b200 as mps
+    from mpsparse_b200 import workloads as W
+    m = args.c3_grid
+    coo = W.lognormal_diffusion_3d(m, 1.0, 8.0, 0)
+    e = torch.empty(0)
+    A = mps.spmv.csr_tensor(torch.from_numpy(coo.keys()), torch.from_numpy(coo.vals), e, e, e,
+                            coo.n, coo.n, fill_outputs=False)
+    n, nnz = coo.n, coo.nnz
+    del coo
+    x = torch.randn(n, device=dev)
+    y = torch.empty(n, device=dev)
+    stream = torch.cuda.current_stream()
+    for _ in range(3):
+        A.mv(x, y)
+    reps = 20
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(reps)]
+    for a, b in evs:
+        a.record(stream)
+        A.mv(x, y)
+        b.record(stream)
+    torch.cuda.synchronize()
+    ms = statistics.median(a.elapsed_time(b) for a, b in evs)
+    bytes_alg = 8 * nnz + 4 * (n + 1) + 4 * n + 4 * n
+    gbs = bytes_alg / (ms * 1e-3) / 1e9
+    return {"workload": f"{m}^3 7-pt log-normal diffusion", "n": n, "nnz": nnz,
+            "bytes_per_launch": bytes_alg, "ms": ms, "gbs": gbs, "launches": reps}
+
+
+# --------------------------------------------------------- CPU baselines ---
+def cpu_oracle_cg(seed, budget_s, threads, target_iters=None):
+    """The oracle's CG (FP64, OpenMP SpMV/dots) on one system, bounded."""
+    from oracle import oracle as O
+    coo, b = c4_system(seed)
+    A = O.Csr(*coo.to_csr(), coo.n)
+    probe = 50
+    t0 = time.perf_counter()
+    O.cg(A, b, tol=1e-300, max_iter=probe, threads=threads)
+    per_it = (time.perf_counter() - t0) / probe
+    cap = max(probe, int(budget_s / per_it))
+    t0 = time.perf_counter()
+    x, info = O.cg(A, b, tol=TOL, max_iter=cap, threads=threads)
+    dt = time.perf_counter() - t0
+    need = info["iters"] if info["converged"] else (target_iters or info["iters"])
+    scale = need / max(info["iters"], 1)
+    return {"ms": dt * 1e3 * scale, "iters_run": info["iters"], "iters_scaled_to": need,
+            "converged_in_sample": info["converged"]}
+
+
+def scipy_cg(seed, budget_s, target_iters=None):
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    coo, b = c4_system(seed)
+    rp, ci, v = coo.to_csr()
+    A = sp.csr_matrix((v.astype(np.float64), ci, rp), shape=(coo.n, coo.n))
+    bb = b.astype(np.float64)
+    t0 = time.perf_counter()
+    spla.cg(A, bb, rtol=1e-300, atol=0.0, maxiter=50)
+    per_it = (time.perf_counter() - t0) / 50
+    cap = max(50, int(budget_s / per_it))
+    it = [0]
+    t0 = time.perf_counter()
+    spla.cg(A, bb, rtol=TOL, maxiter=cap, callback=lambda xk: it.__setitem__(0, it[0] + 1))
+    dt = time.perf_counter() - t0
+    need = target_iters if (it[0] >= cap and target_iters) else it[0]
+    return {"ms": dt * 1e3 * need / max(it[0], 1), "iters_run": it[0], "iters_scaled_to": need}
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------ main ---
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--c3-grid", type=int, default=256)
+    ap.add_argument("--skip-spmv", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        threads = host_threads()
+        ms = []
+        for i in range(args.steps):
+            r = cpu_oracle_cg(TEST_SEED0 + i, args.cpu_budget / max(args.steps, 1), threads)
+            ms.append(r["ms"])
+        v = statistics.mean(ms)
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "solver": "plain CG (oracle port of cgd_op), FP64"},
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                                 "sample": f"{args.steps} systems; each CG run capped at "
+                                           f"{args.cpu_budget / max(args.steps, 1):.1f}s and scaled "
+                                           "to its iteration count to 1e-6"},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local))
+    res = run_ours(args, rank, world, local)
+    hbm, peak_kind = peaks()
+    spmv = res["spmv"]
+    roof = None
+    if spmv:
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "spmv_c3_traffic.json")
+        if os.path.exists(tp):
+            traffic = json.load(open(tp)).get("dram_bytes_per_launch")
+        roof = {"bound": "hbm", "achieved": spmv["gbs"], "peak": hbm, "unit": "GB/s",
+                "frac": spmv["gbs"] / hbm, "traffic": traffic,
+                "kernel": "spmv_tiles<EpiStore> on " + spmv["workload"],
+                "peak_kind": peak_kind, "frac_of_8tbs_spec": spmv["gbs"] / 8000.0}
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        threads = host_threads()
+        target = int(res["plain_cg"]["iters_mean"])
+        o = cpu_oracle_cg(TEST_SEED0, args.cpu_budget, threads, target)
+        s = scipy_cg(TEST_SEED0, args.cpu_budget, target)
+        cpu = {"value": o["ms"], "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"1 system (seed {TEST_SEED0}), oracle CG ran {o['iters_run']} iterations "
+                         f"scaled to {o['iters_scaled_to']}",
+               "scipy_cg": {"value": s["ms"], "unit": UNIT, "iters_run": s["iters_run"],
+                            "iters_scaled_to": s["iters_scaled_to"]}}
+    if rank == 0:
+        line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_solve"],
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "solver": res["solver"], "tol": TOL,
+                           "l2": "flushed between steps (256 MB write)",
+                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                "iters_mean": res["iters_mean"], "true_resid_max": res["true_resid_max"],
+                "plain_cg": res["plain_cg"],
+                "speedup_vs_plain_cg": res["plain_cg"]["ms_per_solve"] / res["ms_per_solve"],
+                "spmv": spmv, "roofline": roof, "cpu_baseline": cpu, "e2e": res["e2e"],
+                "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]}
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -114,7 +114,7 @@ cg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restrict
     s->err = 0;
     s->mode = prm->compat ? 0 : mode;
     s->stall_window = prm->stall_window;
-    s->restart = 1;
+    s->restart = (mode == 2) ? 1 : 0;   // the first G-apply starts the direction
     s->bnorm2 = bb;
     s->rr = bb;
     s->rz = (mode == 1) ? tot[1] : bb;
