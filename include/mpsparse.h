@@ -120,6 +120,23 @@ mps_status mps_csr_spmv(const mps_csr* A, const float* d_x, float* d_y, cudaStre
 mps_status mps_csr_spmv_dot(const mps_csr* A, const float* d_x, const float* d_w, float* d_y,
                             double* d_dot, cudaStream_t stream);
 
+/* y = A x and *d_dot = w . y for callers that cannot allocate device memory
+ * (a process that reserved its whole HBM budget for its own pool at start-up,
+ * or a latency-critical path where an allocation, which can synchronise the
+ * device, is not allowed).  No counterpart in the reference.
+ * Takes the CSR arrays and vectors as device pointers and allocates nothing:
+ * its scratch (tile plan, FP64 partial sums, counter) is one file-scope device
+ * array of about 280 KB that every GPU loading this library holds until exit.
+ * Limit: nnz <= 33,554,432; larger matrices return MPS_ERR_ARG.  The first call
+ * on a device looks up the scratch's device address (cudaGetSymbolAddress), so
+ * make that first call before any stream capture.  All calls share the one
+ * scratch array: calls that overlap on the GPU (other streams, other threads)
+ * race and must not be issued. */
+mps_status mps_csr_spmv_dot_noalloc(const int32_t* d_row_ptr, const int32_t* d_col_ind,
+                                    const float* d_vals, uint32_t n_rows, uint32_t n_cols,
+                                    uint64_t nnz, const float* d_x, const float* d_w, float* d_y,
+                                    double* d_dot, cudaStream_t stream);
+
 /* ---- Solvers on CSR --------------------------------------------------- */
 
 /* CG / Jacobi-PCG / learned-FSAI-PCG, x written in place

@@ -144,3 +144,13 @@ cudaError_t to_bf16_launch(const float* v, __nv_bfloat16* o, uint64_t n, cudaStr
 }
 
 }  // namespace mps
+
+namespace mps {
+// Tile plan into caller-provided memory (used by the allocation-free entry
+// point; spmv_plan_build allocates its own).
+cudaError_t plan_tiles_launch(const int* rp, int n_rows, int tile_nnz, int ntiles, int* tile_row,
+                              cudaStream_t s) {
+    plan_tiles_kernel<<<(ntiles + 1 + 255) / 256, 256, 0, s>>>(rp, n_rows, tile_nnz, ntiles, tile_row);
+    return cudaGetLastError();
+}
+}  // namespace mps
