@@ -187,6 +187,39 @@ mps_status mps_csr_cg_mixed(mps_csr* A, const double* d_b, double* d_x, const mp
 mps_status mps_csr_set_fsai(mps_csr* A, const int32_t* d_g_row_ptr, const int32_t* d_g_col_ind,
                             const float* d_g_vals, uint64_t g_nnz, cudaStream_t stream);
 
+/* Learned FSAI network: per-nonzero MLP 16 -> 64 -> 64 -> 1 (GELU), BF16
+ * weights, FP32 accumulation, run on the tensor cores (tcgen05).  It maps 16
+ * local coefficient features of each nonzero (i, j) of tril(A) to the factor
+ * G (g_ii = softplus(o + log(e-1)) / sqrt(a_ii), g_ij = o / sqrt(a_jj)), so
+ * M^-1 = G^T G is SPD.  Parameters: W1[16][64], b1[64], W2[64][64], b2[64],
+ * w3[64], b3 (mps_fsai_param_count() floats).  No reference counterpart. */
+typedef struct mps_fsai_model mps_fsai_model;
+int32_t mps_fsai_param_count(void);
+/* h_params NULL: deterministic initialisation close to Jacobi. */
+mps_status mps_fsai_model_create(const float* h_params, mps_fsai_model** out);
+mps_status mps_fsai_model_destroy(mps_fsai_model* m);
+mps_status mps_fsai_model_get(const mps_fsai_model* m, float* h_params);
+mps_status mps_fsai_model_set(mps_fsai_model* m, const float* h_params);
+/* Build G = net(A) on tril(A) and attach it for MPS_PRECOND_FSAI. */
+mps_status mps_fsai_attach(mps_csr* A, const mps_fsai_model* m, cudaStream_t stream);
+/* One training step on system A: n_probes Rademacher probes plus n_extra
+ * caller vectors (d_extra, n_extra x n, e.g. CG residuals of A); loss
+ * L = sum ||v - G A G^T v||^2 / (k n) before the step; Adam with rate lr. */
+mps_status mps_fsai_train_step(mps_fsai_model* m, mps_csr* A, int32_t n_probes,
+                               const float* d_extra, int32_t n_extra, float lr, uint64_t seed,
+                               double* loss, cudaStream_t stream);
+/* Inspection: G's pattern and the FP32 features (nnz_g x 16), G's values,
+ * raw network passes on FP32 features, and dL/dg for given probes. */
+mps_status mps_fsai_features(mps_csr* A, float* d_X, int32_t* d_g_row_ptr, int32_t* d_g_col_ind,
+                             uint64_t* nnz_g, cudaStream_t stream);
+mps_status mps_fsai_g_values(mps_csr* A, float* d_g_vals, cudaStream_t stream);
+mps_status mps_fsai_mlp_forward(const mps_fsai_model* m, const float* d_X, uint64_t N,
+                                float* d_out, cudaStream_t stream);
+mps_status mps_fsai_mlp_backward(const mps_fsai_model* m, const float* d_X, const float* d_dout,
+                                 uint64_t N, float* d_grad, cudaStream_t stream);
+mps_status mps_fsai_probe_grad(mps_csr* A, const float* d_V, int32_t k, float* d_grad_g,
+                               double* loss, cudaStream_t stream);
+
 /* ---- BCSR --------------------------------------------------------------- */
 
 /* BCSR from pre-built block arrays: row-major B x B blocks (B = 4 or 8),

@@ -13,6 +13,7 @@
 #pragma once
 #include "common.cuh"
 #include "internal.hpp"
+#include "tma.cuh"
 
 namespace mps {
 
@@ -26,51 +27,6 @@ struct BcsrDev {
     int cap_blocks;         // staged blocks per buffer
     unsigned* err;
 };
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait: false if the limit ran out.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-    for (unsigned i = 0; i < kSpinLimit; ++i) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if (i > 16) __nanosleep(32);
-    }
-    return false;
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
-                                         unsigned long long* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() {
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
 
 // Row k of block j times the x segment: B-wide dot product.
 template <int B>
@@ -92,7 +48,7 @@ __device__ __forceinline__ float block_row_dot(const float* __restrict__ row,
 }
 
 template <int B, class Epi, int NT = kNT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 2)
 bcsr_tiles(BcsrDev A, const float* __restrict__ x, Epi epi) {
     extern __shared__ __align__(128) unsigned char bcsr_smem[];
     __shared__ unsigned long long bar[2];
@@ -118,7 +74,7 @@ bcsr_tiles(BcsrDev A, const float* __restrict__ x, Epi epi) {
 #pragma unroll
     for (int i = 0; i < (Epi::NS > 0 ? Epi::NS : 1); ++i) acc[i] = 0.0;
 
-    unsigned uses[2] = {0u, 0u};   // completed phases per buffer (uniform)
+    unsigned uses0 = 0u, uses1 = 0u;   // completed phases per buffer (uniform)   // completed phases per buffer (uniform)
     auto staged = [&](int t) {
         const int j0 = A.rp[A.tile_brow[t]], j1 = A.rp[A.tile_brow[t + 1]];
         return j1 - j0 <= A.cap_blocks && j1 > j0;
@@ -143,14 +99,14 @@ bcsr_tiles(BcsrDev A, const float* __restrict__ x, Epi epi) {
         const int j0 = A.rp[bs], j1 = A.rp[be];
         const bool use_smem = j1 - j0 <= A.cap_blocks && j1 > j0;
         if (use_smem) {
-            const bool ok = mbar_wait_bounded(&bar[b], uses[b] & 1u);
-            if (!ok) {
+            const unsigned par = (b ? uses1 : uses0) & 1u;
+            if (!mbar_wait_bounded(&bar[b], par)) {
                 // record the phase that never completed; it is waited on
                 // once more (bounded) before the CTA exits
                 atomicOr(A.err, kErrTimeout);
-                timed_out = 1 + (b << 1) + ((uses[b] & 1u) << 2);
+                timed_out = 1 + (b << 1) + (par << 2);
             }
-            ++uses[b];
+            if (b) ++uses1; else ++uses0;
         }
         const int nrows = (be - bs) * B;
         for (int lr = threadIdx.x; lr < nrows; lr += NT) {

@@ -4,7 +4,7 @@
 #include <cstring>
 #include <string>
 
-#include "driver.hpp"
+#include "handles.hpp"
 
 namespace mps {
 
@@ -40,16 +40,10 @@ static mps_status device_error(unsigned err, const char* what) {
 
 using namespace mps;
 
-struct mps_csr {
-    CsrMat A;
-    __nv_bfloat16* vb = nullptr;
-    CsrMat G, Gt;
-    bool has_fsai = false;
-    SolverHost H;
-    unsigned* d_err = nullptr;
-};
 
-static void csr_free(CsrMat& m) {
+namespace mps {
+
+void csr_free(CsrMat& m) {
     if (m.rp) cudaFree(m.rp);
     if (m.ci) cudaFree(m.ci);
     if (m.v) cudaFree(m.v);
@@ -57,12 +51,14 @@ static void csr_free(CsrMat& m) {
     m = CsrMat{};
 }
 
-static mps_status alloc_csr(CsrMat& m, uint32_t n_rows, uint32_t n_cols, uint64_t nnz) {
+mps_status alloc_csr(CsrMat& m, uint32_t n_rows, uint32_t n_cols, uint64_t nnz,
+                     unsigned* err) {
     m.n_rows = n_rows;
     m.n_cols = n_cols;
     m.nnz = nnz;
-    const size_t nz = nnz ? nnz : 1;
-    MPS_CUDA(cudaMalloc(&m.rp, ((size_t)n_rows + 1) * sizeof(int32_t)));
+    m.err = err;
+    const size_t nz = nnz + kCsrPad;
+    MPS_CUDA(cudaMalloc(&m.rp, ((size_t)n_rows + 1 + kCsrPad) * sizeof(int32_t)));
     MPS_CUDA(cudaMalloc(&m.ci, nz * sizeof(int32_t)));
     MPS_CUDA(cudaMalloc(&m.v, nz * sizeof(float)));
     return MPS_OK;
@@ -76,10 +72,10 @@ static mps_status check_shape(uint64_t nnz, uint32_t n_rows, uint32_t n_cols) {
 }
 
 // Sort + CSR + tile plan into a fresh CsrMat.
-static mps_status build_from_keys(CsrMat& m, const uint64_t* keys, const uint32_t* payload,
+mps_status build_from_keys(CsrMat& m, const uint64_t* keys, const uint32_t* payload,
                                   uint64_t nnz, uint32_t n_rows, uint32_t n_cols, unsigned* d_err,
                                   cudaStream_t s) {
-    mps_status st = alloc_csr(m, n_rows, n_cols, nnz);
+    mps_status st = alloc_csr(m, n_rows, n_cols, nnz, d_err);
     if (st != MPS_OK) return st;
     MPS_CUDA(cudaMemsetAsync(d_err, 0, sizeof(unsigned), s));
     MPS_CUDA(sort_to_csr(keys, payload, nnz, n_rows, n_cols, m.rp, m.ci, (uint32_t*)m.v, d_err, s));
@@ -89,6 +85,8 @@ static mps_status build_from_keys(CsrMat& m, const uint64_t* keys, const uint32_
     MPS_CUDA(cudaStreamSynchronize(s));
     return device_error(err, "COO->CSR");
 }
+
+}  // namespace mps
 
 extern "C" {
 
@@ -149,7 +147,7 @@ mps_status mps_csr_create_from_csr(const int32_t* d_row_ptr, const int32_t* d_co
     if (!d_row_ptr || (nnz && (!d_col_ind || !d_vals))) return fail(MPS_ERR_ARG, "null CSR array");
     mps_csr* h = new mps_csr();
     MPS_CUDA(cudaMalloc(&h->d_err, sizeof(unsigned)));
-    st = alloc_csr(h->A, n_rows, n_cols, nnz);
+    st = alloc_csr(h->A, n_rows, n_cols, nnz, h->d_err);
     if (st != MPS_OK) {
         mps_csr_destroy(h);
         return st;
@@ -176,6 +174,7 @@ mps_status mps_csr_destroy(mps_csr* h) {
     csr_free(h->Gt);
     if (h->vb) cudaFree(h->vb);
     if (h->d_err) cudaFree(h->d_err);
+    fsai_work_free(h->fw);
     h->H.destroy();
     delete h;
     return MPS_OK;
@@ -237,7 +236,10 @@ mps_status mps_csr_spmv_dot(const mps_csr* hc, const float* d_x, const float* d_
     return MPS_OK;
 }
 
-static mps_status prepare_precond(mps_csr* h, const mps_solve_opts* o, cudaStream_t s) {
+}  // extern "C"
+
+namespace mps {
+mps_status prepare_precond(mps_csr* h, const mps_solve_opts* o, cudaStream_t s) {
     MPS_CUDA(h->H.ensure(h->A.n_rows));
     const int pc = o ? o->precond : 0;
     if (pc != MPS_PRECOND_NONE && !(o && o->reference_compat)) {
@@ -254,6 +256,9 @@ static mps_status prepare_precond(mps_csr* h, const mps_solve_opts* o, cudaStrea
     }
     return MPS_OK;
 }
+}  // namespace mps
+
+extern "C" {
 
 static mps_status csr_solve(SolverKind kind, mps_csr* h, const float* b, float* x,
                             const mps_solve_opts* o, mps_solve_info* info, cudaStream_t s) {
@@ -288,9 +293,10 @@ mps_status mps_csr_set_fsai(mps_csr* h, const int32_t* d_g_row_ptr, const int32_
     const uint32_t n = h->A.n_rows;
     csr_free(h->G);
     csr_free(h->Gt);
+    fsai_work_free(h->fw);   // a network factor (if any) is replaced
     h->has_fsai = false;
     h->H.drop_graphs();
-    mps_status st = alloc_csr(h->G, n, n, g_nnz);
+    mps_status st = alloc_csr(h->G, n, n, g_nnz, h->d_err);
     if (st != MPS_OK) return st;
     MPS_CUDA(cudaMemcpyAsync(h->G.rp, d_g_row_ptr, ((size_t)n + 1) * 4, cudaMemcpyDeviceToDevice, s));
     MPS_CUDA(cudaMemcpyAsync(h->G.ci, d_g_col_ind, g_nnz * 4, cudaMemcpyDeviceToDevice, s));
@@ -379,7 +385,7 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
     SolverHost& H = h->H;
     const int n = (int)h->A.n_rows;
     if (bf16 && !h->vb) {
-        MPS_CUDA(cudaMalloc(&h->vb, (h->A.nnz ? h->A.nnz : 1) * sizeof(__nv_bfloat16)));
+        MPS_CUDA(cudaMalloc(&h->vb, (h->A.nnz + kCsrPad) * sizeof(__nv_bfloat16)));
         MPS_CUDA(to_bf16_launch(h->A.v, h->vb, h->A.nnz, s));
     }
     double* scal = nullptr;   // [0] = ||b||^2, [1] = ||r||^2

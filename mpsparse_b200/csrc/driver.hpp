@@ -2,6 +2,7 @@
 // graph capture with a device-side WHILE loop, result and info read-back.
 #pragma once
 #include "solvers.cuh"
+#include "csr_stream.cuh"
 
 namespace mps {
 
@@ -16,20 +17,38 @@ inline void smem_optin_k(K kernel, size_t smem) {
         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
+// Resident CTAs per SM of a kernel at a given dynamic shared memory size
+// (cached per kernel and size).
+int resident_ctas(const void* kernel, int threads, size_t smem);
+
+// Persistent grid for a tile loop: every CTA resident at once, so the static
+// tile-to-CTA assignment never runs a second wave.
+template <class K>
+inline int persistent_grid(K kernel, size_t smem, int ntiles) {
+    const int per_sm = resident_ctas(reinterpret_cast<const void*>(kernel), kNT, smem);
+    int g = num_sms() * (per_sm > 0 ? per_sm : 1);
+    if (g > kMaxPartials) g = kMaxPartials;
+    if (g > ntiles) g = ntiles;
+    return g < 1 ? 1 : g;
+}
+
 // CSR operator: A x through the tile kernel with a given epilogue.
 struct CsrOp {
     const CsrMat* A;
     const __nv_bfloat16* vb = nullptr;
     template <class Epi>
     cudaError_t apply(const float* x, const Epi& e, cudaStream_t s) const {
-        const CsrDev v = A->view(vb);
-        const size_t smem = spmv_smem_bytes<float>(v);
+        const CsrStreamDev v = A->stream_view(vb);
         if (vb) {
-            smem_optin_k(spmv_tiles<float, float, true, Epi>, smem);
-            spmv_tiles<float, float, true, Epi><<<A->plan.grid, kNT, smem, s>>>(v, x, e);
+            const size_t smem = 2 * stream_buf_bytes<true>(v.cap, v.rcap);
+            smem_optin_k(spmv_stream<true, Epi>, smem);
+            const int g = persistent_grid(spmv_stream<true, Epi>, smem, v.ntiles);
+            spmv_stream<true, Epi><<<g, kNT, smem, s>>>(v, x, e);
         } else {
-            smem_optin_k(spmv_tiles<float, float, false, Epi>, smem);
-            spmv_tiles<float, float, false, Epi><<<A->plan.grid, kNT, smem, s>>>(v, x, e);
+            const size_t smem = 2 * stream_buf_bytes<false>(v.cap, v.rcap);
+            smem_optin_k(spmv_stream<false, Epi>, smem);
+            const int g = persistent_grid(spmv_stream<false, Epi>, smem, v.ntiles);
+            spmv_stream<false, Epi><<<g, kNT, smem, s>>>(v, x, e);
         }
         return cudaGetLastError();
     }

@@ -1,0 +1,45 @@
+// handles.hpp -- definition of the opaque mps_csr handle, shared by the
+// translation units that operate on it.
+#pragma once
+#include "driver.hpp"
+
+namespace mps {
+
+// Learned-FSAI state of one matrix: G's pattern (tril(A)) and its maps.
+struct FsaiWork {
+    bool ready = false;
+    uint64_t nnz_g = 0;
+    int32_t* g_row = nullptr;      // row of each G nonzero
+    int32_t* g_aidx = nullptr;     // index of the matching entry of A
+    uint32_t* perm = nullptr;      // G^T position -> G position
+    __nv_bfloat16* X = nullptr;    // features [nnz_g][16]
+    float* out = nullptr;          // MLP output per G nonzero
+    float* dgdo = nullptr;         // d g / d out
+    float* grad = nullptr;         // dL/dg, then dL/dout
+    float* rinfo = nullptr;        // per-row feature inputs of A
+    double* d_loss = nullptr;
+    float* vec = nullptr;          // probe work vectors (6 x n)
+};
+
+}  // namespace mps
+
+struct mps_csr {
+    mps::CsrMat A;
+    __nv_bfloat16* vb = nullptr;
+    mps::CsrMat G, Gt;
+    bool has_fsai = false;
+    mps::SolverHost H;
+    unsigned* d_err = nullptr;
+    mps::FsaiWork fw;
+};
+
+namespace mps {
+void csr_free(CsrMat& m);
+mps_status alloc_csr(CsrMat& m, uint32_t n_rows, uint32_t n_cols, uint64_t nnz, unsigned* err);
+mps_status build_from_keys(CsrMat& m, const uint64_t* keys, const uint32_t* payload, uint64_t nnz,
+                           uint32_t n_rows, uint32_t n_cols, unsigned* d_err, cudaStream_t s);
+mps_status prepare_precond(mps_csr* h, const mps_solve_opts* o, cudaStream_t s);
+cudaError_t exclusive_scan_rows(const unsigned* counts, uint64_t n, int32_t* out, unsigned* bsum,
+                                cudaStream_t s);
+void fsai_work_free(FsaiWork& w);
+}  // namespace mps

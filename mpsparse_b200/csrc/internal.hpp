@@ -69,6 +69,23 @@ struct SpmvPlan {
     int cap = 0;
     int grid = 0;          // persistent CTAs
     int* d_tile_row = nullptr;
+    int4* d_meta = nullptr;   // per tile {row begin, row end, nnz begin, nnz end}
+    int cap_s = 0;            // staged nonzeros per buffer of the TMA kernel
+    int rcap = 0;             // staged row_ptr entries per buffer
+    int grid_s = 0;           // persistent CTAs of the TMA kernel
+};
+
+// View of a CSR for the TMA-staged kernel (csr_stream.cuh).
+struct CsrStreamDev {
+    const int* rp;
+    const int* ci;
+    const float* v;
+    const __nv_bfloat16* vb;
+    const int4* meta;
+    int ntiles;
+    int cap;
+    int rcap;
+    unsigned* err;
 };
 
 // Launch geometry of the streaming vector kernels.
@@ -103,10 +120,18 @@ struct CsrMat {
     uint32_t n_rows = 0, n_cols = 0;
     uint64_t nnz = 0;
     SpmvPlan plan;
+    unsigned* err = nullptr;   // device error word (bounded-wait timeouts)
     CsrDev view(const __nv_bfloat16* vb = nullptr) const {
         return CsrDev{rp, ci, v, vb, plan.d_tile_row, (int)n_rows, plan.ntiles, plan.cap};
     }
+    CsrStreamDev stream_view(const __nv_bfloat16* vb = nullptr) const {
+        return CsrStreamDev{rp, ci, v, vb, plan.d_meta, plan.ntiles, plan.cap_s, plan.rcap, err};
+    }
 };
+
+// Spare elements after each CSR array: 16-byte-rounded bulk copies of a tile
+// never leave the allocation.
+constexpr int kCsrPad = 16;
 
 // ---- internal entry points ---------------------------------------------------
 // Sort packed keys into CSR arrays (caller-allocated outputs).  `payload` is

@@ -1,5 +1,8 @@
 // spmv.cu -- SpMV tile plans, plain SpMV launches and CSR utilities.
-#include "spmv_kernels.cuh"
+#include <map>
+#include <mutex>
+
+#include "driver.hpp"
 
 namespace mps {
 namespace {
@@ -29,6 +32,14 @@ __global__ void plan_tiles_kernel(const int* __restrict__ rp, int n_rows, int T,
             hi = mid;
     }
     tile_row[t] = lo;
+}
+
+__global__ void plan_meta_kernel(const int* __restrict__ rp, const int* __restrict__ tile_row,
+                                 int ntiles, int4* __restrict__ meta) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    const int rs = tile_row[t], re = tile_row[t + 1];
+    meta[t] = make_int4(rs, re, rp[rs], rp[re]);
 }
 
 __global__ void diag_inv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
@@ -76,6 +87,7 @@ int default_tile_nnz(uint64_t nnz, uint32_t n_rows) {
 
 void spmv_plan_free(SpmvPlan& p) {
     if (p.d_tile_row) cudaFree(p.d_tile_row);
+    if (p.d_meta) cudaFree(p.d_meta);
     p = SpmvPlan{};
 }
 
@@ -90,13 +102,24 @@ cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s) {
     const int cap_grid = num_sms() * 8;
     p.grid = p.ntiles < cap_grid ? p.ntiles : cap_grid;
     if (p.grid < 1) p.grid = 1;
+    p.cap_s = (tile_nnz + 256 + 7) & ~7;
+    p.rcap = 520;
+    p.grid_s = p.ntiles < num_sms() * 6 ? p.ntiles : num_sms() * 6;
+    if (p.grid_s < 1) p.grid_s = 1;
     cudaError_t e = cudaMalloc(&p.d_tile_row, (size_t)(p.ntiles + 1) * sizeof(int));
     if (e != cudaSuccess) return e;
+    e = cudaMalloc(&p.d_meta, (size_t)p.ntiles * sizeof(int4));
+    if (e != cudaSuccess) {
+        cudaFree(p.d_tile_row);
+        return e;
+    }
     plan_tiles_kernel<<<(p.ntiles + 1 + 255) / 256, 256, 0, s>>>(A.rp, (int)A.n_rows, tile_nnz,
                                                                  p.ntiles, p.d_tile_row);
+    plan_meta_kernel<<<(p.ntiles + 255) / 256, 256, 0, s>>>(A.rp, p.d_tile_row, p.ntiles, p.d_meta);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         cudaFree(p.d_tile_row);
+        cudaFree(p.d_meta);
         return e;
     }
     spmv_plan_free(A.plan);
@@ -109,23 +132,26 @@ static void smem_optin(K kernel, size_t smem) {
     if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
+int resident_ctas(const void* kernel, int threads, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, size_t>, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_pair(kernel, smem);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess) n = 1;
+    cache[key] = n;
+    return n;
+}
+
 cudaError_t spmv_launch(const CsrMat& A, const float* x, float* y, cudaStream_t s) {
-    const CsrDev v = A.view();
-    const size_t smem = spmv_smem_bytes<float>(v);
-    EpiStore e{y};
-    smem_optin(spmv_tiles<float, float, false, EpiStore>, smem);
-    spmv_tiles<float, float, false, EpiStore><<<A.plan.grid, kNT, smem, s>>>(v, x, e);
-    return cudaGetLastError();
+    return CsrOp{&A, nullptr}.apply(x, EpiStore{y}, s);
 }
 
 cudaError_t spmv_dot_launch(const CsrMat& A, const float* x, const float* w, float* y,
                             double* d_dot, double* partials, unsigned* counter, cudaStream_t s) {
-    const CsrDev v = A.view();
-    const size_t smem = spmv_smem_bytes<float>(v);
-    EpiStoreDot e{y, w, d_dot, counter, partials};
-    smem_optin(spmv_tiles<float, float, false, EpiStoreDot>, smem);
-    spmv_tiles<float, float, false, EpiStoreDot><<<A.plan.grid, kNT, smem, s>>>(v, x, e);
-    return cudaGetLastError();
+    return CsrOp{&A, nullptr}.apply(x, EpiStoreDot{y, w, d_dot, counter, partials}, s);
 }
 
 cudaError_t diag_inv_launch(const CsrMat& A, float* dinv, cudaStream_t s) {

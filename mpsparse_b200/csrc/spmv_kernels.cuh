@@ -70,7 +70,7 @@ __device__ __forceinline__ void load_prod4(const CsrDev& A, const XT* __restrict
 //   __device__ void finalize(const double* tot)    last CTA, thread 0
 //   unsigned* counter; double* partials;           (when NS > 0)
 template <typename XT, typename ST, bool BF16, class Epi, int NT = kNT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 4)
 spmv_tiles(CsrDev A, const XT* __restrict__ x, Epi epi) {
     extern __shared__ __align__(16) unsigned char spmv_smem[];
     ST* prod = reinterpret_cast<ST*>(spmv_smem);

@@ -59,6 +59,56 @@ int precond_code(const std::string& p) {
     throw std::invalid_argument("precond must be 'none', 'jacobi' or 'fsai'");
 }
 
+class FsaiModel {
+public:
+    explicit FsaiModel(c10::optional<torch::Tensor> params) {
+        std::vector<float> host;
+        const float* p = nullptr;
+        if (params && params->defined()) {
+            auto t = params->to(torch::kCPU).to(torch::kFloat32).contiguous();
+            TORCH_CHECK(t.numel() == mps_fsai_param_count(), "params must hold ", mps_fsai_param_count(),
+                        " floats");
+            host.assign(t.data_ptr<float>(), t.data_ptr<float>() + t.numel());
+            p = host.data();
+        }
+        check(mps_fsai_model_create(p, &m_), "fsai_model");
+    }
+    ~FsaiModel() { mps_fsai_model_destroy(m_); }
+    torch::Tensor params() const {
+        auto t = torch::empty({mps_fsai_param_count()}, torch::kFloat32);
+        check(mps_fsai_model_get(m_, t.data_ptr<float>()), "params");
+        return t;
+    }
+    void set_params(torch::Tensor p) {
+        auto t = p.to(torch::kCPU).to(torch::kFloat32).contiguous();
+        TORCH_CHECK(t.numel() == mps_fsai_param_count(), "wrong parameter count");
+        check(mps_fsai_model_set(m_, t.data_ptr<float>()), "set_params");
+    }
+    torch::Tensor forward(torch::Tensor X) const {
+        auto x = on_device(X, torch::kFloat32, "X");
+        TORCH_CHECK(x.dim() == 2 && x.size(1) == 16, "X must be N x 16");
+        auto out = torch::empty({x.size(0)}, x.options());
+        check(mps_fsai_mlp_forward(m_, x.data_ptr<float>(), (uint64_t)x.size(0), out.data_ptr<float>(),
+                                   cur_stream()),
+              "mlp_forward");
+        return out;
+    }
+    torch::Tensor backward(torch::Tensor X, torch::Tensor dout) const {
+        auto x = on_device(X, torch::kFloat32, "X");
+        auto d = on_device(dout, torch::kFloat32, "dout");
+        TORCH_CHECK(x.dim() == 2 && x.size(1) == 16 && d.numel() == x.size(0), "shapes");
+        auto g = torch::empty({mps_fsai_param_count()}, x.options());
+        check(mps_fsai_mlp_backward(m_, x.data_ptr<float>(), d.data_ptr<float>(), (uint64_t)x.size(0),
+                                    g.data_ptr<float>(), cur_stream()),
+              "mlp_backward");
+        return g;
+    }
+    mps_fsai_model* handle() const { return m_; }
+
+private:
+    mps_fsai_model* m_ = nullptr;
+};
+
 class CsrTensor {
 public:
     CsrTensor(torch::Tensor keys, torch::Tensor values, torch::Tensor row_ptr,
@@ -214,6 +264,65 @@ public:
         check(mps_csr_set_fsai(h_, r.data_ptr<int32_t>(), c.data_ptr<int32_t>(), w.data_ptr<float>(),
                                (uint64_t)c.numel(), cur_stream()),
               "set_fsai");
+    }
+
+    void attach_fsai(const FsaiModel& m) {
+        c10::cuda::CUDAGuard g(device_);
+        check(mps_fsai_attach(h_, m.handle(), cur_stream()), "attach_fsai");
+    }
+
+    double fsai_train_step(FsaiModel& m, int64_t n_probes, c10::optional<torch::Tensor> extra,
+                           double lr, int64_t seed) {
+        c10::cuda::CUDAGuard g(device_);
+        torch::Tensor e;
+        int64_t ne = 0;
+        if (extra && extra->defined() && extra->numel() > 0) {
+            e = on_device(*extra, torch::kFloat32, "extra");
+            TORCH_CHECK(e.numel() % n_rows_ == 0, "extra must be k x num_rows");
+            ne = e.numel() / n_rows_;
+        }
+        double loss = 0;
+        check(mps_fsai_train_step(m.handle(), h_, (int32_t)n_probes, ne ? e.data_ptr<float>() : nullptr,
+                                  (int32_t)ne, (float)lr, (uint64_t)seed, &loss, cur_stream()),
+              "fsai_train_step");
+        return loss;
+    }
+
+    std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> fsai_features() {
+        c10::cuda::CUDAGuard g(device_);
+        uint64_t nz = 0;
+        check(mps_fsai_features(h_, nullptr, nullptr, nullptr, &nz, cur_stream()), "fsai_features");
+        auto opt = torch::TensorOptions().device(torch::kCUDA, device_);
+        auto X = torch::empty({(int64_t)nz, 16}, opt.dtype(torch::kFloat32));
+        auto rp = torch::empty({n_rows_ + 1}, opt.dtype(torch::kInt32));
+        auto ci = torch::empty({(int64_t)nz}, opt.dtype(torch::kInt32));
+        check(mps_fsai_features(h_, X.data_ptr<float>(), rp.data_ptr<int32_t>(), ci.data_ptr<int32_t>(),
+                                &nz, cur_stream()),
+              "fsai_features");
+        return {X, rp, ci};
+    }
+
+    torch::Tensor fsai_g_values() {
+        c10::cuda::CUDAGuard g(device_);
+        uint64_t nz = 0;
+        check(mps_fsai_features(h_, nullptr, nullptr, nullptr, &nz, cur_stream()), "fsai_g_values");
+        auto v = torch::empty({(int64_t)nz}, torch::TensorOptions().device(torch::kCUDA, device_));
+        check(mps_fsai_g_values(h_, v.data_ptr<float>(), cur_stream()), "fsai_g_values");
+        return v;
+    }
+
+    std::tuple<torch::Tensor, double> fsai_probe_grad(torch::Tensor V) {
+        c10::cuda::CUDAGuard g(device_);
+        auto v = on_device(V, torch::kFloat32, "V");
+        TORCH_CHECK(v.numel() % n_rows_ == 0, "V must be k x num_rows");
+        uint64_t nz = 0;
+        check(mps_fsai_features(h_, nullptr, nullptr, nullptr, &nz, cur_stream()), "fsai_probe_grad");
+        auto grad = torch::empty({(int64_t)nz}, v.options());
+        double loss = 0;
+        check(mps_fsai_probe_grad(h_, v.data_ptr<float>(), (int32_t)(v.numel() / n_rows_),
+                                  grad.data_ptr<float>(), &loss, cur_stream()),
+              "fsai_probe_grad");
+        return {grad, loss};
     }
 
     int64_t nnz() const { return nnz_; }
@@ -421,10 +530,23 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
              py::arg("value_bits") = 32, py::arg("precond") = "none")
         .def("set_fsai", &CsrTensor::set_fsai, py::arg("row_ptr"), py::arg("col_ind"),
              py::arg("values"))
+        .def("attach_fsai", &CsrTensor::attach_fsai, py::arg("model"))
+        .def("fsai_train_step", &CsrTensor::fsai_train_step, py::arg("model"), py::arg("n_probes") = 4,
+             py::arg("extra") = py::none(), py::arg("lr") = 1e-3, py::arg("seed") = 0)
+        .def("fsai_features", &CsrTensor::fsai_features)
+        .def("fsai_g_values", &CsrTensor::fsai_g_values)
+        .def("fsai_probe_grad", &CsrTensor::fsai_probe_grad, py::arg("V"))
         .def("csr", &CsrTensor::export_csr)
         .def_property_readonly("nnz", &CsrTensor::nnz)
         .def_property_readonly("num_rows", &CsrTensor::num_rows)
         .def_property_readonly("num_cols", &CsrTensor::num_cols);
+
+    py::class_<FsaiModel>(m, "fsai_model")
+        .def(py::init<c10::optional<torch::Tensor>>(), py::arg("params") = py::none())
+        .def("params", &FsaiModel::params)
+        .def("set_params", &FsaiModel::set_params, py::arg("params"))
+        .def("forward", &FsaiModel::forward, py::arg("X"))
+        .def("backward", &FsaiModel::backward, py::arg("X"), py::arg("dout"));
 
     py::class_<BcsrTensor>(m, "bcsr_tensor")
         .def(py::init<torch::Tensor, torch::Tensor, torch::Tensor, torch::Tensor, int64_t, int64_t,
@@ -453,4 +575,5 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
           py::arg("row_ptr"), py::arg("col_ind"), py::arg("out_vals"), py::arg("num_rows"),
           py::arg("num_cols"));
     m.def("abi_version", []() { return mps_abi_version(); });
+    m.def("fsai_param_count", []() { return mps_fsai_param_count(); });
 }

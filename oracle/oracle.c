@@ -389,3 +389,229 @@ int orc_richardson(const orc_op* A, const double* b, double* x, const orc_opts* 
     free(s1);
     return 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Learned FSAI (no reference counterpart: restates this package's design)  */
+/* ------------------------------------------------------------------------ */
+
+int64_t orc_fsai_pattern(const orc_op* A, int32_t* g_rp, int32_t* g_ci, int32_t* g_row,
+                         int32_t* g_aidx) {
+    int64_t k = 0;
+    g_rp[0] = 0;
+    for (int64_t i = 0; i < A->n; ++i) {
+        for (int32_t a = A->row_ptr[i]; a < A->row_ptr[i + 1]; ++a) {
+            if (A->col_ind[a] <= i) {
+                g_ci[k] = A->col_ind[a];
+                g_row[k] = (int32_t)i;
+                g_aidx[k] = a;
+                ++k;
+            }
+        }
+        g_rp[i + 1] = (int32_t)k;
+    }
+    return k;
+}
+
+typedef struct {
+    double diag, dd;
+    int32_t ln, lf, un, uf;     /* nearest / farther lower and upper neighbours (-1: none) */
+    double lnv, lfv, unv, ufv;  /* their coefficients */
+} orc_rowinfo;
+
+static void row_info(const orc_op* A, int64_t i, orc_rowinfo* ri) {
+    ri->diag = 0.0;
+    ri->ln = ri->lf = ri->un = ri->uf = -1;
+    ri->lnv = ri->lfv = ri->unv = ri->ufv = 0.0;
+    double off = 0.0;
+    for (int32_t a = A->row_ptr[i]; a < A->row_ptr[i + 1]; ++a) {
+        const int32_t c = A->col_ind[a];
+        const double v = A->val[a];
+        if (c == i) {
+            ri->diag += v;
+            continue;
+        }
+        off += fabs(v);
+        if (c < i) {          /* columns ascend: the last lower ones are nearest */
+            ri->lf = ri->ln;
+            ri->lfv = ri->lnv;
+            ri->ln = c;
+            ri->lnv = v;
+        } else if (ri->un < 0) {
+            ri->un = c;
+            ri->unv = v;
+        } else if (ri->uf < 0) {
+            ri->uf = c;
+            ri->ufv = v;
+        }
+    }
+    ri->dd = ri->diag != 0.0 ? (ri->diag - off) / ri->diag : 0.0;
+}
+
+static double diag_at(const orc_op* A, int64_t i) {
+    double d = 0.0;
+    for (int32_t a = A->row_ptr[i]; a < A->row_ptr[i + 1]; ++a)
+        if (A->col_ind[a] == i) d += A->val[a];
+    return d;
+}
+
+static double nrm(double v, double di, double dj) { return v / sqrt(di * dj); }
+
+void orc_fsai_features(const orc_op* A, int64_t nnz_g, const int32_t* g_row, const int32_t* g_ci,
+                       const int32_t* g_aidx, float* X) {
+    for (int64_t k = 0; k < nnz_g; ++k) {
+        const int64_t i = g_row[k], j = g_ci[k];
+        orc_rowinfo ri, rj;
+        row_info(A, i, &ri);
+        row_info(A, j, &rj);
+        const double di = ri.diag, dj = rj.diag;
+        float* f = X + k * ORC_NF;
+        f[0] = 1.0f;
+        f[1] = (float)(i == j);
+        f[2] = (float)(j == ri.ln);
+        f[3] = (float)(j == ri.lf);
+        f[4] = ri.ln >= 0 ? (float)nrm(ri.lnv, di, diag_at(A, ri.ln)) : 0.0f;
+        f[5] = ri.lf >= 0 ? (float)nrm(ri.lfv, di, diag_at(A, ri.lf)) : 0.0f;
+        f[6] = ri.un >= 0 ? (float)nrm(ri.unv, di, diag_at(A, ri.un)) : 0.0f;
+        f[7] = ri.uf >= 0 ? (float)nrm(ri.ufv, di, diag_at(A, ri.uf)) : 0.0f;
+        f[8] = ri.ln >= 0 ? (float)log(di / diag_at(A, ri.ln)) : 0.0f;
+        f[9] = ri.lf >= 0 ? (float)log(di / diag_at(A, ri.lf)) : 0.0f;
+        f[10] = i == j ? 1.0f : (float)nrm(A->val[g_aidx[k]], di, dj);
+        f[11] = (float)log(di / dj);
+        f[12] = (float)ri.dd;
+        f[13] = (float)rj.dd;
+        f[14] = rj.ln >= 0 ? (float)nrm(rj.lnv, dj, diag_at(A, rj.ln)) : 0.0f;
+        f[15] = rj.lf >= 0 ? (float)nrm(rj.lfv, dj, diag_at(A, rj.lf)) : 0.0f;
+    }
+}
+
+/* Round-to-nearest-even to bfloat16 (kept as a float). */
+static float bf16r(float f) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) return f;       /* inf / nan */
+    u += 0x7fffu + ((u >> 16) & 1u);
+    u &= 0xffff0000u;
+    float r;
+    memcpy(&r, &u, 4);
+    return r;
+}
+
+static double gelu(double x) { return 0.5 * x * (1.0 + erf(x / sqrt(2.0))); }
+static double gelu_d(double x) {
+    return 0.5 * (1.0 + erf(x / sqrt(2.0))) + x * exp(-0.5 * x * x) / sqrt(2.0 * M_PI);
+}
+
+typedef struct {
+    const float *W1, *b1, *W2, *b2, *w3, *b3;
+} orc_mlp;
+
+static orc_mlp mlp_view(const float* p) {
+    orc_mlp m;
+    m.W1 = p;
+    m.b1 = m.W1 + ORC_NF * ORC_NH;
+    m.W2 = m.b1 + ORC_NH;
+    m.b2 = m.W2 + ORC_NH * ORC_NH;
+    m.w3 = m.b2 + ORC_NH;
+    m.b3 = m.w3 + ORC_NH;
+    return m;
+}
+
+/* One row through the network; z1, h1 (bf16-rounded), z2, h2 out. */
+static double mlp_row(const orc_mlp* m, const float* x, double* z1, double* h1, double* z2,
+                      double* h2) {
+    float xb[ORC_NF];
+    for (int f = 0; f < ORC_NF; ++f) xb[f] = bf16r(x[f]);
+    for (int o = 0; o < ORC_NH; ++o) {
+        double s = 0.0;
+        for (int f = 0; f < ORC_NF; ++f) s += (double)xb[f] * bf16r(m->W1[f * ORC_NH + o]);
+        z1[o] = s + m->b1[o];
+        h1[o] = bf16r((float)gelu(z1[o]));
+    }
+    double out = m->b3[0];
+    for (int o = 0; o < ORC_NH; ++o) {
+        double s = 0.0;
+        for (int f = 0; f < ORC_NH; ++f) s += h1[f] * bf16r(m->W2[f * ORC_NH + o]);
+        z2[o] = s + m->b2[o];
+        h2[o] = gelu(z2[o]);
+        out += h2[o] * bf16r(m->w3[o]);
+    }
+    return out;
+}
+
+void orc_mlp_forward(const float* params, const float* X, int64_t N, double* out) {
+    orc_mlp m = mlp_view(params);
+    double z1[ORC_NH], h1[ORC_NH], z2[ORC_NH], h2[ORC_NH];
+    for (int64_t r = 0; r < N; ++r) out[r] = mlp_row(&m, X + r * ORC_NF, z1, h1, z2, h2);
+}
+
+void orc_mlp_backward(const float* params, const float* X, int64_t N, const double* dout,
+                      double* grad) {
+    orc_mlp m = mlp_view(params);
+    for (int i = 0; i < ORC_NPARAM; ++i) grad[i] = 0.0;
+    double *gW1 = grad, *gb1 = gW1 + ORC_NF * ORC_NH, *gW2 = gb1 + ORC_NH,
+           *gb2 = gW2 + ORC_NH * ORC_NH, *gw3 = gb2 + ORC_NH, *gb3 = gw3 + ORC_NH;
+    double z1[ORC_NH], h1[ORC_NH], z2[ORC_NH], h2[ORC_NH], dz2[ORC_NH], dz1[ORC_NH];
+    for (int64_t r = 0; r < N; ++r) {
+        const float* x = X + r * ORC_NF;
+        mlp_row(&m, x, z1, h1, z2, h2);
+        const double d = dout[r];
+        gb3[0] += d;
+        for (int o = 0; o < ORC_NH; ++o) {
+            gw3[o] += d * h2[o];
+            const double g = d * bf16r(m.w3[o]) * gelu_d(z2[o]);
+            gb2[o] += g;
+            dz2[o] = bf16r((float)g);
+        }
+        for (int f = 0; f < ORC_NH; ++f)
+            for (int o = 0; o < ORC_NH; ++o) gW2[f * ORC_NH + o] += h1[f] * dz2[o];
+        for (int f = 0; f < ORC_NH; ++f) {
+            double s = 0.0;
+            for (int o = 0; o < ORC_NH; ++o) s += dz2[o] * bf16r(m.W2[f * ORC_NH + o]);
+            const double g = s * gelu_d(z1[f]);
+            gb1[f] += g;
+            dz1[f] = bf16r((float)g);
+        }
+        for (int f = 0; f < ORC_NF; ++f) {
+            const double xb = bf16r(x[f]);
+            for (int o = 0; o < ORC_NH; ++o) gW1[f * ORC_NH + o] += xb * dz1[o];
+        }
+    }
+}
+
+static void apply_t(const orc_op* G, const double* v, double* u) {   /* u = G^T v */
+    for (int64_t j = 0; j < G->n; ++j) u[j] = 0.0;
+    for (int64_t i = 0; i < G->n; ++i)
+        for (int32_t a = G->row_ptr[i]; a < G->row_ptr[i + 1]; ++a)
+            u[G->col_ind[a]] += (double)G->val[a] * v[i];
+}
+
+double orc_fsai_probe_loss_grad(const orc_op* A, const orc_op* G, const double* V, int k,
+                                double* grad_g) {
+    const int64_t n = A->n;
+    double *u = malloc(n * 8), *w = malloc(n * 8), *y = malloc(n * 8), *e = malloc(n * 8),
+           *t = malloc(n * 8), *s = malloc(n * 8);
+    const int64_t nnz = G->row_ptr[n];
+    for (int64_t a = 0; a < nnz; ++a) grad_g[a] = 0.0;
+    double loss = 0.0;
+    for (int p = 0; p < k; ++p) {
+        const double* v = V + (int64_t)p * n;
+        apply_t(G, v, u);
+        apply(A, u, w, 1);
+        apply(G, w, y, 1);
+        for (int64_t i = 0; i < n; ++i) {
+            e[i] = y[i] - v[i];
+            loss += e[i] * e[i];
+        }
+        apply_t(G, e, t);
+        apply(A, t, s, 1);
+        for (int64_t i = 0; i < n; ++i)
+            for (int32_t a = G->row_ptr[i]; a < G->row_ptr[i + 1]; ++a) {
+                const int32_t j = G->col_ind[a];
+                grad_g[a] += e[i] * w[j] + v[i] * s[j];
+            }
+    }
+    const double sc = 1.0 / ((double)k * (double)n);
+    for (int64_t a = 0; a < nnz; ++a) grad_g[a] *= 2.0 * sc;
+    free(u); free(w); free(y); free(e); free(t); free(s);
+    return loss * sc;
+}

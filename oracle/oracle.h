@@ -74,6 +74,31 @@ int orc_richardson(const orc_op* A, const double* b, double* x, const orc_opts* 
 /* ||b - A x|| / ||b|| in FP64. */
 double orc_true_residual(const orc_op* A, const double* b, const double* x);
 
+/* ---- learned FSAI preconditioner (no reference counterpart) -------------- */
+#define ORC_NF 16
+#define ORC_NH 64
+/* parameter vector: W1[16][64], b1[64], W2[64][64], b2[64], w3[64], b3 */
+#define ORC_NPARAM (ORC_NF * ORC_NH + ORC_NH + ORC_NH * ORC_NH + ORC_NH + ORC_NH + 1)
+
+/* Lower-triangular pattern of A (cols <= row); returns nnz(G).  Arrays are
+ * sized by the caller: g_rp[n+1], the others nnz(A). */
+int64_t orc_fsai_pattern(const orc_op* A, int32_t* g_rp, int32_t* g_ci, int32_t* g_row,
+                         int32_t* g_aidx);
+/* 16 features per G nonzero (row-major X[nnzG][16]). */
+void orc_fsai_features(const orc_op* A, int64_t nnz_g, const int32_t* g_row, const int32_t* g_ci,
+                       const int32_t* g_aidx, float* X);
+/* MLP 16->64->64->1 (GELU) with the device's rounding points: features,
+ * W1, W2, w3 and the first hidden layer in BF16, FP64 accumulation here. */
+void orc_mlp_forward(const float* params, const float* X, int64_t N, double* out);
+/* Parameter gradient for dL/dout (same rounding points as the device:
+ * dz2 and dz1 rounded to BF16 before the weight-gradient products). */
+void orc_mlp_backward(const float* params, const float* X, int64_t N, const double* dout,
+                      double* grad);
+/* Probe estimate L = sum_v ||v - G A G^T v||^2 / (k n) and dL/dG on G's
+ * pattern.  V is k x n row-major. */
+double orc_fsai_probe_loss_grad(const orc_op* A, const orc_op* G, const double* V, int k,
+                                double* grad_g);
+
 #ifdef __cplusplus
 }
 #endif

@@ -68,6 +68,13 @@ def _declare(L):
         f.restype = C.c_int
     L.orc_true_residual.argtypes = [C.POINTER(_Op), vp, vp]
     L.orc_true_residual.restype = C.c_double
+    L.orc_fsai_pattern.argtypes = [C.POINTER(_Op), vp, vp, vp, vp]
+    L.orc_fsai_pattern.restype = C.c_int64
+    L.orc_fsai_features.argtypes = [C.POINTER(_Op), C.c_int64, vp, vp, vp, vp]
+    L.orc_mlp_forward.argtypes = [vp, vp, C.c_int64, vp]
+    L.orc_mlp_backward.argtypes = [vp, vp, C.c_int64, vp, vp]
+    L.orc_fsai_probe_loss_grad.argtypes = [C.POINTER(_Op), C.POINTER(_Op), vp, C.c_int, vp]
+    L.orc_fsai_probe_loss_grad.restype = C.c_double
 
 
 def _p(a: np.ndarray):
@@ -149,3 +156,62 @@ def true_residual(A: Csr, b, x) -> float:
     x = np.ascontiguousarray(x, dtype=np.float64)
     op = A._op()
     return float(lib().orc_true_residual(C.byref(op), _p(b), _p(x)))
+
+
+# ---- learned FSAI (no reference counterpart) ------------------------------
+NPARAM = 16 * 64 + 64 + 64 * 64 + 64 + 64 + 1
+
+
+def fsai_pattern(A: Csr):
+    """G's pattern (tril(A)): (row_ptr, col_ind, row, a_index)."""
+    nnz = int(A.row_ptr[-1])
+    rp = np.empty(A.n + 1, np.int32)
+    ci = np.empty(max(nnz, 1), np.int32)
+    row = np.empty(max(nnz, 1), np.int32)
+    aidx = np.empty(max(nnz, 1), np.int32)
+    op = A._op()
+    k = lib().orc_fsai_pattern(C.byref(op), _p(rp), _p(ci), _p(row), _p(aidx))
+    return rp, ci[:k], row[:k], aidx[:k]
+
+
+def fsai_features(A: Csr):
+    rp, ci, row, aidx = fsai_pattern(A)
+    X = np.empty((ci.shape[0], 16), np.float32)
+    op = A._op()
+    lib().orc_fsai_features(C.byref(op), ci.shape[0], _p(row), _p(ci), _p(aidx), _p(X))
+    return X, rp, ci, row
+
+
+def mlp_forward(params, X):
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    out = np.empty(X.shape[0], np.float64)
+    lib().orc_mlp_forward(_p(params), _p(X), X.shape[0], _p(out))
+    return out
+
+
+def mlp_backward(params, X, dout):
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    dout = np.ascontiguousarray(dout, dtype=np.float64)
+    g = np.empty(NPARAM, np.float64)
+    lib().orc_mlp_backward(_p(params), _p(X), X.shape[0], _p(dout), _p(g))
+    return g
+
+
+def fsai_value_map(out, row, col, diag):
+    """g_ii = softplus(o + log(e-1)) / sqrt(a_ii), g_ij = o / sqrt(a_jj)."""
+    out = np.asarray(out, np.float64)
+    s = 1.0 / np.sqrt(diag[col])
+    z = out + np.log(np.e - 1.0)
+    sp = np.where(z > 20, z, np.log1p(np.exp(np.minimum(z, 20))))
+    return np.where(row == col, sp * s, out * s)
+
+
+def fsai_probe_loss_grad(A: Csr, G: Csr, V):
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    k = V.shape[0]
+    grad = np.empty(int(G.row_ptr[-1]), np.float64)
+    opA, opG = A._op(), G._op()
+    loss = lib().orc_fsai_probe_loss_grad(C.byref(opA), C.byref(opG), _p(V), k, _p(grad))
+    return float(loss), grad
