@@ -149,8 +149,31 @@ def run_ours(args, rank, world, dev):
         info = A.cgd(b, x, tol=TOL, max_iter=args.max_iter, host_loop=args.host_loop)
         return x, info
 
-    headline = solve_plain
-    solver_name = "plain FP32 CG (drop-in cgd)"
+    def solve_jacobi(i):
+        coo, A, b = systems[i]
+        x = torch.zeros(n, device=dev)
+        info = A.cgd(b, x, tol=TOL, max_iter=args.max_iter, precond="jacobi")
+        return x, info
+
+    b64 = [s[2].double() for s in systems]
+
+    def solve_learned(i):
+        coo, A, b = systems[i]
+        fsai.attach(A)                     # network forward -> G on this system
+        x = torch.zeros(n, dtype=torch.float64, device=dev)
+        info = A.cg_mixed(b64[i], x, tol=TOL, inner_tol=args.inner_tol, max_inner=args.max_iter,
+                          precond="fsai")
+        return x, {"iters": info["inner_iters"], "outer": info["outer_iters"],
+                   "converged": info["converged"], "rel_resid": info["rel_resid"]}
+
+    if args.solver == "learned":
+        from mpsparse_b200.fsai import LearnedFsai, DEFAULT_WEIGHTS
+        fsai = LearnedFsai.load(DEFAULT_WEIGHTS)
+        headline = solve_learned
+        solver_name = "learned-FSAI mixed-precision PCG (FP32 inner PCG, FP64 outer IR)"
+    else:
+        headline = solve_plain
+        solver_name = "plain FP32 CG (drop-in cgd)"
 
     def timed(fn):
         times, infos, xs = [], [], []
@@ -168,11 +191,18 @@ def run_ours(args, rank, world, dev):
                 xs.append(x)
         return times, infos, xs
 
-    # per-handle setup (workspace, CUDA-graph capture) happens on a handle's
-    # first solve: do it for every system before the timed region
+    # per-handle setup (workspace, CUDA-graph capture, the FSAI pattern and
+    # features) happens on a handle's first solve: do it for every system
+    # before the timed region; time it on the first system
+    setup_ms = None
     for i in range(nsys):
+        t0 = time.perf_counter()
         headline(i)
+        torch.cuda.synchronize()
+        if i == 0:
+            setup_ms = (time.perf_counter() - t0) * 1e3
         solve_plain(i)
+        solve_jacobi(i)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -194,6 +224,7 @@ def run_ours(args, rank, world, dev):
     ptimes, pinfos, pxs = timed(solve_plain)
     presid = [true_residual_gpu(systems[warm + k][1].csr(), systems[warm + k][2], x)
               for k, x in enumerate(pxs)]
+    jtimes, jinfos, jxs = timed(solve_jacobi)
 
     total_ms = sum(times)
     if world > 1:
@@ -201,7 +232,12 @@ def run_ours(args, rank, world, dev):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
     iters = [i["iters"] for i in infos]
-    launches = sum(2 + 3 * it for it in iters)          # init + 3 kernels/iteration + result copy
+    if args.solver == "learned":
+        # per solve: attach (3) + sumsq + per outer step (residual + init 3 + 5/iteration +
+        # result copy + accumulate) + final residual
+        launches = sum(3 + 1 + i["outer"] * 6 + 5 * i["iters"] + 1 for i in infos)
+    else:
+        launches = sum(2 + 3 * it for it in iters)      # init + 3 kernels/iteration + result copy
 
     out = {
         "solver": solver_name,
@@ -212,15 +248,21 @@ def run_ours(args, rank, world, dev):
         "plain_cg": {"ms_per_solve": statistics.mean(ptimes),
                      "iters_mean": statistics.mean(i["iters"] for i in pinfos),
                      "true_resid_max": max(presid)},
+        "jacobi_pcg": {"ms_per_solve": statistics.mean(jtimes),
+                       "iters_mean": statistics.mean(i["iters"] for i in jinfos)},
+        "outer_mean": statistics.mean(i.get("outer", 0) for i in infos),
+        "setup_ms_first_solve": setup_ms,
         "clocks": clocks, "gpu_launches": launches, "wall_s": t_wall,
     }
-    out["e2e"] = e2e_drop_in(args, systems, dev, warm, steps)
+    out["e2e"] = e2e_drop_in(args, systems, dev, warm, steps,
+                             fsai if args.solver == "learned" else None)
     out["spmv"] = spmv_c3(args, dev) if not args.skip_spmv else None
     return out
 
 
-def e2e_drop_in(args, systems, dev, warm, steps):
-    """csr_tensor from pinned host COO + cgd with pinned host b/x, per step."""
+def e2e_drop_in(args, systems, dev, warm, steps, fsai=None):
+    """csr_tensor from pinned host COO + the solve with pinned host b/x, per
+    step (learned: attach the network factor, then cg_mixed in FP64)."""
     import torch
     import mpsparse_b200 as mps
     n = systems[0][0].n
@@ -232,24 +274,34 @@ def e2e_drop_in(args, systems, dev, warm, steps):
         coo = systems[i][0]
         keys = torch.from_numpy(coo.keys()).pin_memory()
         vals = torch.from_numpy(coo.vals).pin_memory()
-        b = systems[i][2].cpu().pin_memory()
-        x = torch.zeros(n).pin_memory()
+        if fsai is not None:
+            b = systems[i][2].cpu().double().pin_memory()
+            x = torch.zeros(n, dtype=torch.float64).pin_memory()
+        else:
+            b = systems[i][2].cpu().pin_memory()
+            x = torch.zeros(n).pin_memory()
         torch.cuda.synchronize()
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         A = mps.spmv.csr_tensor(keys, vals, e, e, e, n, n, fill_outputs=False)
-        A.cgd(b, x, tol=TOL, max_iter=args.max_iter)
+        if fsai is not None:
+            fsai.attach(A)
+            A.cg_mixed(b, x, tol=TOL, inner_tol=args.inner_tol, max_inner=args.max_iter,
+                       precond="fsai")
+        else:
+            A.cgd(b, x, tol=TOL, max_iter=args.max_iter)
         ev1.record(stream)
         torch.cuda.synchronize()
         if i >= warm:
             times.append(ev0.elapsed_time(ev1))
-            h2d = keys.numel() * 8 + vals.numel() * 4 + b.numel() * 4
-            d2h = x.numel() * 4
+            h2d = keys.numel() * 8 + vals.numel() * 4 + b.numel() * b.element_size()
+            d2h = x.numel() * x.element_size()
         del A
+    path = ("spmv.csr_tensor(pinned host COO) + attach_fsai + cg_mixed(pinned host b, x FP64)"
+            if fsai is not None else "spmv.csr_tensor(pinned host COO) + cgd(pinned host b, x)")
     return {"value": statistics.mean(times), "unit": UNIT, "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h,
-            "path": "spmv.csr_tensor(pinned host COO) + cgd(pinned host b, x)"}
+            "d2h_bytes_per_step": d2h, "path": path}
 
 
 def spmv_c3(args, dev):
@@ -343,6 +395,10 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--only-spmv", action="store_true",
                     help="only the 256^3 (or --c3-grid) SpMV measurement; for ncu captures")
+    ap.add_argument("--solver", default="learned", choices=["learned", "plain"],
+                    help="headline solver (plain: the FP32 CG drop-in)")
+    ap.add_argument("--inner-tol", type=float, default=1e-4,
+                    help="relative residual reduction of each inner FP32 PCG sweep")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive iterations from the host (kernels visible to ncu launch lists)")
     ap.add_argument("--max-iter", type=int, default=MAX_ITER,
@@ -412,13 +468,16 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_solve"],
-                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+f64" if args.solver == "learned" else "f32",
                 "data": "synthetic",
                 "config": {"workload": WORKLOAD, "solver": res["solver"], "tol": TOL,
                            "l2": "flushed between steps (256 MB write)",
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-                "iters_mean": res["iters_mean"], "true_resid_max": res["true_resid_max"],
-                "plain_cg": res["plain_cg"],
+                "iters_mean": res["iters_mean"], "outer_mean": res["outer_mean"],
+                "true_resid_max": res["true_resid_max"],
+                "setup_ms_first_solve": res["setup_ms_first_solve"],
+                "plain_cg": res["plain_cg"], "jacobi_pcg": res["jacobi_pcg"],
                 "speedup_vs_plain_cg": res["plain_cg"]["ms_per_solve"] / res["ms_per_solve"],
                 "spmv": spmv, "roofline": roof, "cpu_baseline": cpu, "e2e": res["e2e"],
                 "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]}

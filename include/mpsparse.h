@@ -53,8 +53,9 @@ typedef struct {
     double tol;               /* relative residual ||r||/||b|| target (0: 1e-6) */
     double omega;             /* Richardson weight (0: 0.01) */
     int32_t precond;          /* MPS_PRECOND_* (CG only) */
-    int32_t stall_window;     /* FSAI: fall back to Jacobi when ||r|| has not
-                                 dropped by 2x over this many iterations (0: 200) */
+    int32_t stall_window;     /* FSAI: fall back to Jacobi when the preconditioned
+                                 residual r.z has not dropped 4x within this many
+                                 iterations (0: 400) */
     int32_t host_loop;        /* 0: the whole iteration loop is one CUDA-graph
                                  launch with a device-side WHILE condition;
                                  1: the host launches the same kernels and polls

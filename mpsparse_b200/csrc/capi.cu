@@ -98,7 +98,7 @@ void mps_solve_opts_default(mps_solve_opts* o) {
     o->tol = 1e-6;
     o->max_iter = 2000;
     o->omega = 0.01;
-    o->stall_window = 200;
+    o->stall_window = 400;
 }
 
 const char* mps_last_error_string(void) { return g_last_error.c_str(); }
@@ -269,7 +269,13 @@ static mps_status csr_solve(SolverKind kind, mps_csr* h, const float* b, float* 
     CsrOp op{&h->A, nullptr};
     CsrOp g{&h->G, nullptr}, gt{&h->Gt, nullptr};
     PrecondOps<CsrOp> pc{h->has_fsai ? &g : nullptr, h->has_fsai ? &gt : nullptr};
-    return run_solve(kind, op, pc, h->H, b, x, o, info, s);
+    MPS_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), s));
+    st = run_solve(kind, op, pc, h->H, b, x, o, info, s);
+    unsigned err = 0;
+    MPS_CUDA(cudaMemcpy(&err, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (st == MPS_OK && (err & kErrTimeout))
+        return fail(MPS_ERR_TIMEOUT, "SpMV: a bulk-copy wait gave up");
+    return st;
 }
 
 mps_status mps_csr_cg(mps_csr* h, const float* b, float* x, const mps_solve_opts* o,
@@ -382,6 +388,7 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
     io.precond = o.precond;
     mps_status st = prepare_precond(h, &io, s);
     if (st != MPS_OK) return st;
+    MPS_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), s));
     SolverHost& H = h->H;
     const int n = (int)h->A.n_rows;
     if (bf16 && !h->vb) {
@@ -431,6 +438,12 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
         if (ii.iters == 0) break;
     }
     cudaFreeAsync(scal, s);
+    {
+        unsigned err = 0;
+        MPS_CUDA(cudaMemcpy(&err, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        if (st == MPS_OK && (err & kErrTimeout))
+            st = fail(MPS_ERR_TIMEOUT, "SpMV: a bulk-copy wait gave up");
+    }
     if (info) {
         info->outer_iters = outer;
         info->inner_iters = inner_total;

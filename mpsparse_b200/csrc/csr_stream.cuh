@@ -16,11 +16,19 @@
 // more rows than the staged row_ptr holds) are reduced straight from global
 // memory.  The handle's CSR arrays carry 16 spare elements so a copy rounded
 // out to 16-byte boundaries never leaves its allocation.
+//
+// Three buffers per CTA: a tile's copy is issued two tiles ahead, right after
+// the barrier that ends the product phase of the current tile (by then every
+// thread has finished the tile that last used that buffer), so each tile needs
+// a single block barrier.  col_ind/values are copied with an L2 evict-first
+// policy so that x, gathered by every tile, stays resident in L2.
 #pragma once
 #include "spmv_kernels.cuh"
 #include "tma.cuh"
 
 namespace mps {
+
+constexpr int kStreamStages = 3;
 
 template <bool BF16>
 __host__ __device__ constexpr size_t stream_buf_bytes(int cap, int rcap) {
@@ -31,7 +39,9 @@ template <bool BF16, class Epi, int NT = kNT>
 __global__ void __launch_bounds__(NT, 4)
 spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ unsigned long long bar[2];
+    constexpr int NB = kStreamStages;
+    __shared__ unsigned long long bar[NB];
+    __shared__ int4 s_meta[NB];
     __shared__ double red[NT / 32];
     __shared__ float redf[NT / 32];
     __shared__ int last_flag;
@@ -44,12 +54,11 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
     constexpr int GA = BF16 ? 8 : 4;   // elements per 16 bytes of the value array
     const size_t bb = stream_buf_bytes<BF16>(A.cap, A.rcap);
     if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+#pragma unroll
+        for (int i = 0; i < NB; ++i) mbar_init(&bar[i], 1);
         timed_out = 0;
         fence_mbar_init();
     }
-    __syncthreads();
     double acc[Epi::NS > 0 ? Epi::NS : 1];
 #pragma unroll
     for (int i = 0; i < (Epi::NS > 0 ? Epi::NS : 1); ++i) acc[i] = 0.0;
@@ -59,6 +68,7 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
         const int r0 = m.x & ~3, r1 = (m.y + 1 + 3) & ~3;
         return m.w > m.z && (a1 - a0) <= A.cap && (r1 - r0) <= A.rcap;
     };
+    uint64_t pol = 0;
     auto issue = [&](const int4 m, int b) {   // one thread
         const int a0 = m.z & ~(GA - 1), a1 = (m.w + GA - 1) & ~(GA - 1);
         const int r0 = m.x & ~3, r1 = (m.y + 1 + 3) & ~3;
@@ -68,73 +78,88 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
         unsigned char* base = smem + (size_t)b * bb;
         fence_proxy_async();
         mbar_expect_tx(&bar[b], bc + bv + br);
-        bulk_g2s(base, A.ci + a0, bc, &bar[b]);
+        bulk_g2s_hint(base, A.ci + a0, bc, &bar[b], pol);
         if (BF16)
-            bulk_g2s(base + (size_t)A.cap * 4, A.vb + a0, bv, &bar[b]);
+            bulk_g2s_hint(base + (size_t)A.cap * 4, A.vb + a0, bv, &bar[b], pol);
         else
-            bulk_g2s(base + (size_t)A.cap * 4, A.v + a0, bv, &bar[b]);
+            bulk_g2s_hint(base + (size_t)A.cap * 4, A.v + a0, bv, &bar[b], pol);
         bulk_g2s(base + (size_t)A.cap * (BF16 ? 6 : 8), A.rp + r0, br, &bar[b]);
     };
 
-    unsigned uses0 = 0u, uses1 = 0u;   // completed phases per buffer (uniform)
-    // Tile metadata: thread 0 keeps the next two tiles' {rs, re, k0, k1} in
-    // registers (loaded two iterations ahead) and publishes the upcoming
-    // tile's through shared memory, so no thread waits on a metadata load.
-    __shared__ int4 s_meta[2];
+    // Thread 0 keeps the metadata of the next tiles in registers (loaded
+    // ahead) and publishes each tile's through shared memory two tiles ahead.
     const int4 none = make_int4(0, 0, 0, 0);
     const int t0 = blockIdx.x, G = gridDim.x;
-    int4 m_next = none, m_next2 = none;
-    if (threadIdx.x == 0 && t0 < A.ntiles) {
-        const int4 m0 = A.meta[t0];
-        m_next = t0 + G < A.ntiles ? A.meta[t0 + G] : none;
-        m_next2 = t0 + 2 * G < A.ntiles ? A.meta[t0 + 2 * G] : none;
-        if (staged(m0)) issue(m0, 0);
-        s_meta[0] = m0;
+    int4 m_ahead = none;           // metadata of tile it + 2 (issued next)
+    int4 m_ahead2 = none;          // tile it + 3
+    if (threadIdx.x == 0) {
+        pol = policy_evict_first();
+        for (int i = 0; i < NB - 1; ++i) {
+            const int ti = t0 + i * G;
+            const int4 mi = ti < A.ntiles ? A.meta[ti] : none;
+            if (ti < A.ntiles && staged(mi)) issue(mi, i);
+            s_meta[i] = mi;
+        }
+        m_ahead = t0 + 2 * G < A.ntiles ? A.meta[t0 + 2 * G] : none;
+        m_ahead2 = t0 + 3 * G < A.ntiles ? A.meta[t0 + 3 * G] : none;
     }
     __syncthreads();
+    unsigned phase_bits = 0u;      // completed-phase parity per buffer (uniform)
     int it = 0;
     for (int t = t0; t < A.ntiles; t += G, ++it) {
-        const int b = it & 1;
-        if (threadIdx.x == 0 && t + G < A.ntiles && staged(m_next)) issue(m_next, b ^ 1);
+        const int b = it % NB;
         const int4 m = s_meta[b];
         const int rs = m.x, re = m.y, k0 = m.z, k1 = m.w;
+        const bool stg = rs < re && staged(m);
+        unsigned char* base = smem + (size_t)b * bb;
+        const int a0 = k0 & ~(GA - 1), r0 = rs & ~3;
+        if (stg) {
+            const unsigned par = (phase_bits >> b) & 1u;
+            if (!mbar_wait_bounded(&bar[b], par)) {
+                atomicOr(A.err, kErrTimeout);
+                timed_out = 1 + (b << 1) + (par << 3);
+            }
+            phase_bits ^= 1u << b;
+            const int* cols = reinterpret_cast<const int*>(base);
+            float* prod = reinterpret_cast<float*>(base);
+            // products: U independent gathers in flight per thread (the staged
+            // col_ind is overwritten by the products, so all loads of a round
+            // are issued before any store)
+            constexpr int U = 8;
+            for (int kb = k0 + threadIdx.x; kb < k1; kb += NT * U) {
+                int c[U];
+                float v[U], xv[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int i = kb + u * NT - a0;
+                    const bool in = kb + u * NT < k1;
+                    c[u] = in ? cols[i] : -1;
+                    if (BF16)
+                        v[u] = in ? bf16_to_f(reinterpret_cast<const __nv_bfloat16*>(base + (size_t)A.cap * 4)[i]) : 0.f;
+                    else
+                        v[u] = in ? reinterpret_cast<const float*>(base + (size_t)A.cap * 4)[i] : 0.f;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : 0.f;
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (kb + u * NT < k1) prod[kb + u * NT - a0] = v[u] * xv[u];
+            }
+        }
+        // Products visible; every thread is past tile it - 1, so the buffer of
+        // tile it + 2 (the one tile it - 1 used) can be refilled.
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int b2 = (it + 2) % NB;
+            if (t + 2 * G < A.ntiles && staged(m_ahead)) issue(m_ahead, b2);
+            s_meta[b2] = m_ahead;
+            m_ahead = m_ahead2;
+            m_ahead2 = t + 4 * G < A.ntiles ? A.meta[t + 4 * G] : none;
+        }
         if (rs < re) {
-            if (staged(m)) {
-                const unsigned par = (b ? uses1 : uses0) & 1u;
-                if (!mbar_wait_bounded(&bar[b], par)) {
-                    atomicOr(A.err, kErrTimeout);
-                    timed_out = 1 + (b << 1) + (par << 2);
-                }
-                if (b) ++uses1; else ++uses0;
-                unsigned char* base = smem + (size_t)b * bb;
-                const int* cols = reinterpret_cast<const int*>(base);
-                float* prod = reinterpret_cast<float*>(base);
+            if (stg) {
+                const float* prod = reinterpret_cast<const float*>(base);
                 const int* rps = reinterpret_cast<const int*>(base + (size_t)A.cap * (BF16 ? 6 : 8));
-                const int a0 = k0 & ~(GA - 1), r0 = rs & ~3;
-                // products: U independent gathers in flight per thread (the
-                // staged col_ind is overwritten by the products, so all loads
-                // of a round are issued before any store)
-                constexpr int U = 8;
-                for (int kb = k0 + threadIdx.x; kb < k1; kb += NT * U) {
-                    int c[U];
-                    float v[U], xv[U];
-#pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        const int i = kb + u * NT - a0;
-                        const bool in = kb + u * NT < k1;
-                        c[u] = in ? cols[i] : -1;
-                        if (BF16)
-                            v[u] = in ? bf16_to_f(reinterpret_cast<const __nv_bfloat16*>(base + (size_t)A.cap * 4)[i]) : 0.f;
-                        else
-                            v[u] = in ? reinterpret_cast<const float*>(base + (size_t)A.cap * 4)[i] : 0.f;
-                    }
-#pragma unroll
-                    for (int u = 0; u < U; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : 0.f;
-#pragma unroll
-                    for (int u = 0; u < U; ++u)
-                        if (kb + u * NT < k1) prod[kb + u * NT - a0] = v[u] * xv[u];
-                }
-                __syncthreads();
                 const int nrows = re - rs;
                 if ((k1 - k0) > 16 * nrows) {
                     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -179,15 +204,10 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
                 }
             }
         }
-        if (threadIdx.x == 0) {
-            s_meta[b ^ 1] = m_next;
-            m_next = m_next2;
-            m_next2 = t + 3 * G < A.ntiles ? A.meta[t + 3 * G] : none;
-        }
-        __syncthreads();   // buffer b is refilled by the next iteration's prefetch
     }
+    __syncthreads();
     if (threadIdx.x == 0 && timed_out) {   // a copy whose wait ran out: wait again, bounded
-        mbar_wait_bounded(&bar[(timed_out >> 1) & 1], (unsigned)(timed_out >> 2) & 1u);
+        mbar_wait_bounded(&bar[(timed_out >> 1) & 3], (unsigned)(timed_out >> 3) & 1u);
     }
     if constexpr (Epi::NS > 0) {
 #pragma unroll

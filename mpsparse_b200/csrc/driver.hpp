@@ -40,12 +40,12 @@ struct CsrOp {
     cudaError_t apply(const float* x, const Epi& e, cudaStream_t s) const {
         const CsrStreamDev v = A->stream_view(vb);
         if (vb) {
-            const size_t smem = 2 * stream_buf_bytes<true>(v.cap, v.rcap);
+            const size_t smem = kStreamStages * stream_buf_bytes<true>(v.cap, v.rcap);
             smem_optin_k(spmv_stream<true, Epi>, smem);
             const int g = persistent_grid(spmv_stream<true, Epi>, smem, v.ntiles);
             spmv_stream<true, Epi><<<g, kNT, smem, s>>>(v, x, e);
         } else {
-            const size_t smem = 2 * stream_buf_bytes<false>(v.cap, v.rcap);
+            const size_t smem = kStreamStages * stream_buf_bytes<false>(v.cap, v.rcap);
             smem_optin_k(spmv_stream<false, Epi>, smem);
             const int g = persistent_grid(spmv_stream<false, Epi>, smem, v.ntiles);
             spmv_stream<false, Epi><<<g, kNT, smem, s>>>(v, x, e);
@@ -282,7 +282,7 @@ mps_status run_solve(SolverKind kind, const Op& op, const PrecondOps<Op>& pc, So
     P.max_iter = o.max_iter > 0 ? o.max_iter : 2000;
     P.compat = o.reference_compat ? 1 : 0;
     P.precond = kind == kCG && !P.compat ? o.precond : 0;
-    P.stall_window = o.stall_window > 0 ? o.stall_window : 200;
+    P.stall_window = o.stall_window > 0 ? o.stall_window : 400;
     const int precond = P.precond;
     MPS_CUDA(cudaMemcpyAsync(H.ws.d_params, H.h_params, sizeof(SolveParams), cudaMemcpyHostToDevice, s));
     MPS_CUDA(cudaMemcpyAsync(H.v(vB), d_b, (size_t)H.n * sizeof(float), cudaMemcpyDeviceToDevice, s));

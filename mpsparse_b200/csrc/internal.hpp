@@ -31,6 +31,7 @@ struct DevScalars {
     double rho, rho_old, omega, sigma, phi1, phi2, rnorm2;
     double bnorm2, tol2, staged, best_rr;
     double omega_rich;
+    double rz_jac;      // r . D^-1 r of the last update (Jacobi fallback)
     // control
     int iter, max_iter, done, converged, breakdown, stalled, snapshot, compat;
     int mode;           // preconditioner in force: 0 none, 1 Jacobi, 2 FSAI

@@ -119,9 +119,10 @@ cg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restrict
     s->rr = bb;
     s->rz = (mode == 1) ? tot[1] : bb;
     s->tol2 = prm->tol * prm->tol * bb;
-    s->best_rr = bb;
+    s->best_rr = 1e300;
     s->best_iter = 0;
     s->beta = 0.0;
+    s->rz_jac = 0.0;
     s->guard = 0;
     s->guard_limit = s->max_iter + 8;
     if (!isfinite(bb)) {
@@ -198,18 +199,7 @@ static __device__ void cg_finalize_xr(DevScalars* s, double rr_new, double rz_ja
         s->done = 1;
         return;
     }
-    if (s->mode == 2) {   // stall watch of the learned preconditioner
-        if (rr_new < 0.25 * s->best_rr) {
-            s->best_rr = rr_new;
-            s->best_iter = it;
-        } else if (it - s->best_iter >= s->stall_window) {
-            s->mode = 1;          // fall back to Jacobi and restart the direction
-            s->stalled = 1;
-            s->restart = 1;
-            s->best_iter = it;
-            s->best_rr = rr_new;
-        }
-    }
+    s->rz_jac = rz_jac;
     if (s->mode == 1) {
         s->beta = s->restart ? 0.0 : rz_jac / s->rz;
         s->rz = rz_jac;
@@ -276,6 +266,23 @@ struct EpiFsai1 {
     }
     __device__ void finalize(const double* tot) const {
         const double rz = tot[0];
+        // Stall watch on the preconditioned residual r . G^T G r: when it has
+        // not dropped 4x within stall_window iterations, fall back to Jacobi
+        // (restart the direction from z = D^-1 r).
+        const int it = sc->iter;
+        if (!sc->restart && sc->stall_window > 0) {
+            if (rz < 0.25 * sc->best_rr) {
+                sc->best_rr = rz;
+                sc->best_iter = it;
+            } else if (it - sc->best_iter >= sc->stall_window) {
+                sc->mode = 1;
+                sc->stalled = 1;
+                sc->beta = 0.0;
+                sc->rz = sc->rz_jac;
+                sc->restart = 0;
+                return;
+            }
+        }
         sc->beta = sc->restart ? 0.0 : rz / sc->rz;
         sc->rz = rz;
         sc->restart = 0;

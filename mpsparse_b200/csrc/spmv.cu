@@ -102,7 +102,7 @@ cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s) {
     const int cap_grid = num_sms() * 8;
     p.grid = p.ntiles < cap_grid ? p.ntiles : cap_grid;
     if (p.grid < 1) p.grid = 1;
-    p.cap_s = (tile_nnz + 256 + 7) & ~7;
+    p.cap_s = (tile_nnz + 128 + 7) & ~7;
     p.rcap = 520;
     p.grid_s = p.ntiles < num_sms() * 6 ? p.ntiles : num_sms() * 6;
     if (p.grid_s < 1) p.grid_s = 1;

@@ -502,25 +502,25 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
              },
              py::arg("b"), py::arg("x"), py::arg("tol") = 1e-6, py::arg("max_iter") = 2000,
              py::arg("precond") = "none", py::arg("reference_compat") = false,
-             py::arg("host_loop") = false, py::arg("stall_window") = 200)
+             py::arg("host_loop") = false, py::arg("stall_window") = 400)
         .def("iter_solve",
              [](CsrTensor& t, torch::Tensor b, torch::Tensor x, double tol, int64_t max_iter,
                 const std::string& precond, bool compat) {
-                 return t.solve(0, b, x, tol, max_iter, 0.01, precond, compat, false, 200);
+                 return t.solve(0, b, x, tol, max_iter, 0.01, precond, compat, false, 400);
              },
              py::arg("b"), py::arg("x"), py::arg("tol") = 1e-6, py::arg("max_iter") = 2000,
              py::arg("precond") = "none", py::arg("reference_compat") = false)
         .def("bicgstab",
              [](CsrTensor& t, torch::Tensor b, torch::Tensor x, double tol, int64_t max_iter,
                 bool compat, bool host_loop) {
-                 return t.solve(1, b, x, tol, max_iter, 0.01, "none", compat, host_loop, 200);
+                 return t.solve(1, b, x, tol, max_iter, 0.01, "none", compat, host_loop, 400);
              },
              py::arg("b"), py::arg("x"), py::arg("tol") = 1e-6, py::arg("max_iter") = 2000,
              py::arg("reference_compat") = false, py::arg("host_loop") = false)
         .def("richardson",
              [](CsrTensor& t, torch::Tensor b, torch::Tensor x, double omega, int64_t iters,
                 double tol, bool compat, bool host_loop) {
-                 return t.solve(2, b, x, tol, iters, omega, "none", compat, host_loop, 200);
+                 return t.solve(2, b, x, tol, iters, omega, "none", compat, host_loop, 400);
              },
              py::arg("b"), py::arg("x"), py::arg("omega") = 0.01, py::arg("iters") = 1000,
              py::arg("tol") = 0.0, py::arg("reference_compat") = false,

@@ -227,3 +227,43 @@ def diffusion_256cubed(seed: int = 0) -> Coo:
 def diffusion_512sq(seed: int) -> Coo:
     """2D 5-point log-normal diffusion, 512^2 cells, sigma 1.5, corr length 16."""
     return lognormal_diffusion_2d(512, 512, 1.5, 16.0, seed)
+
+
+def lognormal_diffusion_2d_torch(nx: int, ny: int, sigma: float, corr_len: float, seed: int,
+                                 device="cuda"):
+    """Same operator as ``lognormal_diffusion_2d`` (same seed -> same white
+    noise from numpy), with the FFT filter and the assembly done by torch on
+    ``device``.  Returns (keys int64, values float32, n) tensors on ``device``."""
+    import torch
+
+    w = np.random.default_rng(seed).standard_normal((ny, nx))
+    wt = torch.from_numpy(w).to(device)
+    fw = torch.fft.rfftn(wt)
+    fy = torch.fft.fftfreq(ny, device=device, dtype=torch.float64)
+    fx = torch.fft.rfftfreq(nx, device=device, dtype=torch.float64)
+    k2 = (2 * np.pi * fy)[:, None] ** 2 + (2 * np.pi * fx)[None, :] ** 2
+    g = torch.fft.irfftn(fw * torch.exp(-0.5 * k2 * corr_len ** 2), s=(ny, nx))
+    g = g - g.mean()
+    sd = g.std(unbiased=False)
+    g = g * (sigma / sd)
+    k = torch.exp(g)
+    n = nx * ny
+    idx = torch.arange(n, device=device, dtype=torch.int64).reshape(ny, nx)
+    diag = torch.zeros((ny, nx), device=device, dtype=torch.float64)
+    ky = torch.sqrt(k[:-1, :] * k[1:, :])                 # faces between rows j, j+1
+    diag[:-1, :] += ky
+    diag[1:, :] += ky
+    diag[0, :] += k[0, :]
+    diag[-1, :] += k[-1, :]
+    kx = torch.sqrt(k[:, :-1] * k[:, 1:])                 # faces between columns i, i+1
+    diag[:, :-1] += kx
+    diag[:, 1:] += kx
+    diag[:, 0] += k[:, 0]
+    diag[:, -1] += k[:, -1]
+    a_y, b_y = idx[:-1, :].reshape(-1), idx[1:, :].reshape(-1)
+    a_x, b_x = idx[:, :-1].reshape(-1), idx[:, 1:].reshape(-1)
+    rows = torch.cat([idx.reshape(-1), a_y, b_y, a_x, b_x])
+    cols = torch.cat([idx.reshape(-1), b_y, a_y, b_x, a_x])
+    vals = torch.cat([diag.reshape(-1), -ky.reshape(-1), -ky.reshape(-1), -kx.reshape(-1),
+                      -kx.reshape(-1)]).to(torch.float32)
+    return (rows << 32) | cols, vals, n
