@@ -221,6 +221,38 @@ mps_status mps_fsai_mlp_backward(const mps_fsai_model* m, const float* d_X, cons
 mps_status mps_fsai_probe_grad(mps_csr* A, const float* d_V, int32_t k, float* d_grad_g,
                                double* loss, cudaStream_t stream);
 
+/* ---- Batched solve ------------------------------------------------------ */
+
+/* Thousands of independent SPD systems solved by PCG in one persistent,
+ * CUDA-graph-captured launch.  The systems are stacked into one block-diagonal
+ * CSR (global row and column indices); system s owns rows
+ * [h_row_off[s], h_row_off[s+1]).  Groups of warps take systems from a queue
+ * ordered largest-first and iterate each to convergence with group-level
+ * barriers only.  No reference counterpart. */
+typedef struct mps_batch mps_batch;
+mps_status mps_batch_create(const int32_t* d_row_ptr, const int32_t* d_col_ind,
+                            const float* d_vals, uint64_t nnz, uint32_t total_rows,
+                            const int32_t* h_row_off, int32_t n_systems, mps_batch** out,
+                            cudaStream_t stream);
+mps_status mps_batch_destroy(mps_batch* B);
+/* Build the learned factor on the whole block-diagonal matrix. */
+mps_status mps_batch_attach_fsai(mps_batch* B, const mps_fsai_model* m, cudaStream_t stream);
+/* Per system: MPS_PRECOND_NONE / JACOBI (default) / FSAI, or MPS_BATCH_SKIP
+ * (the system is not solved: x untouched, iters 0, converged 0, relres -1). */
+#define MPS_BATCH_SKIP 3
+mps_status mps_batch_set_precond(mps_batch* B, const int8_t* h_kind);
+/* Autotuner: time the candidate warps-per-system (1, 2, 4, 8, 16) on a sample
+ * spanning the batch's sizes and keep the fastest (h_ms: 5 timings, may be
+ * NULL). */
+mps_status mps_batch_autotune(mps_batch* B, const float* d_b, double tol, int32_t max_iter,
+                              int32_t* h_chosen_wps, float* h_ms, cudaStream_t stream);
+int32_t mps_batch_warps_per_system(const mps_batch* B);
+/* Solve all systems: per-system iteration count, converged flag (the
+ * convergence mask) and recurrence relative residual. */
+mps_status mps_batch_cg(mps_batch* B, const float* d_b, float* d_x, double tol, int32_t max_iter,
+                        int32_t* d_iters, int32_t* d_converged, float* d_relres,
+                        cudaStream_t stream);
+
 /* ---- BCSR --------------------------------------------------------------- */
 
 /* BCSR from pre-built block arrays: row-major B x B blocks (B = 4 or 8),

@@ -1,0 +1,475 @@
+// batched.cu -- thousands of independent SPD systems in one persistent launch.
+//
+// The systems are stacked into one block-diagonal CSR (global row and column
+// indices; system s owns rows [row_off[s], row_off[s+1])).  A persistent
+// kernel of 512-thread CTAs splits each CTA into groups of WPS warps; every
+// group takes the next system from a queue ordered largest-first (longest
+// processing time first, so the big systems do not finish last) and runs PCG
+// on it to convergence with group-level barriers only (named barriers, or
+// __syncwarp when a group is one warp): no grid-wide synchronisation, no host
+// round trip.  Per system: preconditioner none / Jacobi / learned FSAI (with
+// the same stall watch and Jacobi fallback as the single-system solver), and a
+// convergence record (iterations, converged flag, relative residual) -- the
+// per-system convergence mask.  WPS (warps per system, hence rows per warp)
+// is chosen by the autotuner, which times candidate launches on a sample of
+// the batch.  No reference counterpart (the reference solves one system per
+// call).
+#include <algorithm>
+#include <chrono>
+#include <numeric>
+#include <vector>
+
+#include "handles.hpp"
+
+namespace mps {
+namespace {
+
+constexpr int kBatchNT = 512;
+
+struct BatchDev {
+    const int* rp;
+    const int* ci;
+    const float* v;
+    const int* grp;       // G (learned factor), may be null
+    const int* gci;
+    const float* gv;
+    const int* gtrp;      // G^T
+    const int* gtci;
+    const float* gtv;
+    const float* dinv;
+    const int* row_off;   // n_sys + 1
+    const int* order;     // queue order (largest first)
+    const signed char* kind;   // per system: 0 none, 1 Jacobi, 2 FSAI, 3 skip
+    int n_sys;            // systems in the queue
+    float* r;
+    float* p;
+    float* q;
+    float* w;
+};
+
+struct BatchOut {
+    int* iters;
+    int* converged;
+    float* relres;
+};
+
+template <int WPS>
+__device__ __forceinline__ void group_sync(int g) {
+    if (WPS == 1) {
+        __syncwarp();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(WPS * 32) : "memory");
+    }
+}
+
+// Sum NS doubles over the group (fixed order: every thread gets the same bits).
+template <int WPS, int NS>
+__device__ __forceinline__ void group_reduce(double* v, double (*red)[4], int g, int lt) {
+#pragma unroll
+    for (int i = 0; i < NS; ++i) v[i] = warp_sum(v[i]);
+    const int w = lt >> 5;
+    if ((lt & 31) == 0)
+#pragma unroll
+        for (int i = 0; i < NS; ++i) red[w][i] = v[i];
+    group_sync<WPS>(g);
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < WPS; ++k) s += red[k][i];
+        v[i] = s;
+    }
+    group_sync<WPS>(g);
+}
+
+__device__ __forceinline__ float row_dot(const int* __restrict__ rp, const int* __restrict__ ci,
+                                         const float* __restrict__ v, const float* __restrict__ x,
+                                         int r) {
+    float s = 0.f;
+    const int e = rp[r + 1];
+    for (int k = rp[r]; k < e; ++k) s = fmaf(v[k], x[ci[k]], s);
+    return s;
+}
+
+template <int WPS>
+__global__ void __launch_bounds__(kBatchNT)
+batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchOut out, double tol,
+          int max_iter, int stall_window, unsigned* queue) {
+    constexpr int GS = WPS * 32;
+    constexpr int NG = kBatchNT / GS;
+    __shared__ double red[NG][WPS][4];
+    __shared__ int s_next[NG];
+    const int g = threadIdx.x / GS, lt = threadIdx.x % GS;
+    for (;;) {
+        if (lt == 0) s_next[g] = (int)atomicAdd(queue, 1u);
+        group_sync<WPS>(g);
+        const int qi = s_next[g];
+        group_sync<WPS>(g);
+        if (qi >= B.n_sys) break;
+        const int sys = B.order[qi];
+        const int lo = B.row_off[sys], hi = B.row_off[sys + 1];
+        int mode = B.kind[sys];
+        if (mode == 3) {                          // masked out: x untouched
+            if (lt == 0) {
+                out.iters[sys] = 0;
+                out.converged[sys] = 0;
+                out.relres[sys] = -1.f;
+            }
+            continue;
+        }
+        // init: x = 0, r = b, p = M b
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int i = lo + lt; i < hi; i += GS) {
+            const float bi = b[i];
+            x[i] = 0.f;
+            B.r[i] = bi;
+            const float z = mode == 1 ? bi * B.dinv[i] : bi;
+            if (mode != 2) B.p[i] = z;
+            acc[0] += (double)bi * bi;
+            acc[1] += (double)bi * z;
+        }
+        group_reduce<WPS, 2>(acc, red[g], g, lt);
+        const double bb = acc[0];
+        double rz = acc[1], rr = bb;
+        const double thresh = tol * tol * bb;
+        int it = 0, conv = bb == 0.0, best_it = 0;
+        double best = 1e300;
+        if (!conv && mode == 2) {                 // p = G^T G b
+            double a2[1] = {0.0};
+            for (int i = lo + lt; i < hi; i += GS) {
+                const float wi = row_dot(B.grp, B.gci, B.gv, B.r, i);
+                B.w[i] = wi;
+                a2[0] += (double)wi * wi;
+            }
+            group_reduce<WPS, 1>(a2, red[g], g, lt);
+            rz = a2[0];
+            for (int i = lo + lt; i < hi; i += GS) B.p[i] = row_dot(B.gtrp, B.gtci, B.gtv, B.w, i);
+            group_sync<WPS>(g);
+        }
+        while (!conv && it < max_iter) {
+            double a[1] = {0.0};
+            for (int i = lo + lt; i < hi; i += GS) {
+                const float qv = row_dot(B.rp, B.ci, B.v, B.p, i);
+                B.q[i] = qv;
+                a[0] += (double)B.p[i] * qv;
+            }
+            group_reduce<WPS, 1>(a, red[g], g, lt);
+            if (!(a[0] > 0.0)) break;             // breakdown (not SPD)
+            const float alpha = (float)(rz / a[0]);
+            double c[2] = {0.0, 0.0};
+            for (int i = lo + lt; i < hi; i += GS) {
+                x[i] = fmaf(alpha, B.p[i], x[i]);
+                const float ri = fmaf(-alpha, B.q[i], B.r[i]);
+                B.r[i] = ri;
+                c[0] += (double)ri * ri;
+                c[1] += (double)ri * ri * B.dinv[i];
+            }
+            group_reduce<WPS, 2>(c, red[g], g, lt);
+            ++it;
+            rr = c[0];
+            if (rr <= thresh) {
+                conv = 1;
+                break;
+            }
+            double beta;
+            if (mode == 2) {
+                double d[1] = {0.0};
+                for (int i = lo + lt; i < hi; i += GS) {
+                    const float wi = row_dot(B.grp, B.gci, B.gv, B.r, i);
+                    B.w[i] = wi;
+                    d[0] += (double)wi * wi;
+                }
+                group_reduce<WPS, 1>(d, red[g], g, lt);
+                if (stall_window > 0 && !(d[0] < 0.25 * best) && it - best_it >= stall_window) {
+                    mode = 1;                     // stalled: Jacobi from here, restart p
+                    rz = c[1];
+                    for (int i = lo + lt; i < hi; i += GS) B.p[i] = B.r[i] * B.dinv[i];
+                    group_sync<WPS>(g);
+                    continue;
+                }
+                if (d[0] < 0.25 * best) {
+                    best = d[0];
+                    best_it = it;
+                }
+                beta = d[0] / rz;
+                rz = d[0];
+                const float bf = (float)beta;
+                for (int i = lo + lt; i < hi; i += GS)
+                    B.p[i] = fmaf(bf, B.p[i], row_dot(B.gtrp, B.gtci, B.gtv, B.w, i));
+            } else {
+                const double rzn = mode == 1 ? c[1] : c[0];
+                beta = rzn / rz;
+                rz = rzn;
+                const float bf = (float)beta;
+                for (int i = lo + lt; i < hi; i += GS) {
+                    const float z = mode == 1 ? B.r[i] * B.dinv[i] : B.r[i];
+                    B.p[i] = fmaf(bf, B.p[i], z);
+                }
+            }
+            group_sync<WPS>(g);
+        }
+        if (lt == 0) {
+            out.iters[sys] = it;
+            out.converged[sys] = conv;
+            out.relres[sys] = bb > 0.0 ? (float)sqrt(rr / bb) : 0.f;
+        }
+    }
+}
+
+using BatchKernel = void (*)(BatchDev, const float*, float*, BatchOut, double, int, int, unsigned*);
+
+BatchKernel batch_kernel(int wps) {
+    switch (wps) {
+        case 1: return batch_pcg<1>;
+        case 2: return batch_pcg<2>;
+        case 4: return batch_pcg<4>;
+        case 8: return batch_pcg<8>;
+        default: return batch_pcg<16>;
+    }
+}
+
+}  // namespace
+}  // namespace mps
+
+using namespace mps;
+
+struct mps_batch {
+    mps_csr* A = nullptr;          // the block-diagonal matrix (owns G/G^T/diagonal)
+    int n_sys = 0;
+    std::vector<int> row_off;      // host copy
+    int* d_row_off = nullptr;
+    int* d_order = nullptr;
+    int* d_sample_order = nullptr;
+    int n_sample = 0;
+    signed char* d_kind = nullptr;
+    float* d_work = nullptr;       // r, p, q, w
+    unsigned* d_queue = nullptr;
+    int wps = 4;
+    // one-launch graph of the last call: [queue reset, persistent kernel]
+    cudaGraphExec_t exec = nullptr;
+    const void* exec_key[5] = {};
+    int exec_wps = 0;
+    double exec_tol = -1.0;
+    int exec_max_iter = -1;
+    cudaStream_t cap = nullptr;
+};
+
+static BatchDev batch_view(mps_batch* B, bool sample) {
+    mps_csr* h = B->A;
+    const size_t n = h->A.n_rows;
+    BatchDev d{};
+    d.rp = h->A.rp;
+    d.ci = h->A.ci;
+    d.v = h->A.v;
+    if (h->has_fsai) {
+        d.grp = h->G.rp;
+        d.gci = h->G.ci;
+        d.gv = h->G.v;
+        d.gtrp = h->Gt.rp;
+        d.gtci = h->Gt.ci;
+        d.gtv = h->Gt.v;
+    }
+    d.dinv = h->H.dinv;
+    d.row_off = B->d_row_off;
+    d.order = sample ? B->d_sample_order : B->d_order;
+    d.kind = B->d_kind;
+    d.n_sys = sample ? B->n_sample : B->n_sys;
+    d.r = B->d_work;
+    d.p = B->d_work + (n + 4);
+    d.q = B->d_work + 2 * (n + 4);
+    d.w = B->d_work + 3 * (n + 4);
+    return d;
+}
+
+static mps_status batch_launch(mps_batch* B, int wps, bool sample, const float* b, float* x,
+                               double tol, int max_iter, int stall_window, BatchOut out,
+                               cudaStream_t s) {
+    BatchKernel k = batch_kernel(wps);
+    int per_sm = resident_ctas(reinterpret_cast<const void*>(k), kBatchNT, 0);
+    const int grid = num_sms() * (per_sm > 0 ? per_sm : 1);
+    MPS_CUDA(cudaMemsetAsync(B->d_queue, 0, sizeof(unsigned), s));
+    k<<<grid, kBatchNT, 0, s>>>(batch_view(B, sample), b, x, out, tol, max_iter, stall_window, B->d_queue);
+    MPS_CUDA(cudaGetLastError());
+    return MPS_OK;
+}
+
+extern "C" {
+
+mps_status mps_batch_create(const int32_t* d_row_ptr, const int32_t* d_col_ind, const float* d_vals,
+                            uint64_t nnz, uint32_t total_rows, const int32_t* h_row_off,
+                            int32_t n_systems, mps_batch** out, cudaStream_t s) {
+    if (!out || !h_row_off || n_systems <= 0) return fail(MPS_ERR_ARG, "bad batch arguments");
+    *out = nullptr;
+    if (h_row_off[0] != 0 || (uint32_t)h_row_off[n_systems] != total_rows)
+        return fail(MPS_ERR_ARG, "row_off must start at 0 and end at total_rows");
+    for (int i = 0; i < n_systems; ++i)
+        if (h_row_off[i + 1] < h_row_off[i]) return fail(MPS_ERR_ARG, "row_off must be ascending");
+    mps_batch* B = new mps_batch();
+    mps_status st = mps_csr_create_from_csr(d_row_ptr, d_col_ind, d_vals, total_rows, total_rows, nnz,
+                                            &B->A, s);
+    if (st != MPS_OK) {
+        delete B;
+        return st;
+    }
+    B->n_sys = n_systems;
+    B->row_off.assign(h_row_off, h_row_off + n_systems + 1);
+    // largest first
+    std::vector<int> order(n_systems);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return (h_row_off[a + 1] - h_row_off[a]) > (h_row_off[b + 1] - h_row_off[b]);
+    });
+    // autotuning sample: every k-th system of the size order (spans all sizes)
+    std::vector<int> sample;
+    const int step = std::max(1, n_systems / 64);
+    for (int i = 0; i < n_systems; i += step) sample.push_back(order[i]);
+    B->n_sample = (int)sample.size();
+    cudaError_t e = cudaSuccess;
+    const size_t n = total_rows;
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_row_off, (n_systems + 1) * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_order, n_systems * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_sample_order, sample.size() * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_kind, n_systems);
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_work, 4 * (n + 4) * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_queue, sizeof(unsigned));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(B->d_row_off, h_row_off, (n_systems + 1) * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(B->d_order, order.data(), n_systems * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(B->d_sample_order, sample.data(), sample.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(B->d_kind, 1, n_systems);   // Jacobi by default
+    if (e != cudaSuccess) {
+        mps_batch_destroy(B);
+        return cuda_fail(e, "batch_create");
+    }
+    // Jacobi diagonal of the whole batch
+    mps_solve_opts o;
+    mps_solve_opts_default(&o);
+    o.precond = MPS_PRECOND_JACOBI;
+    st = prepare_precond(B->A, &o, s);
+    if (st != MPS_OK) {
+        mps_batch_destroy(B);
+        return st;
+    }
+    *out = B;
+    return MPS_OK;
+}
+
+mps_status mps_batch_destroy(mps_batch* B) {
+    if (!B) return MPS_OK;
+    if (B->A) mps_csr_destroy(B->A);
+    cudaFree(B->d_row_off);
+    cudaFree(B->d_order);
+    cudaFree(B->d_sample_order);
+    cudaFree(B->d_kind);
+    cudaFree(B->d_work);
+    cudaFree(B->d_queue);
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->cap) cudaStreamDestroy(B->cap);
+    delete B;
+    return MPS_OK;
+}
+
+mps_status mps_batch_attach_fsai(mps_batch* B, const mps_fsai_model* m, cudaStream_t s) {
+    if (!B || !m) return fail(MPS_ERR_ARG, "null argument");
+    if (B->exec) {                     // the captured launch holds the old factor's pointers
+        cudaGraphExecDestroy(B->exec);
+        B->exec = nullptr;
+    }
+    return mps_fsai_attach(B->A, m, s);
+}
+
+mps_status mps_batch_set_precond(mps_batch* B, const int8_t* h_kind) {
+    if (!B || !h_kind) return fail(MPS_ERR_ARG, "null argument");
+    for (int i = 0; i < B->n_sys; ++i) {
+        if (h_kind[i] < 0 || h_kind[i] > 3) return fail(MPS_ERR_ARG, "kind must be 0, 1, 2 or 3");
+        if (h_kind[i] == 2 && !B->A->has_fsai) return fail(MPS_ERR_ARG, "FSAI requested without a factor");
+    }
+    MPS_CUDA(cudaMemcpy(B->d_kind, h_kind, B->n_sys, cudaMemcpyHostToDevice));
+    return MPS_OK;
+}
+
+int32_t mps_batch_warps_per_system(const mps_batch* B) { return B ? B->wps : 0; }
+
+mps_status mps_batch_autotune(mps_batch* B, const float* d_b, double tol, int32_t max_iter,
+                              int32_t* h_chosen_wps, float* h_ms /* 5 candidates */, cudaStream_t s) {
+    if (!B || !d_b) return fail(MPS_ERR_ARG, "null argument");
+    const size_t n = B->A->A.n_rows;
+    float* xs = nullptr;
+    int* it = nullptr;
+    MPS_CUDA(cudaMalloc(&xs, n * sizeof(float)));
+    MPS_CUDA(cudaMalloc(&it, 3 * B->n_sys * sizeof(int)));
+    BatchOut o{it, it + B->n_sys, reinterpret_cast<float*>(it + 2 * B->n_sys)};
+    const int cands[5] = {1, 2, 4, 8, 16};
+    float best = 1e30f;
+    int best_w = B->wps;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    mps_status st = MPS_OK;
+    for (int c = 0; c < 5 && st == MPS_OK; ++c) {
+        float ms = 0.f;
+        for (int rep = 0; rep < 2; ++rep) {   // first run warms up
+            cudaEventRecord(e0, s);
+            st = batch_launch(B, cands[c], true, d_b, xs, tol, max_iter, 400, o, s);
+            if (st != MPS_OK) break;
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            cudaEventElapsedTime(&ms, e0, e1);
+        }
+        if (h_ms) h_ms[c] = ms;
+        if (ms < best) {
+            best = ms;
+            best_w = cands[c];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(xs);
+    cudaFree(it);
+    if (st != MPS_OK) return st;
+    B->wps = best_w;
+    if (h_chosen_wps) *h_chosen_wps = best_w;
+    return MPS_OK;
+}
+
+mps_status mps_batch_cg(mps_batch* B, const float* d_b, float* d_x, double tol, int32_t max_iter,
+                        int32_t* d_iters, int32_t* d_converged, float* d_relres, cudaStream_t s) {
+    if (!B || !d_b || !d_x || !d_iters || !d_converged || !d_relres)
+        return fail(MPS_ERR_ARG, "null argument");
+    BatchOut o{d_iters, d_converged, d_relres};
+    tol = tol > 0 ? tol : 1e-6;
+    max_iter = max_iter > 0 ? max_iter : 20000;
+    // The whole batch is one CUDA-graph launch (queue reset + persistent
+    // kernel), captured once per set of buffers and reused.
+    const void* key[5] = {d_b, d_x, d_iters, d_converged, d_relres};
+    bool same = B->exec && B->exec_wps == B->wps;
+    for (int i = 0; i < 5 && same; ++i) same = key[i] == B->exec_key[i];
+    same = same && B->exec_tol == tol && B->exec_max_iter == max_iter;
+    if (!same) {
+        if (B->exec) cudaGraphExecDestroy(B->exec);
+        B->exec = nullptr;
+        if (!B->cap) MPS_CUDA(cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking));
+        MPS_CUDA(cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal));
+        mps_status st = batch_launch(B, B->wps, false, d_b, d_x, tol, max_iter, 400, o, B->cap);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(B->cap, &g);
+        if (st != MPS_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "batch graph capture");
+        e = cudaGraphInstantiate(&B->exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(e, "batch graph instantiate");
+        for (int i = 0; i < 5; ++i) B->exec_key[i] = key[i];
+        B->exec_wps = B->wps;
+        B->exec_tol = tol;
+        B->exec_max_iter = max_iter;
+    }
+    MPS_CUDA(cudaGraphLaunch(B->exec, s));
+    return MPS_OK;
+}
+
+}  // extern "C"

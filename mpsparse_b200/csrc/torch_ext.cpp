@@ -453,6 +453,74 @@ private:
     int device_ = 0;
 };
 
+// Batched solver over a block-diagonal stack of systems.
+class BatchSolver {
+public:
+    BatchSolver(torch::Tensor row_ptr, torch::Tensor col_ind, torch::Tensor vals, torch::Tensor row_off) {
+        auto rp = on_device(row_ptr, torch::kInt32, "row_ptr");
+        auto ci = on_device(col_ind, torch::kInt32, "col_ind");
+        auto v = on_device(vals, torch::kFloat32, "vals");
+        auto ro = row_off.to(torch::kCPU).to(torch::kInt32).contiguous();
+        n_sys_ = ro.numel() - 1;
+        TORCH_CHECK(n_sys_ > 0, "row_off needs at least two entries");
+        n_ = ro.data_ptr<int32_t>()[n_sys_];
+        TORCH_CHECK(rp.numel() == n_ + 1, "row_ptr must have total_rows + 1 entries");
+        device_ = rp.get_device();
+        c10::cuda::CUDAGuard g(device_);
+        check(mps_batch_create(rp.data_ptr<int32_t>(), ci.data_ptr<int32_t>(), v.data_ptr<float>(),
+                               (uint64_t)ci.numel(), (uint32_t)n_, ro.data_ptr<int32_t>(), (int32_t)n_sys_,
+                               &h_, cur_stream()),
+              "batch");
+    }
+    ~BatchSolver() {
+        if (h_) {
+            c10::cuda::CUDAGuard g(device_);
+            mps_batch_destroy(h_);
+        }
+    }
+    void attach_fsai(const FsaiModel& m) {
+        c10::cuda::CUDAGuard g(device_);
+        check(mps_batch_attach_fsai(h_, m.handle(), cur_stream()), "attach_fsai");
+    }
+    void set_precond(torch::Tensor kinds) {
+        auto k = kinds.to(torch::kCPU).to(torch::kInt8).contiguous();
+        TORCH_CHECK(k.numel() == n_sys_, "one preconditioner kind per system");
+        check(mps_batch_set_precond(h_, k.data_ptr<int8_t>()), "set_precond");
+    }
+    std::tuple<int64_t, std::vector<double>> autotune(torch::Tensor b, double tol, int64_t max_iter) {
+        c10::cuda::CUDAGuard g(device_);
+        auto bd = on_device(b, torch::kFloat32, "b");
+        int32_t w = 0;
+        float ms[5];
+        check(mps_batch_autotune(h_, bd.data_ptr<float>(), tol, (int32_t)max_iter, &w, ms, cur_stream()),
+              "autotune");
+        return {w, std::vector<double>(ms, ms + 5)};
+    }
+    std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> cg(torch::Tensor b, torch::Tensor x, double tol,
+                                                               int64_t max_iter) {
+        c10::cuda::CUDAGuard g(device_);
+        auto bd = on_device(b, torch::kFloat32, "b");
+        TORCH_CHECK(bd.numel() == n_ && x.numel() == n_, "b and x need total_rows entries");
+        TORCH_CHECK(x.is_cuda() && x.is_contiguous() && x.scalar_type() == torch::kFloat32,
+                    "x must be a contiguous CUDA float32 tensor");
+        auto opt = bd.options();
+        auto it = torch::empty({n_sys_}, opt.dtype(torch::kInt32));
+        auto cv = torch::empty({n_sys_}, opt.dtype(torch::kInt32));
+        auto rr = torch::empty({n_sys_}, opt.dtype(torch::kFloat32));
+        check(mps_batch_cg(h_, bd.data_ptr<float>(), x.data_ptr<float>(), tol, (int32_t)max_iter,
+                           it.data_ptr<int32_t>(), cv.data_ptr<int32_t>(), rr.data_ptr<float>(), cur_stream()),
+              "batch cg");
+        return {it, cv, rr};
+    }
+    int64_t warps_per_system() const { return mps_batch_warps_per_system(h_); }
+    int64_t num_systems() const { return n_sys_; }
+
+private:
+    mps_batch* h_ = nullptr;
+    int64_t n_sys_ = 0, n_ = 0;
+    int device_ = 0;
+};
+
 // coo_csr.coo_csr: sort on the GPU and write the caller's three tensors.
 void coo_csr_fn(torch::Tensor keys, torch::Tensor values, torch::Tensor row_ptr,
                 torch::Tensor col_ind, torch::Tensor out_vals, int64_t num_rows, int64_t num_cols) {
@@ -547,6 +615,18 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         .def("set_params", &FsaiModel::set_params, py::arg("params"))
         .def("forward", &FsaiModel::forward, py::arg("X"))
         .def("backward", &FsaiModel::backward, py::arg("X"), py::arg("dout"));
+
+    py::class_<BatchSolver>(m, "batch_solver")
+        .def(py::init<torch::Tensor, torch::Tensor, torch::Tensor, torch::Tensor>(), py::arg("row_ptr"),
+             py::arg("col_ind"), py::arg("values"), py::arg("row_off"))
+        .def("attach_fsai", &BatchSolver::attach_fsai, py::arg("model"))
+        .def("set_precond", &BatchSolver::set_precond, py::arg("kinds"))
+        .def("autotune", &BatchSolver::autotune, py::arg("b"), py::arg("tol") = 1e-6,
+             py::arg("max_iter") = 20000)
+        .def("cg", &BatchSolver::cg, py::arg("b"), py::arg("x"), py::arg("tol") = 1e-6,
+             py::arg("max_iter") = 20000)
+        .def_property_readonly("warps_per_system", &BatchSolver::warps_per_system)
+        .def_property_readonly("num_systems", &BatchSolver::num_systems);
 
     py::class_<BcsrTensor>(m, "bcsr_tensor")
         .def(py::init<torch::Tensor, torch::Tensor, torch::Tensor, torch::Tensor, int64_t, int64_t,

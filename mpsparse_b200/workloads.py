@@ -267,3 +267,69 @@ def lognormal_diffusion_2d_torch(nx: int, ny: int, sigma: float, corr_len: float
     vals = torch.cat([diag.reshape(-1), -ky.reshape(-1), -ky.reshape(-1), -kx.reshape(-1),
                       -kx.reshape(-1)]).to(torch.float32)
     return (rows << 32) | cols, vals, n
+
+
+def graph_laplacian_torch(n: int, mean_degree: float, seed: int, shift: float = 1e-2,
+                          device="cuda"):
+    """Random graph Laplacian on ``device`` (torch generator): n*deg/2 uniform
+    random edges, deduplicated, no self loops, weights U(0.1, 1), plus
+    shift*I.  Returns (keys, values, n)."""
+    import torch
+
+    g = torch.Generator(device=device).manual_seed(seed)
+    m = int(round(n * mean_degree / 2))
+    a = torch.randint(0, n, (m,), generator=g, device=device)
+    b = torch.randint(0, n - 1, (m,), generator=g, device=device)
+    b = torch.where(b >= a, b + 1, b)
+    key = torch.unique(torch.minimum(a, b) * n + torch.maximum(a, b))
+    lo, hi = key // n, key % n
+    w = 0.1 + 0.9 * torch.rand(key.shape[0], generator=g, device=device, dtype=torch.float64)
+    diag = torch.full((n,), shift, device=device, dtype=torch.float64)
+    diag.index_add_(0, lo, w)
+    diag.index_add_(0, hi, w)
+    idx = torch.arange(n, device=device)
+    rows = torch.cat([idx, lo, hi])
+    cols = torch.cat([idx, hi, lo])
+    vals = torch.cat([diag, -w, -w]).to(torch.float32)
+    return (rows << 32) | cols, vals, n
+
+
+def batch_systems(n_systems: int, seed: int, n_min: int = 1024, n_max: int = 65536,
+                  grid_sigma: float = 1.0, grid_corr: float = 8.0, mean_degree: float = 8.0,
+                  device="cuda"):
+    """Independent SPD systems with row counts log-uniform in [n_min, n_max]:
+    even indices are 2D 5-point log-normal diffusion grids (near-square),
+    odd indices random graph Laplacians + 1e-2 I.  Returns the stacked
+    (keys, values) on ``device`` with global indices, row offsets (numpy) and
+    the kind of every system (0 grid, 1 graph)."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(n_min), np.log(n_max), n_systems))
+    keys, vals, off, kinds = [], [], [0], []
+    for s, target in enumerate(sizes):
+        if s % 2 == 0:
+            nx = max(2, int(round(np.sqrt(target))))
+            ny = max(2, int(round(target / nx)))
+            k, v, n = lognormal_diffusion_2d_torch(nx, ny, grid_sigma, grid_corr,
+                                                   seed * 1_000_003 + s, device)
+            kinds.append(0)
+        else:
+            k, v, n = graph_laplacian_torch(int(round(target)), mean_degree,
+                                            seed * 1_000_003 + s, device=device)
+            kinds.append(1)
+        base = off[-1]
+        keys.append(k + ((base << 32) | base))
+        vals.append(v)
+        off.append(base + n)
+    return torch.cat(keys), torch.cat(vals), np.asarray(off, np.int64), np.asarray(kinds, np.int8)
+
+
+def stack(systems) -> tuple[Coo, np.ndarray]:
+    """Block-diagonal stack of Coo systems: (global Coo, row offsets)."""
+    off = np.zeros(len(systems) + 1, np.int64)
+    off[1:] = np.cumsum([s.n for s in systems])
+    rows = np.concatenate([s.rows + o for s, o in zip(systems, off)])
+    cols = np.concatenate([s.cols + o for s, o in zip(systems, off)])
+    vals = np.concatenate([s.vals for s in systems])
+    return Coo(rows, cols, vals, int(off[-1])), off

@@ -1,0 +1,156 @@
+"""Batched persistent PCG (many independent systems in one launch) against
+the FP64 oracle, system by system.
+
+Tolerances: iterates after k steps within 1e-5 relative (2-norm) of the
+oracle's FP64 PCG (FP32 arithmetic, FP64 reductions); converged answers
+judged by each system's FP64 true residual (below 2*tol, or at the FP32
+rounding floor when that is higher); iteration counts within 3% + 2 of the
+oracle's."""
+import numpy as np
+import pytest
+import torch
+
+from mpsparse_b200 import workloads as W
+from tests.helpers import assert_solved_fp32
+
+pytestmark = pytest.mark.gpu
+
+
+def _systems():
+    out = []
+    rng = np.random.default_rng(7)
+    for s in range(16):
+        n = int(np.exp(rng.uniform(np.log(64), np.log(3000))))
+        if s % 2 == 0:
+            nx = max(2, int(np.sqrt(n)))
+            out.append(W.lognormal_diffusion_2d(nx, max(2, n // nx), 1.0, 4.0, 100 + s))
+        else:
+            out.append(W.graph_laplacian(n, 8.0, 200 + s))
+    out.insert(5, W.Coo(np.zeros(0, np.int64), np.zeros(0, np.int64), np.zeros(0, np.float32), 0))
+    return out
+
+
+@pytest.fixture(scope="module")
+def batch(mps):
+    from mpsparse_b200.batched import BatchedSolver
+    systems = _systems()
+    coo, off = W.stack(systems)
+    coo = coo.shuffled(3)
+    S = BatchedSolver.from_coo(torch.from_numpy(coo.keys()).cuda(),
+                               torch.from_numpy(coo.vals).cuda(), off)
+    b = np.concatenate([W.rhs(s.n, 10 + i) if s.n else np.zeros(0) for i, s in enumerate(systems)])
+    return S, systems, off, b
+
+
+def _oracle_A(oracle, coo):
+    return oracle.Csr(*coo.to_csr(), coo.n)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_batched_first_iterates(mps, oracle, batch):
+    S, systems, off, b = batch
+    S.set_precond(np.full(S.n_systems, 1, np.int8))
+    bt = torch.from_numpy(b).float().cuda()
+    for k in (1, 3, 8):
+        x = torch.zeros(S.n, device="cuda")
+        it, cv, _ = S.solve(bt, x, tol=1e-300, max_iter=k)
+        it, x = it.cpu().numpy(), x.cpu().numpy()
+        for s, sysm in enumerate(systems):
+            if sysm.n == 0:
+                assert it[s] == 0
+                continue
+            assert it[s] == k, (s, it[s])
+            xo, _ = oracle.cg(_oracle_A(oracle, sysm), b[off[s]:off[s + 1]], tol=0.0, max_iter=k,
+                              precond="jacobi")
+            assert _rel(x[off[s]:off[s + 1]], xo) <= 1e-5, (k, s)
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_batched_converges_per_system(mps, oracle, batch, kind):
+    S, systems, off, b = batch
+    S.set_precond(np.full(S.n_systems, kind, np.int8))
+    x = torch.zeros(S.n, device="cuda")
+    it, cv, rr = S.solve(torch.from_numpy(b).float().cuda(), x, tol=1e-6, max_iter=20000)
+    it, cv, rr, x = it.cpu().numpy(), cv.cpu().numpy(), rr.cpu().numpy(), x.cpu().numpy()
+    assert cv.all()
+    for s, sysm in enumerate(systems):
+        if sysm.n == 0:
+            assert it[s] == 0 and rr[s] == 0
+            continue
+        A = _oracle_A(oracle, sysm)
+        bs = b[off[s]:off[s + 1]]
+        assert_solved_fp32(oracle, A, bs, x[off[s]:off[s + 1]], 1e-6)
+        _, io = oracle.cg(A, bs, tol=1e-6, max_iter=20000, precond="jacobi" if kind else None)
+        assert abs(it[s] - io["iters"]) <= 0.03 * io["iters"] + 2, (s, it[s], io["iters"])
+        assert rr[s] <= 1e-6
+
+
+def test_batched_mask_and_skip(mps, batch):
+    S, systems, off, b = batch
+    kinds = np.full(S.n_systems, 1, np.int8)
+    kinds[2] = 3                                   # masked out
+    S.set_precond(kinds)
+    x = torch.full((S.n,), 7.0, device="cuda")
+    it, cv, rr = S.solve(torch.from_numpy(b).float().cuda(), x, tol=1e-6, max_iter=4)
+    it, cv, rr, x = it.cpu().numpy(), cv.cpu().numpy(), rr.cpu().numpy(), x.cpu().numpy()
+    assert it[2] == 0 and cv[2] == 0 and rr[2] == -1
+    assert np.all(x[off[2]:off[3]] == 7.0)        # untouched
+    big = [s for s, m in enumerate(systems) if m.n > 200 and s != 2]
+    assert np.all(cv[big] == 0) and np.all(it[big] == 4) and np.all(rr[big] > 1e-6)
+    with pytest.raises(RuntimeError):
+        S.set_precond(np.full(S.n_systems, 5, np.int8))
+
+
+def test_batched_warps_per_system_agree(mps, oracle, batch):
+    S, systems, off, b = batch
+    S.set_precond(np.full(S.n_systems, 1, np.int8))
+    bt = torch.from_numpy(b).float().cuda()
+    info = S.autotune(bt, 1e-6, 20000)
+    assert info["warps_per_system"] in (1, 2, 4, 8, 16)
+    assert all(t > 0 for t in info["candidates_ms"].values())
+    x = torch.zeros(S.n, device="cuda")
+    it, cv, _ = S.solve(bt, x, tol=1e-6)
+    assert cv.cpu().numpy().all()
+    x = x.cpu().numpy()
+    for s in (0, 1, 7):
+        A = _oracle_A(oracle, systems[s])
+        assert_solved_fp32(oracle, A, b[off[s]:off[s + 1]], x[off[s]:off[s + 1]], 1e-6)
+
+
+def test_batched_fsai_matches_single_system(mps, oracle, batch):
+    from mpsparse_b200.fsai import LearnedFsai
+    S, systems, off, b = batch
+    f = LearnedFsai.load()
+    S.attach_fsai(f)
+    S.set_precond(np.full(S.n_systems, 2, np.int8))
+    x = torch.zeros(S.n, device="cuda")
+    it, cv, _ = S.solve(torch.from_numpy(b).float().cuda(), x, tol=1e-6)
+    it, cv, x = it.cpu().numpy(), cv.cpu().numpy(), x.cpu().numpy()
+    assert cv.all()
+    for s in (0, 1, 4):
+        sysm = systems[s]
+        A = _oracle_A(oracle, sysm)
+        bs = b[off[s]:off[s + 1]]
+        assert_solved_fp32(oracle, A, bs, x[off[s]:off[s + 1]], 1e-6)
+        e = torch.empty(0)
+        T = mps.spmv.csr_tensor(torch.from_numpy(sysm.keys()), torch.from_numpy(sysm.vals), e, e, e,
+                                sysm.n, sysm.n)
+        f.attach(T)
+        xs = torch.zeros(sysm.n, device="cuda")
+        info = T.cgd(torch.from_numpy(bs).float().cuda(), xs, tol=1e-6, max_iter=20000, precond="fsai")
+        assert abs(it[s] - info["iters"]) <= 0.03 * info["iters"] + 2, (s, it[s], info["iters"])
+    info = S.choose_precond(torch.from_numpy(b).float().cuda(),
+                            np.array([s % 2 for s in range(S.n_systems)]), sample=4)
+    assert set(info) == {0, 1}
+
+
+def test_batch_generator_blocks(mps):
+    keys, vals, off, kinds = W.batch_systems(6, seed=1, n_min=256, n_max=2048)
+    rows, cols = (keys >> 32).cpu().numpy(), (keys & 0xFFFFFFFF).cpu().numpy()
+    sys_r = np.searchsorted(off, rows, side="right") - 1
+    sys_c = np.searchsorted(off, cols, side="right") - 1
+    assert np.array_equal(sys_r, sys_c)            # block diagonal
+    assert off[0] == 0 and np.all(np.diff(off) >= 256 // 2) and list(kinds) == [0, 1] * 3
