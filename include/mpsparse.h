@@ -116,6 +116,20 @@ mps_status mps_coo_to_csr(const uint64_t* d_keys, const float* d_vals, uint64_t 
  * kernel spmv_op, spmv.metal:11-49). */
 mps_status mps_csr_spmv(const mps_csr* A, const float* d_x, float* d_y, cudaStream_t stream);
 
+/* SpMV autotuner (no reference counterpart): times the tile-plan candidates
+ * (nonzeros per tile: half / default / twice the default; TMA pipeline depth
+ * 2 / 3; L2 evict-first hint on the streamed arrays off / on) on this matrix
+ * and keeps the fastest for every later SpMV and solve of the handle.  Any
+ * pointer may be NULL; h_best_us is the winner's time per SpMV.
+ * Synchronises the stream. */
+mps_status mps_csr_autotune_spmv(mps_csr* A, int32_t* h_tile_nnz, int32_t* h_stages,
+                                 int32_t* h_evict_first, float* h_best_us, cudaStream_t stream);
+/* Set the SpMV tile plan by hand (tile_nnz 0: default size, else 256..8192;
+ * stages 0: keep, else 2 or 3; evict_first < 0: keep).  No reference
+ * counterpart. */
+mps_status mps_csr_set_spmv_plan(mps_csr* A, int32_t tile_nnz, int32_t stages,
+                                 int32_t evict_first, cudaStream_t stream);
+
 /* y = A x and *d_dot = w . y in FP64 (fused_spvmv, spmv.metal:70-132;
  * deterministic). */
 mps_status mps_csr_spmv_dot(const mps_csr* A, const float* d_x, const float* d_w, float* d_y,

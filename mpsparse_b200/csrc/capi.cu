@@ -227,6 +227,70 @@ mps_status mps_csr_spmv(const mps_csr* h, const float* d_x, float* d_y, cudaStre
     return MPS_OK;
 }
 
+mps_status mps_csr_set_spmv_plan(mps_csr* h, int32_t tile_nnz, int32_t stages, int32_t evict_first,
+                                 cudaStream_t s) {
+    if (!h) return fail(MPS_ERR_ARG, "null handle");
+    if (stages != 0 && stages != 2 && stages != 3) return fail(MPS_ERR_ARG, "stages must be 2 or 3");
+    if (tile_nnz < 0 || tile_nnz > 8192) return fail(MPS_ERR_ARG, "tile_nnz must be in [0, 8192]");
+    MPS_CUDA(spmv_plan_build(h->A, tile_nnz < 256 && tile_nnz > 0 ? 256 : tile_nnz, s, stages,
+                             evict_first < 0 ? -1 : (evict_first ? 1 : 0)));
+    h->H.drop_graphs();
+    return MPS_OK;
+}
+
+mps_status mps_csr_autotune_spmv(mps_csr* h, int32_t* h_tile_nnz, int32_t* h_stages,
+                                 int32_t* h_evict_first, float* h_best_us, cudaStream_t s) {
+    if (!h) return fail(MPS_ERR_ARG, "null handle");
+    if (h->A.nnz == 0) return MPS_OK;
+    // Candidates: tile size (half, default, twice the default nonzeros per
+    // tile), pipeline depth 2 / 3, L2 evict-first hint off / on; each timed
+    // over 5 launches after 2 warm-ups, with x = 0 (timing only).
+    const int T0 = default_tile_nnz(h->A.nnz, h->A.n_rows);
+    int tiles[3] = {T0 / 2, T0, 2 * T0};
+    for (int& t : tiles) t = t < 256 ? 256 : (t > 8192 ? 8192 : t);
+    float* buf = nullptr;
+    MPS_CUDA(cudaMalloc(&buf, ((size_t)h->A.n_cols + h->A.n_rows + 8) * sizeof(float)));
+    float* x = buf;
+    float* y = buf + h->A.n_cols + 4;
+    cudaError_t e = cudaMemsetAsync(x, 0, (size_t)h->A.n_cols * sizeof(float), s);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    float best = 1e30f;
+    int bt = T0, bs = h->A.plan.stages, bh = h->A.plan.evict_first;
+    for (int ti = 0; ti < 3 && e == cudaSuccess; ++ti) {
+        if (ti > 0 && tiles[ti] == tiles[ti - 1]) continue;
+        for (int st = 2; st <= 3 && e == cudaSuccess; ++st)
+            for (int hint = 0; hint <= 1 && e == cudaSuccess; ++hint) {
+                e = spmv_plan_build(h->A, tiles[ti], s, st, hint);
+                for (int w = 0; w < 2 && e == cudaSuccess; ++w) e = spmv_launch(h->A, x, y, s);
+                if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+                for (int r = 0; r < 5 && e == cudaSuccess; ++r) e = spmv_launch(h->A, x, y, s);
+                if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                float ms = 0.f;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+                if (e == cudaSuccess && ms < best) {
+                    best = ms;
+                    bt = tiles[ti];
+                    bs = st;
+                    bh = hint;
+                }
+            }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(buf);
+    if (e == cudaSuccess) e = spmv_plan_build(h->A, bt, s, bs, bh);
+    if (e != cudaSuccess) return cuda_fail(e, "autotune_spmv");
+    h->H.drop_graphs();        // captured solves hold the old plan's launch shapes
+    if (h_tile_nnz) *h_tile_nnz = bt;
+    if (h_stages) *h_stages = bs;
+    if (h_evict_first) *h_evict_first = bh;
+    if (h_best_us) *h_best_us = best * 1e3f / 5.f;
+    return MPS_OK;
+}
+
 mps_status mps_csr_spmv_dot(const mps_csr* hc, const float* d_x, const float* d_w, float* d_y,
                             double* d_dot, cudaStream_t s) {
     mps_csr* h = const_cast<mps_csr*>(hc);

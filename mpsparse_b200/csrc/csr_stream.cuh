@@ -4,9 +4,7 @@
 // col_ind, values and row_ptr segments are contiguous byte ranges, so one
 // thread stages them into shared memory with bulk async copies
 // (cp.async.bulk.shared::cluster.global, completion counted on an mbarrier; no
-// multicast).  Two buffers per CTA: while the CTA multiplies tile t, the copy
-// of its next tile is already in flight, so the HBM stream never waits for
-// the per-tile reduction.  Per tile:
+// multicast) while the CTA multiplies earlier tiles.  Per tile:
 //   1. wait (bounded) for the tile's bytes;
 //   2. one thread per nonzero: prod = val * x[col] (x gathered through the
 //      read-only path and L2), written over the staged col_ind in place;
@@ -17,29 +15,31 @@
 // memory.  The handle's CSR arrays carry 16 spare elements so a copy rounded
 // out to 16-byte boundaries never leaves its allocation.
 //
-// Three buffers per CTA: a tile's copy is issued two tiles ahead, right after
-// the barrier that ends the product phase of the current tile (by then every
-// thread has finished the tile that last used that buffer), so each tile needs
-// a single block barrier.  col_ind/values are copied with an L2 evict-first
-// policy so that x, gathered by every tile, stays resident in L2.
+// Pipeline depth NB (buffers per CTA), chosen per matrix by the autotuner:
+//   * NB == 2: the copy of tile it+1 is issued at the top of tile it, after
+//     the barrier that ends tile it-1 (two block barriers per tile; the copy
+//     overlaps all of tile it);
+//   * NB >= 3: the copy of tile it+NB-1 is issued right after the barrier that
+//     ends the product phase of tile it (by then every thread has finished
+//     tile it-1, the buffer's last user), so each tile needs one barrier.
+// col_ind/values are copied with an optional L2 evict-first policy so that x,
+// gathered by every tile, stays resident in L2.
 #pragma once
 #include "spmv_kernels.cuh"
 #include "tma.cuh"
 
 namespace mps {
 
-constexpr int kStreamStages = 3;
-
 template <bool BF16>
 __host__ __device__ constexpr size_t stream_buf_bytes(int cap, int rcap) {
     return (size_t)cap * 4 + (size_t)cap * (BF16 ? 2 : 4) + (size_t)rcap * 4;
 }
 
-template <bool BF16, class Epi, int NT = kNT>
+template <bool BF16, class Epi, int NB, int NT = kNT>
 __global__ void __launch_bounds__(NT, 4)
 spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
+    static_assert(NB >= 2 && NB <= 4, "2 to 4 stages");
     extern __shared__ __align__(128) unsigned char smem[];
-    constexpr int NB = kStreamStages;
     __shared__ unsigned long long bar[NB];
     __shared__ int4 s_meta[NB];
     __shared__ double red[NT / 32];
@@ -69,6 +69,7 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
         return m.w > m.z && (a1 - a0) <= A.cap && (r1 - r0) <= A.rcap;
     };
     uint64_t pol = 0;
+    const bool hint = A.evict_first != 0;
     auto issue = [&](const int4 m, int b) {   // one thread
         const int a0 = m.z & ~(GA - 1), a1 = (m.w + GA - 1) & ~(GA - 1);
         const int r0 = m.x & ~3, r1 = (m.y + 1 + 3) & ~3;
@@ -78,36 +79,52 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
         unsigned char* base = smem + (size_t)b * bb;
         fence_proxy_async();
         mbar_expect_tx(&bar[b], bc + bv + br);
-        bulk_g2s_hint(base, A.ci + a0, bc, &bar[b], pol);
-        if (BF16)
-            bulk_g2s_hint(base + (size_t)A.cap * 4, A.vb + a0, bv, &bar[b], pol);
-        else
-            bulk_g2s_hint(base + (size_t)A.cap * 4, A.v + a0, bv, &bar[b], pol);
+        const void* vsrc = BF16 ? static_cast<const void*>(A.vb + a0) : static_cast<const void*>(A.v + a0);
+        if (hint) {
+            bulk_g2s_hint(base, A.ci + a0, bc, &bar[b], pol);
+            bulk_g2s_hint(base + (size_t)A.cap * 4, vsrc, bv, &bar[b], pol);
+        } else {
+            bulk_g2s(base, A.ci + a0, bc, &bar[b]);
+            bulk_g2s(base + (size_t)A.cap * 4, vsrc, bv, &bar[b]);
+        }
         bulk_g2s(base + (size_t)A.cap * (BF16 ? 6 : 8), A.rp + r0, br, &bar[b]);
     };
 
     // Thread 0 keeps the metadata of the next tiles in registers (loaded
-    // ahead) and publishes each tile's through shared memory two tiles ahead.
+    // ahead) and publishes each tile's through shared memory when it issues
+    // the tile's copy.
     const int4 none = make_int4(0, 0, 0, 0);
     const int t0 = blockIdx.x, G = gridDim.x;
-    int4 m_ahead = none;           // metadata of tile it + 2 (issued next)
-    int4 m_ahead2 = none;          // tile it + 3
+    int4 m_ahead = none;           // metadata of tile it + NB - 1 (issued next)
+    int4 m_ahead2 = none;          // tile it + NB
     if (threadIdx.x == 0) {
-        pol = policy_evict_first();
+        if (hint) pol = policy_evict_first();
         for (int i = 0; i < NB - 1; ++i) {
             const int ti = t0 + i * G;
             const int4 mi = ti < A.ntiles ? A.meta[ti] : none;
             if (ti < A.ntiles && staged(mi)) issue(mi, i);
             s_meta[i] = mi;
         }
-        m_ahead = t0 + 2 * G < A.ntiles ? A.meta[t0 + 2 * G] : none;
-        m_ahead2 = t0 + 3 * G < A.ntiles ? A.meta[t0 + 3 * G] : none;
+        m_ahead = t0 + (NB - 1) * G < A.ntiles ? A.meta[t0 + (NB - 1) * G] : none;
+        m_ahead2 = t0 + NB * G < A.ntiles ? A.meta[t0 + NB * G] : none;
     }
     __syncthreads();
+    // Issue the copy of tile it + NB - 1 into the buffer tile it - 1 used.
+    auto issue_ahead = [&](int t, int it) {   // one thread
+        const int bn = (it + NB - 1) % NB;
+        if (t + (NB - 1) * G < A.ntiles && staged(m_ahead)) issue(m_ahead, bn);
+        s_meta[bn] = m_ahead;
+        m_ahead = m_ahead2;
+        m_ahead2 = t + (NB + 1) * G < A.ntiles ? A.meta[t + (NB + 1) * G] : none;
+    };
     unsigned phase_bits = 0u;      // completed-phase parity per buffer (uniform)
     int it = 0;
     for (int t = t0; t < A.ntiles; t += G, ++it) {
         const int b = it % NB;
+        if constexpr (NB == 2) {
+            if (it > 0) __syncthreads();      // every thread is done with tile it - 1
+            if (threadIdx.x == 0) issue_ahead(t, it);
+        }
         const int4 m = s_meta[b];
         const int rs = m.x, re = m.y, k0 = m.z, k1 = m.w;
         const bool stg = rs < re && staged(m);
@@ -146,15 +163,11 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
                     if (kb + u * NT < k1) prod[kb + u * NT - a0] = v[u] * xv[u];
             }
         }
-        // Products visible; every thread is past tile it - 1, so the buffer of
-        // tile it + 2 (the one tile it - 1 used) can be refilled.
+        // Products visible.  With NB >= 3, every thread is past tile it - 1,
+        // so its buffer takes the copy of tile it + NB - 1.
         __syncthreads();
-        if (threadIdx.x == 0) {
-            const int b2 = (it + 2) % NB;
-            if (t + 2 * G < A.ntiles && staged(m_ahead)) issue(m_ahead, b2);
-            s_meta[b2] = m_ahead;
-            m_ahead = m_ahead2;
-            m_ahead2 = t + 4 * G < A.ntiles ? A.meta[t + 4 * G] : none;
+        if constexpr (NB >= 3) {
+            if (threadIdx.x == 0) issue_ahead(t, it);
         }
         if (rs < re) {
             if (stg) {

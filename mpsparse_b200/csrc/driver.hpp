@@ -39,18 +39,22 @@ struct CsrOp {
     template <class Epi>
     cudaError_t apply(const float* x, const Epi& e, cudaStream_t s) const {
         const CsrStreamDev v = A->stream_view(vb);
+        const int nb = A->plan.stages;
         if (vb) {
-            const size_t smem = kStreamStages * stream_buf_bytes<true>(v.cap, v.rcap);
-            smem_optin_k(spmv_stream<true, Epi>, smem);
-            const int g = persistent_grid(spmv_stream<true, Epi>, smem, v.ntiles);
-            spmv_stream<true, Epi><<<g, kNT, smem, s>>>(v, x, e);
+            if (nb >= 3) launch<true, 3>(v, x, e, s);
+            else launch<true, 2>(v, x, e, s);
         } else {
-            const size_t smem = kStreamStages * stream_buf_bytes<false>(v.cap, v.rcap);
-            smem_optin_k(spmv_stream<false, Epi>, smem);
-            const int g = persistent_grid(spmv_stream<false, Epi>, smem, v.ntiles);
-            spmv_stream<false, Epi><<<g, kNT, smem, s>>>(v, x, e);
+            if (nb >= 3) launch<false, 3>(v, x, e, s);
+            else launch<false, 2>(v, x, e, s);
         }
         return cudaGetLastError();
+    }
+    template <bool BF16, int NB, class Epi>
+    static void launch(const CsrStreamDev& v, const float* x, const Epi& e, cudaStream_t s) {
+        const size_t smem = NB * stream_buf_bytes<BF16>(v.cap, v.rcap);
+        smem_optin_k(spmv_stream<BF16, Epi, NB>, smem);
+        const int g = persistent_grid(spmv_stream<BF16, Epi, NB>, smem, v.ntiles);
+        spmv_stream<BF16, Epi, NB><<<g, kNT, smem, s>>>(v, x, e);
     }
 };
 

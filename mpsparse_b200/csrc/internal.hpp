@@ -74,6 +74,10 @@ struct SpmvPlan {
     int cap_s = 0;            // staged nonzeros per buffer of the TMA kernel
     int rcap = 0;             // staged row_ptr entries per buffer
     int grid_s = 0;           // persistent CTAs of the TMA kernel
+    int stages = 3;           // TMA pipeline depth (2 or 3)
+    int evict_first = 0;      // L2 evict-first hint on the col_ind/value copies
+    int max_tile_nnz = 0;     // largest tile (nonzeros) and row count of the plan
+    int max_tile_rows = 0;
 };
 
 // View of a CSR for the TMA-staged kernel (csr_stream.cuh).
@@ -86,6 +90,7 @@ struct CsrStreamDev {
     int ntiles;
     int cap;
     int rcap;
+    int evict_first;
     unsigned* err;
 };
 
@@ -126,7 +131,8 @@ struct CsrMat {
         return CsrDev{rp, ci, v, vb, plan.d_tile_row, (int)n_rows, plan.ntiles, plan.cap};
     }
     CsrStreamDev stream_view(const __nv_bfloat16* vb = nullptr) const {
-        return CsrStreamDev{rp, ci, v, vb, plan.d_meta, plan.ntiles, plan.cap_s, plan.rcap, err};
+        return CsrStreamDev{rp, ci, v, vb, plan.d_meta, plan.ntiles, plan.cap_s, plan.rcap,
+                            plan.evict_first, err};
     }
 };
 
@@ -142,7 +148,11 @@ cudaError_t sort_to_csr(const uint64_t* keys, const uint32_t* payload, uint64_t 
                         uint32_t n_rows, uint32_t n_cols, int32_t* row_ptr, int32_t* col_out,
                         uint32_t* payload_out, unsigned* d_err, cudaStream_t s);
 
-cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s);
+// Tile plan of A (tile_nnz <= 0: the default size; stages <= 0 /
+// evict_first < 0: keep the current plan's choice).  Synchronises `s` once to
+// size the staging buffers to the largest tile.
+cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s, int stages = 0,
+                            int evict_first = -1);
 void spmv_plan_free(SpmvPlan& p);
 cudaError_t spmv_launch(const CsrMat& A, const float* x, float* y, cudaStream_t s);
 cudaError_t spmv_dot_launch(const CsrMat& A, const float* x, const float* w, float* y,

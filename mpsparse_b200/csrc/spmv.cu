@@ -42,6 +42,24 @@ __global__ void plan_meta_kernel(const int* __restrict__ rp, const int* __restri
     meta[t] = make_int4(rs, re, rp[rs], rp[re]);
 }
 
+// Largest tile of a plan: stats[0] = max nonzeros, stats[1] = max rows.
+__global__ void plan_stats_kernel(const int4* __restrict__ meta, int ntiles, int* __restrict__ stats) {
+    int mn = 0, mr = 0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+        const int4 m = meta[t];
+        mn = max(mn, m.w - m.z);
+        mr = max(mr, m.y - m.x);
+    }
+    for (int o = 16; o; o >>= 1) {
+        mn = max(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mr = max(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(stats, mn);
+        atomicMax(stats + 1, mr);
+    }
+}
+
 __global__ void diag_inv_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
                                 const float* __restrict__ v, int n, float* __restrict__ dinv) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
@@ -91,7 +109,7 @@ void spmv_plan_free(SpmvPlan& p) {
     p = SpmvPlan{};
 }
 
-cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s) {
+cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s, int stages, int evict_first) {
     if (tile_nnz <= 0) tile_nnz = default_tile_nnz(A.nnz, A.n_rows);
     tile_nnz = (tile_nnz + 3) & ~3;
     const uint64_t nt = A.nnz ? (A.nnz + tile_nnz - 1) / tile_nnz : 1;
@@ -102,11 +120,12 @@ cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s) {
     const int cap_grid = num_sms() * 8;
     p.grid = p.ntiles < cap_grid ? p.ntiles : cap_grid;
     if (p.grid < 1) p.grid = 1;
-    p.cap_s = (tile_nnz + 128 + 7) & ~7;
-    p.rcap = 520;
+    p.stages = stages > 0 ? stages : A.plan.stages;
+    p.evict_first = evict_first >= 0 ? evict_first : A.plan.evict_first;
     p.grid_s = p.ntiles < num_sms() * 6 ? p.ntiles : num_sms() * 6;
     if (p.grid_s < 1) p.grid_s = 1;
-    cudaError_t e = cudaMalloc(&p.d_tile_row, (size_t)(p.ntiles + 1) * sizeof(int));
+    // tile_row has 2 spare ints at the end for the plan statistics
+    cudaError_t e = cudaMalloc(&p.d_tile_row, (size_t)(p.ntiles + 3) * sizeof(int));
     if (e != cudaSuccess) return e;
     e = cudaMalloc(&p.d_meta, (size_t)p.ntiles * sizeof(int4));
     if (e != cudaSuccess) {
@@ -116,12 +135,34 @@ cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s) {
     plan_tiles_kernel<<<(p.ntiles + 1 + 255) / 256, 256, 0, s>>>(A.rp, (int)A.n_rows, tile_nnz,
                                                                  p.ntiles, p.d_tile_row);
     plan_meta_kernel<<<(p.ntiles + 255) / 256, 256, 0, s>>>(A.rp, p.d_tile_row, p.ntiles, p.d_meta);
-    e = cudaGetLastError();
+    int* d_stats = p.d_tile_row + p.ntiles + 1;
+    int stats[2] = {0, 0};
+    e = cudaMemsetAsync(d_stats, 0, 2 * sizeof(int), s);
+    if (e == cudaSuccess) {
+        plan_stats_kernel<<<grid_for(p.ntiles, 256), 256, 0, s>>>(p.d_meta, p.ntiles, d_stats);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(stats, d_stats, sizeof(stats), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         cudaFree(p.d_tile_row);
         cudaFree(p.d_meta);
         return e;
     }
+    // Staging buffers sized to the largest tile (plus the 16-byte rounding
+    // of both ends), with every stage's buffer inside the 227 KB a CTA may
+    // hold (1 KB kept for the kernel's static shared memory, 8 bytes per
+    // staged nonzero); larger tiles take the unstaged path.
+    p.max_tile_nnz = stats[0];
+    p.max_tile_rows = stats[1];
+    const int r_need = p.max_tile_rows + 8;
+    p.rcap = ((r_need < 2048 ? r_need : 2048) + 3) & ~3;
+    const int stage_bytes = (227 * 1024 - 1024) / (p.stages < 2 ? 2 : p.stages);
+    int cap_lim = 2 * tile_nnz + 64;
+    const int cap_smem = (stage_bytes - p.rcap * 4) / 8;
+    if (cap_lim > cap_smem) cap_lim = cap_smem;
+    const int cap_need = p.max_tile_nnz + 16;
+    p.cap_s = (cap_need < cap_lim ? cap_need : cap_lim) & ~7;
     spmv_plan_free(A.plan);
     A.plan = p;
     return cudaSuccess;

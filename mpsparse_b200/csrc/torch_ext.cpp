@@ -144,6 +144,26 @@ public:
         }
     }
 
+    py::dict autotune() {
+        c10::cuda::CUDAGuard g(device_);
+        int32_t t = 0, st = 0, hint = 0;
+        float us = 0.f;
+        check(mps_csr_autotune_spmv(h_, &t, &st, &hint, &us, cur_stream()), "autotune");
+        py::dict d;
+        d["tile_nnz"] = t;
+        d["stages"] = st;
+        d["evict_first"] = hint;
+        d["spmv_us"] = us;
+        return d;
+    }
+
+    void set_plan(int64_t tile_nnz, int64_t stages, int64_t evict_first) {
+        c10::cuda::CUDAGuard g(device_);
+        check(mps_csr_set_spmv_plan(h_, (int32_t)tile_nnz, (int32_t)stages, (int32_t)evict_first,
+                                    cur_stream()),
+              "set_plan");
+    }
+
     std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> export_csr() {
         c10::cuda::CUDAGuard g(device_);
         auto opt = torch::TensorOptions().device(torch::kCUDA, device_);
@@ -605,6 +625,10 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         .def("fsai_g_values", &CsrTensor::fsai_g_values)
         .def("fsai_probe_grad", &CsrTensor::fsai_probe_grad, py::arg("V"))
         .def("csr", &CsrTensor::export_csr)
+        .def("set_plan", &CsrTensor::set_plan, py::arg("tile_nnz") = 0, py::arg("stages") = 0,
+             py::arg("evict_first") = -1)
+        .def("autotune", &CsrTensor::autotune,
+             "time the SpMV tile-plan candidates on this matrix and keep the fastest")
         .def_property_readonly("nnz", &CsrTensor::nnz)
         .def_property_readonly("num_rows", &CsrTensor::num_rows)
         .def_property_readonly("num_cols", &CsrTensor::num_cols);

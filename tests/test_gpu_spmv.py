@@ -96,3 +96,54 @@ def test_spmv_through_cabi(mps, golden):
     assert np.allclose(y.cpu().numpy(), g["y"], rtol=1e-5, atol=1e-5)
     assert torch.equal(y, y2)
     assert abs(d.item() - float(g["x"].astype(np.float64) @ g["y"])) < 1e-3
+
+
+@pytest.mark.parametrize("kind", ["c1", "longrows", "emptyrows"])
+def test_every_plan_variant(mps, oracle, kind):
+    """Each tile plan the autotuner can pick (tile size, TMA pipeline depth,
+    L2 hint) gives the same answer within the FP32 bound."""
+    from mpsparse_b200 import workloads as W
+    rng = np.random.default_rng(3)
+    if kind == "c1":
+        c = W.lognormal_diffusion_2d(200, 150, 1.0, 8.0, 4)
+        rp, ci, cv = c.to_csr(); nr = nc = c.n
+    else:
+        nr = nc = 30000
+        lens = rng.integers(0, 12, nr)
+        if kind == "longrows":
+            lens[9] = 70000; lens[1000] = 3000; lens[1001] = 2049
+        else:
+            lens[rng.random(nr) < 0.8] = 0
+        rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+        ci = np.concatenate([np.sort(rng.choice(nc, l, replace=l > nc)) for l in lens]).astype(np.int32)
+        cv = rng.standard_normal(rp[-1]).astype(np.float32)
+    A = _make(mps, rp, ci, cv, nr, nc)
+    x = rng.standard_normal(nc).astype(np.float32)
+    xt = torch.from_numpy(x).cuda()
+    for tile in (256, 0, 8192):
+        for stages in (2, 3):
+            for hint in (0, 1):
+                A.set_plan(tile, stages, hint)
+                y = torch.full((nr,), float("nan"), device="cuda")
+                A.mv(xt, y)
+                _check(oracle, rp, ci, cv, nr, x, y.cpu().numpy())
+    with pytest.raises(RuntimeError):
+        A.set_plan(0, 5, 0)
+
+
+def test_autotune_then_solve(mps, oracle):
+    from mpsparse_b200 import workloads as W
+    from tests.helpers import assert_solved_fp32
+    c = W.lognormal_diffusion_2d(128, 128, 1.0, 8.0, 5)
+    rp, ci, cv = c.to_csr()
+    A = _make(mps, rp, ci, cv, c.n, c.n)
+    b = W.rhs(c.n, 1)
+    x = torch.zeros(c.n, device="cuda")
+    A.cgd(torch.from_numpy(b).float().cuda(), x, tol=1e-6, max_iter=5000)   # graph captured
+    choice = A.autotune()
+    assert choice["stages"] in (2, 3) and choice["evict_first"] in (0, 1)
+    assert 256 <= choice["tile_nnz"] <= 8192 and choice["spmv_us"] > 0
+    x.zero_()
+    info = A.cgd(torch.from_numpy(b).float().cuda(), x, tol=1e-6, max_iter=5000)
+    assert info["converged"]
+    assert_solved_fp32(oracle, oracle.Csr(rp, ci, cv, c.n), b, x.cpu().numpy(), 1e-6)
