@@ -31,6 +31,7 @@ class BatchedSolver:
         rp_at = row_ptr[torch.from_numpy(self.row_off).to(row_ptr.device)].cpu().numpy()
         self.nnz = np.diff(rp_at.astype(np.int64))           # nonzeros per system
         self.rows = np.diff(self.row_off)
+        self.csr = (row_ptr, col_ind, vals)                  # the stacked CSR (device)
         self.impl = batch_solver(row_ptr, col_ind, vals,
                                  torch.from_numpy(self.row_off.astype(np.int32)))
         self.kinds = np.full(self.n_systems, JACOBI, np.int8)
