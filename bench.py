@@ -152,7 +152,7 @@ def run_ours(args, rank, world, dev):
     def solve_jacobi(i):
         coo, A, b = systems[i]
         x = torch.zeros(n, device=dev)
-        info = A.cgd(b, x, tol=TOL, max_iter=args.max_iter, precond="jacobi")
+        info = A.cgd(b, x, tol=TOL, max_iter=args.max_iter, precond="jacobi", host_loop=args.host_loop)
         return x, info
 
     b64 = [s[2].double() for s in systems]
@@ -162,7 +162,7 @@ def run_ours(args, rank, world, dev):
         fsai.attach(A)                     # network forward -> G on this system
         x = torch.zeros(n, dtype=torch.float64, device=dev)
         info = A.cg_mixed(b64[i], x, tol=TOL, inner_tol=args.inner_tol, max_inner=args.max_iter,
-                          precond="fsai")
+                          precond="fsai", host_loop=args.host_loop)
         return x, {"iters": info["inner_iters"], "outer": info["outer_iters"],
                    "converged": info["converged"], "rel_resid": info["rel_resid"]}
 

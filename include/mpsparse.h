@@ -181,6 +181,8 @@ typedef struct {
     int32_t max_inner;        /* 0: 2000 */
     int32_t value_bits;       /* 32 or 16 */
     int32_t precond;          /* MPS_PRECOND_NONE / JACOBI / FSAI for the inner CG */
+    int32_t host_loop;        /* inner CG iterations launched from the host (see mps_solve_opts) */
+    int32_t reserved;
 } mps_ir_opts;
 
 typedef struct {

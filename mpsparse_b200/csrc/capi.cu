@@ -234,6 +234,7 @@ mps_status mps_csr_set_spmv_plan(mps_csr* h, int32_t tile_nnz, int32_t stages, i
     if (tile_nnz < 0 || tile_nnz > 8192) return fail(MPS_ERR_ARG, "tile_nnz must be in [0, 8192]");
     MPS_CUDA(spmv_plan_build(h->A, tile_nnz < 256 && tile_nnz > 0 ? 256 : tile_nnz, s, stages,
                              evict_first < 0 ? -1 : (evict_first ? 1 : 0)));
+    MPS_CUDA(factor_plans_follow(h, s));
     h->H.drop_graphs();
     return MPS_OK;
 }
@@ -282,6 +283,7 @@ mps_status mps_csr_autotune_spmv(mps_csr* h, int32_t* h_tile_nnz, int32_t* h_sta
     if (e1) cudaEventDestroy(e1);
     cudaFree(buf);
     if (e == cudaSuccess) e = spmv_plan_build(h->A, bt, s, bs, bh);
+    if (e == cudaSuccess) e = factor_plans_follow(h, s);
     if (e != cudaSuccess) return cuda_fail(e, "autotune_spmv");
     h->H.drop_graphs();        // captured solves hold the old plan's launch shapes
     if (h_tile_nnz) *h_tile_nnz = bt;
@@ -303,6 +305,14 @@ mps_status mps_csr_spmv_dot(const mps_csr* hc, const float* d_x, const float* d_
 }  // extern "C"
 
 namespace mps {
+cudaError_t factor_plans_follow(mps_csr* h, cudaStream_t s) {
+    cudaError_t e = cudaSuccess;
+    if (h->G.rp && h->G.n_rows) e = spmv_plan_build(h->G, 0, s, h->A.plan.stages, h->A.plan.evict_first);
+    if (e == cudaSuccess && h->Gt.rp && h->Gt.n_rows)
+        e = spmv_plan_build(h->Gt, 0, s, h->A.plan.stages, h->A.plan.evict_first);
+    return e;
+}
+
 mps_status prepare_precond(mps_csr* h, const mps_solve_opts* o, cudaStream_t s) {
     MPS_CUDA(h->H.ensure(h->A.n_rows));
     const int pc = o ? o->precond : 0;
@@ -380,6 +390,7 @@ mps_status mps_csr_set_fsai(mps_csr* h, const int32_t* d_g_row_ptr, const int32_
                          reinterpret_cast<const uint32_t*>(h->G.v), g_nnz, n, n, h->d_err, s);
     cudaFreeAsync(keys, s);
     if (st != MPS_OK) return st;
+    MPS_CUDA(factor_plans_follow(h, s));
     h->has_fsai = true;
     return MPS_OK;
 }
@@ -450,6 +461,7 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
     io.tol = inner_tol;
     io.max_iter = max_inner;
     io.precond = o.precond;
+    io.host_loop = o.host_loop;
     mps_status st = prepare_precond(h, &io, s);
     if (st != MPS_OK) return st;
     MPS_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), s));

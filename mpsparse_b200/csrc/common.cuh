@@ -21,6 +21,17 @@ enum : unsigned {
 // mbarrier waits).  With the nanosleep back-off this is well under a second.
 constexpr unsigned kSpinLimit = 1u << 22;
 
+// Programmatic dependent launch: a kernel launched with the programmatic
+// serialization attribute starts while its predecessor drains and waits here
+// until the predecessor has completed and its writes are visible; it then lets
+// its own successor begin launching.  Without the attribute both are no-ops.
+// Every kernel the solvers launch with the attribute calls this first, before
+// touching memory.
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;

@@ -39,6 +39,7 @@ template <bool BF16, class Epi, int NB, int NT = kNT>
 __global__ void __launch_bounds__(NT, 4)
 spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
     static_assert(NB >= 2 && NB <= 4, "2 to 4 stages");
+    pdl_begin();
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ unsigned long long bar[NB];
     __shared__ int4 s_meta[NB];

@@ -11,6 +11,31 @@ cudaError_t transpose_keys_launch(const CsrMat& A, unsigned long long* keys, cud
 cudaError_t to_bf16_launch(const float* v, __nv_bfloat16* o, uint64_t n, cudaStream_t s);
 int default_tile_nnz(uint64_t nnz, uint32_t n_rows);
 
+// Programmatic dependent launch for the solver kernels (each calls
+// pdl_begin() first): the next kernel's launch overlaps the tail of the
+// current one.  On unless MPS_PDL=0; a graph capture that rejects it is
+// retried without it (pdl_suspend).
+bool pdl_enabled();
+void pdl_suspend(bool off);
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(void (*k)(KArgs...), dim3 g, dim3 b, size_t smem, cudaStream_t s,
+                            Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = g;
+    cfg.blockDim = b;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    if (pdl_enabled()) {
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+    }
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 template <class K>
 inline void smem_optin_k(K kernel, size_t smem) {
     if (smem > 48 * 1024)
@@ -54,7 +79,7 @@ struct CsrOp {
         const size_t smem = NB * stream_buf_bytes<BF16>(v.cap, v.rcap);
         smem_optin_k(spmv_stream<BF16, Epi, NB>, smem);
         const int g = persistent_grid(spmv_stream<BF16, Epi, NB>, smem, v.ntiles);
-        spmv_stream<BF16, Epi, NB><<<g, kNT, smem, s>>>(v, x, e);
+        launch_k(spmv_stream<BF16, Epi, NB>, dim3(g), dim3(kNT), smem, s, v, x, e);
     }
 };
 
@@ -148,7 +173,7 @@ cudaError_t launch_init(SolverKind kind, int precond, const Op& op, const Precon
     DevScalars* sc = H.ws.sc;
     switch (kind) {
         case kCG:
-            cg_init<<<g, kNT, 0, s>>>(H.v4(vB), H.v4(vX), H.v4(vR), H.v4(vP),
+            launch_k(cg_init, dim3(g), dim3(kNT), 0, s, H.v4(vB), H.v4(vX), H.v4(vR), H.v4(vP),
                                       reinterpret_cast<const float4*>(H.dinv), n4, H.n,
                                       H.ws.d_params, c);
             if (precond == MPS_PRECOND_FSAI) {
@@ -159,11 +184,11 @@ cudaError_t launch_init(SolverKind kind, int precond, const Op& op, const Precon
             }
             break;
         case kBiCG:
-            bicg_init<<<g, kNT, 0, s>>>(H.v4(vB), H.v4(vX), H.v4(vR), H.v4(vR0), H.v4(vP),
+            launch_k(bicg_init, dim3(g), dim3(kNT), 0, s, H.v4(vB), H.v4(vX), H.v4(vR), H.v4(vR0), H.v4(vP),
                                         H.v4(vQ), n4, H.n, H.ws.d_params, c);
             break;
         case kRich:
-            rich_init<<<g, kNT, 0, s>>>(H.v4(vB), H.v4(vX), n4, H.n, H.ws.d_params, c);
+            launch_k(rich_init, dim3(g), dim3(kNT), 0, s, H.v4(vB), H.v4(vX), n4, H.n, H.ws.d_params, c);
             break;
     }
     return cudaGetLastError();
@@ -180,7 +205,7 @@ cudaError_t launch_body(SolverKind kind, int precond, const Op& op, const Precon
         case kCG:
             e = op.apply(H.v(vP), EpiCgPq{H.v(vQ), H.v(vP), sc, c.ctr + 1, c.part}, s);
             if (e != cudaSuccess) return e;
-            cg_update_xr<<<g, kNT, 0, s>>>(H.v4(vX), H.v4(vR), H.v4(vP), H.v4(vQ),
+            launch_k(cg_update_xr, dim3(g), dim3(kNT), 0, s, H.v4(vX), H.v4(vR), H.v4(vP), H.v4(vQ),
                                            precond ? dinv4 : nullptr, n4, c);
             if (precond == MPS_PRECOND_FSAI) {
                 e = pc.G->apply(H.v(vR), EpiFsai1{H.v(vW), sc, c.ctr + 3, c.part}, s);
@@ -188,16 +213,16 @@ cudaError_t launch_body(SolverKind kind, int precond, const Op& op, const Precon
                 e = pc.Gt->apply(H.v(vW), EpiFsai2{H.v(vP), sc}, s);
                 if (e != cudaSuccess) return e;
             }
-            cg_update_p<<<g, kNT, 0, s>>>(H.v4(vP), H.v4(vR), dinv4, n4, c);
+            launch_k(cg_update_p, dim3(g), dim3(kNT), 0, s, H.v4(vP), H.v4(vR), dinv4, n4, c);
             break;
         case kBiCG:
-            bicg_update_p<<<g, kNT, 0, s>>>(H.v4(vP), H.v4(vR), H.v4(vQ), n4, c);
+            launch_k(bicg_update_p, dim3(g), dim3(kNT), 0, s, H.v4(vP), H.v4(vR), H.v4(vQ), n4, c);
             e = op.apply(H.v(vP), EpiBicgV{H.v(vQ), H.v(vR0), sc, c.ctr + 5, c.part}, s);
             if (e != cudaSuccess) return e;
-            bicg_update_s<<<g, kNT, 0, s>>>(H.v4(vS), H.v4(vR), H.v4(vQ), n4, c);
+            launch_k(bicg_update_s, dim3(g), dim3(kNT), 0, s, H.v4(vS), H.v4(vR), H.v4(vQ), n4, c);
             e = op.apply(H.v(vS), EpiBicgT{H.v(vT), H.v(vS), sc, c.ctr + 6, c.part}, s);
             if (e != cudaSuccess) return e;
-            bicg_update_xr<<<g, kNT, 0, s>>>(H.v4(vX), H.v4(vR), H.v4(vP), H.v4(vR0), H.v4(vS),
+            launch_k(bicg_update_xr, dim3(g), dim3(kNT), 0, s, H.v4(vX), H.v4(vR), H.v4(vP), H.v4(vR0), H.v4(vS),
                                              H.v4(vT), H.v4(vXAlt), n4, c);
             break;
         case kRich:
@@ -296,6 +321,12 @@ mps_status run_solve(SolverKind kind, const Op& op, const PrecondOps<Op>& pc, So
             // captured once per (solver, preconditioner) on the handle's
             // private stream; the graph only references handle-owned buffers
             cudaError_t e = build_graph(kind, precond, op, pc, H, gc);
+            if (e != cudaSuccess && pdl_enabled()) {   // retry with plain stream order
+                cudaGetLastError();
+                pdl_suspend(true);
+                e = build_graph(kind, precond, op, pc, H, gc);
+                pdl_suspend(false);
+            }
             if (e != cudaSuccess) return cuda_fail(e, "solver graph capture");
         }
         MPS_CUDA(cudaGraphLaunch(gc.exec, s));
@@ -312,8 +343,9 @@ mps_status run_solve(SolverKind kind, const Op& op, const PrecondOps<Op>& pc, So
     }
     {
         const int nb = (H.n + 255) / 256;
-        copy_result<<<nb < 1184 ? (nb ? nb : 1) : 1184, 256, 0, s>>>(
-            H.v(vX), H.v(vXAlt), H.v(vXAlt), d_x, H.n, kind == kRich ? kResRich : kResX, H.ws.sc);
+        launch_k(copy_result, dim3(nb < 1184 ? (nb ? nb : 1) : 1184), dim3(256), 0, s, H.v(vX),
+                 static_cast<const float*>(H.v(vXAlt)), H.v(vXAlt), d_x, H.n,
+                 kind == kRich ? kResRich : kResX, static_cast<const DevScalars*>(H.ws.sc));
         MPS_CUDA(cudaGetLastError());
     }
     MPS_CUDA(cudaMemcpyAsync(H.ws.h_sc, H.ws.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));

@@ -331,6 +331,7 @@ static mps_status fsai_prepare(mps_csr* h, cudaStream_t s) {
     if (st != MPS_OK) return st;
     // the sorted payload landed in Gt.v: it is the permutation
     MPS_CUDA(cudaMemcpyAsync(w.perm, h->Gt.v, (size_t)nnz_g * 4, cudaMemcpyDeviceToDevice, s));
+    MPS_CUDA(factor_plans_follow(h, s));
     RowInfoDev ri = rinfo_of(w, n);
     row_info_kernel<<<g1(n), 256, 0, s>>>(A.rp, A.ci, A.v, n, ri);
     features_kernel<<<g1(nnz_g), 256, 0, s>>>(nnz_g, w.g_row, h->G.ci, w.g_aidx, A.v, ri, w.X, nullptr);

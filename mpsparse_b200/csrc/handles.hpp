@@ -42,4 +42,6 @@ mps_status prepare_precond(mps_csr* h, const mps_solve_opts* o, cudaStream_t s);
 cudaError_t exclusive_scan_rows(const unsigned* counts, uint64_t n, int32_t* out, unsigned* bsum,
                                 cudaStream_t s);
 void fsai_work_free(FsaiWork& w);
+// Rebuild the SpMV plans of G and G^T with A's pipeline depth and L2 hint.
+cudaError_t factor_plans_follow(mps_csr* h, cudaStream_t s);
 }  // namespace mps

@@ -82,6 +82,7 @@ static __global__ void __launch_bounds__(kNT)
 cg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restrict__ r,
         float4* __restrict__ p, const float4* __restrict__ dinv, int n4, int n,
         const SolveParams* __restrict__ prm, Ctx c) {
+    pdl_begin();
     const int mode = prm->precond;
     double acc[2] = {0.0, 0.0};
     MPS_GRID_STRIDE(i, n4) {
@@ -214,6 +215,7 @@ static __device__ void cg_finalize_xr(DevScalars* s, double rr_new, double rz_ja
 static __global__ void __launch_bounds__(kNT)
 cg_update_xr(float4* __restrict__ x, float4* __restrict__ r, const float4* __restrict__ p,
              const float4* __restrict__ q, const float4* __restrict__ dinv, int n4, Ctx c) {
+    pdl_begin();
     if (c.sc->done) return;
     const float a = (float)c.sc->alpha;
     double acc[2] = {0.0, 0.0};
@@ -235,6 +237,7 @@ cg_update_xr(float4* __restrict__ x, float4* __restrict__ r, const float4* __res
 static __global__ void __launch_bounds__(kNT)
 cg_update_p(float4* __restrict__ p, const float4* __restrict__ r, const float4* __restrict__ dinv,
             int n4, Ctx c) {
+    pdl_begin();
     DevScalars* s = c.sc;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         loop_watchdog(s);
@@ -312,6 +315,7 @@ static __global__ void __launch_bounds__(kNT)
 bicg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restrict__ r,
           float4* __restrict__ r0, float4* __restrict__ p, float4* __restrict__ v, int n4, int n,
           const SolveParams* __restrict__ prm, Ctx c) {
+    pdl_begin();
     double acc[1] = {0.0};
     MPS_GRID_STRIDE(i, n4) {
         const float4 bv = b[i];
@@ -366,6 +370,7 @@ bicg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restri
 static __global__ void __launch_bounds__(kNT)
 bicg_update_p(float4* __restrict__ p, const float4* __restrict__ r, const float4* __restrict__ v,
               int n4, Ctx c) {
+    pdl_begin();
     DevScalars* s = c.sc;
     if (s->done) return;
     if (s->iter == 0) {
@@ -412,6 +417,7 @@ struct EpiBicgV {
 static __global__ void __launch_bounds__(kNT)
 bicg_update_s(float4* __restrict__ s_, const float4* __restrict__ r, const float4* __restrict__ v,
               int n4, Ctx c) {
+    pdl_begin();
     if (c.sc->done) return;
     const float a = (float)c.sc->alpha;
     MPS_GRID_STRIDE(i, n4) s_[i] = axpy4(-a, v[i], r[i]);
@@ -446,6 +452,7 @@ static __global__ void __launch_bounds__(kNT)
 bicg_update_xr(float4* __restrict__ x, float4* __restrict__ r, const float4* __restrict__ p,
                const float4* __restrict__ r0, const float4* __restrict__ s_,
                const float4* __restrict__ t, float4* __restrict__ xsnap, int n4, Ctx c) {
+    pdl_begin();
     DevScalars* s = c.sc;
     if (blockIdx.x == 0 && threadIdx.x == 0) loop_watchdog(s);
     if (s->done) {
@@ -521,6 +528,7 @@ bicg_update_xr(float4* __restrict__ x, float4* __restrict__ r, const float4* __r
 static __global__ void __launch_bounds__(kNT)
 rich_init(const float4* __restrict__ b, float4* __restrict__ x0, int n4, int n,
           const SolveParams* __restrict__ prm, Ctx c) {
+    pdl_begin();
     double acc[1] = {0.0};
     MPS_GRID_STRIDE(i, n4) {
         const float4 bv = b[i];
@@ -599,6 +607,7 @@ enum { kResX = 0, kResRich = 1 };
 static __global__ void copy_result(const float* __restrict__ x0, const float* __restrict__ x1,
                             const float* __restrict__ xsnap, float* __restrict__ out, int n,
                             int kind, const DevScalars* __restrict__ sc) {
+    pdl_begin();
     const float* src = x0;
     if (kind == kResRich)
         src = (sc->iter & 1) ? x1 : x0;

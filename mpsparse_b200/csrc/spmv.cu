@@ -1,4 +1,6 @@
 // spmv.cu -- SpMV tile plans, plain SpMV launches and CSR utilities.
+#include <atomic>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 
@@ -172,6 +174,24 @@ template <class K>
 static void smem_optin(K kernel, size_t smem) {
     if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
+
+namespace {
+std::atomic<int> g_pdl{-1};
+thread_local bool t_pdl_off = false;
+}  // namespace
+
+bool pdl_enabled() {
+    if (t_pdl_off) return false;
+    int v = g_pdl.load();
+    if (v < 0) {
+        const char* e = std::getenv("MPS_PDL");
+        v = (e && e[0] == '0') ? 0 : 1;
+        g_pdl.store(v);
+    }
+    return v == 1;
+}
+
+void pdl_suspend(bool off) { t_pdl_off = off; }
 
 int resident_ctas(const void* kernel, int threads, size_t smem) {
     static std::mutex mu;

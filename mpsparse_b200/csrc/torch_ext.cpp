@@ -243,7 +243,7 @@ public:
 
     py::dict cg_mixed(torch::Tensor b, torch::Tensor x, double tol, double inner_tol,
                       int64_t max_outer, int64_t max_inner, int64_t value_bits,
-                      const std::string& precond) {
+                      const std::string& precond, bool host_loop) {
         c10::cuda::CUDAGuard g(device_);
         TORCH_CHECK(b.numel() >= n_rows_ && x.numel() >= n_cols_, "b / x too short");
         auto bd = on_device(b, torch::kFloat64, "b");
@@ -257,6 +257,7 @@ public:
         o.max_inner = (int32_t)max_inner;
         o.value_bits = (int32_t)value_bits;
         o.precond = precond_code(precond);
+        o.host_loop = host_loop ? 1 : 0;
         mps_ir_info info{};
         mps_status s;
         {
@@ -615,7 +616,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
              py::arg("host_loop") = false)
         .def("cg_mixed", &CsrTensor::cg_mixed, py::arg("b"), py::arg("x"), py::arg("tol") = 1e-10,
              py::arg("inner_tol") = 1e-3, py::arg("max_outer") = 50, py::arg("max_inner") = 2000,
-             py::arg("value_bits") = 32, py::arg("precond") = "none")
+             py::arg("value_bits") = 32, py::arg("precond") = "none", py::arg("host_loop") = false)
         .def("set_fsai", &CsrTensor::set_fsai, py::arg("row_ptr"), py::arg("col_ind"),
              py::arg("values"))
         .def("attach_fsai", &CsrTensor::attach_fsai, py::arg("model"))
