@@ -182,11 +182,17 @@ typedef struct {
     int32_t value_bits;       /* 32 or 16 */
     int32_t precond;          /* MPS_PRECOND_NONE / JACOBI / FSAI for the inner CG */
     int32_t host_loop;        /* inner CG iterations launched from the host (see mps_solve_opts) */
-    int32_t reserved;
+    int32_t ir_mode;          /* MPS_IR_AUTO: reliable updates for FP32 values, restarted
+                                 refinement for BF16; MPS_IR_RESTART: x += CG(b - A x) sweeps,
+                                 each to inner_tol; MPS_IR_REPLACE: one FP32 PCG whose
+                                 residual is replaced by the FP64 b - A x each time it has
+                                 dropped by inner_tol, with x accumulated in FP64 */
 } mps_ir_opts;
 
+enum { MPS_IR_AUTO = 0, MPS_IR_RESTART = 1, MPS_IR_REPLACE = 2 };
+
 typedef struct {
-    int32_t outer_iters;
+    int32_t outer_iters;      /* refinement sweeps (restart) or residual replacements */
     int32_t inner_iters;      /* total inner CG iterations */
     int32_t converged;
     int32_t reserved;

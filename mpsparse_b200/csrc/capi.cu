@@ -491,6 +491,45 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
     int outer = 0, inner_total = 0;
     bool converged = false;
     double rel = 1.0;
+    if (o.ir_mode < MPS_IR_AUTO || o.ir_mode > MPS_IR_REPLACE || (o.ir_mode == MPS_IR_REPLACE && bf16)) {
+        cudaFreeAsync(scal, s);
+        return fail(MPS_ERR_ARG, o.ir_mode == MPS_IR_REPLACE ? "reliable updates run on FP32 values"
+                                                              : "unknown ir_mode");
+    }
+    if (!bf16 && o.ir_mode != MPS_IR_RESTART && bnorm > 0 && std::isfinite(bnorm)) {
+        // Reliable updates: one FP32 PCG, x in FP64, r replaced by the FP64
+        // b - A x whenever it has dropped by inner_tol; then the FP64 true
+        // residual of the result for the report.
+        mps_solve_opts ro = io;
+        ro.tol = tol;
+        const long cap = (long)max_inner * max_outer;
+        ro.max_iter = cap > (1L << 30) ? (1 << 30) : (int)cap;
+        mps_solve_info ii{};
+        int rep = 0;
+        st = run_solve(kCG, inner, pc, H, nullptr, nullptr, &ro, &ii, s, 0, d_b, d_x, inner_tol, &rep);
+        if (st == MPS_OK) {
+            spmv_tiles<double, double, false, EpiResid64><<<h->A.plan.grid, kNT, smem, s>>>(
+                view, d_x, EpiResid64{d_b, r32, scal + 1, H.ws.counters + 14, H.ws.partials});
+            st = cudaGetLastError() == cudaSuccess ? MPS_OK : cuda_fail(cudaErrorLaunchFailure, "residual");
+        }
+        if (st == MPS_OK) {
+            MPS_CUDA(cudaMemcpyAsync(hs + 1, scal + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+            MPS_CUDA(cudaStreamSynchronize(s));
+            rel = std::sqrt(hs[1]) / bnorm;
+        }
+        cudaFreeAsync(scal, s);
+        unsigned err = 0;
+        MPS_CUDA(cudaMemcpy(&err, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        if (st == MPS_OK && (err & kErrTimeout)) st = fail(MPS_ERR_TIMEOUT, "SpMV: a bulk-copy wait gave up");
+        if (info) {
+            info->outer_iters = rep;
+            info->inner_iters = ii.iters;
+            info->converged = ii.converged && rel <= tol;
+            info->reserved = 0;
+            info->rel_resid = rel;
+        }
+        return st;
+    }
     for (;; ++outer) {
         // FP64 outer residual r = b - A x (FP32 copy feeds the inner solve)
         spmv_tiles<double, double, false, EpiResid64><<<h->A.plan.grid, kNT, smem, s>>>(

@@ -1,6 +1,8 @@
 // driver.hpp -- host driver shared by the CSR and BCSR solvers: workspace,
 // graph capture with a device-side WHILE loop, result and info read-back.
 #pragma once
+#include <type_traits>
+
 #include "solvers.cuh"
 #include "csr_stream.cuh"
 
@@ -90,6 +92,8 @@ enum VecSlot { vB = 0, vX, vR, vP, vQ, vR0, vS, vT, vXAlt, vW, vTmp0, vTmp1 };
 struct SolverHost {
     Workspace ws;
     GraphCache graphs[32];
+    GraphCache graphs_ir[4];           // reliable-update CG per preconditioner
+    double* v64 = nullptr;             // reliable updates: x (FP64) | b (FP64), n_pad each
     cudaStream_t cap = nullptr;
     SolveParams* h_params = nullptr;   // pinned
     float* dinv = nullptr;             // padded
@@ -131,7 +135,18 @@ struct SolverHost {
         ws.n_pad = n_pad ? n_pad : 4;
         return cudaSuccess;
     }
+    cudaError_t ensure_ir() {
+        if (v64) return cudaSuccess;
+        return cudaMalloc(&v64, 2 * ws.n_pad * sizeof(double));
+    }
+    double* x64() const { return v64; }
+    double* b64() const { return v64 + ws.n_pad; }
     void drop_graphs() {
+        for (auto& g : graphs_ir) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            if (g.graph) cudaGraphDestroy(g.graph);
+            g = GraphCache{};
+        }
         for (auto& g : graphs) {
             if (g.exec) cudaGraphExecDestroy(g.exec);
             if (g.graph) cudaGraphDestroy(g.graph);
@@ -148,6 +163,8 @@ struct SolverHost {
         if (ws.h_sc) cudaFreeHost(ws.h_sc);
         if (h_params) cudaFreeHost(h_params);
         if (dinv) cudaFree(dinv);
+        if (v64) cudaFree(v64);
+        v64 = nullptr;
         ws = Workspace{};
         h_params = nullptr;
         dinv = nullptr;
@@ -168,11 +185,23 @@ struct PrecondOps {
 
 template <class Op>
 cudaError_t launch_init(SolverKind kind, int precond, const Op& op, const PrecondOps<Op>& pc,
-                        SolverHost& H, const Ctx& c, cudaStream_t s) {
+                        SolverHost& H, const Ctx& c, cudaStream_t s, bool ir = false) {
     const int n4 = H.n4(), g = H.vgrid();
     DevScalars* sc = H.ws.sc;
     switch (kind) {
         case kCG:
+            if (ir) {
+                launch_k(cg_init_ir, dim3(g), dim3(kNT), 0, s, static_cast<const double*>(H.b64()), H.x64(),
+                         H.v(vR), H.v(vP), static_cast<const float*>(H.dinv), H.n,
+                         static_cast<const SolveParams*>(H.ws.d_params), c);
+                if (precond == MPS_PRECOND_FSAI) {
+                    cudaError_t e = pc.G->apply(H.v(vR), EpiFsai1{H.v(vW), sc, c.ctr + 3, c.part}, s);
+                    if (e != cudaSuccess) return e;
+                    e = pc.Gt->apply(H.v(vW), EpiFsai2{H.v(vP), sc}, s);
+                    if (e != cudaSuccess) return e;
+                }
+                break;
+            }
             launch_k(cg_init, dim3(g), dim3(kNT), 0, s, H.v4(vB), H.v4(vX), H.v4(vR), H.v4(vP),
                                       reinterpret_cast<const float4*>(H.dinv), n4, H.n,
                                       H.ws.d_params, c);
@@ -196,7 +225,7 @@ cudaError_t launch_init(SolverKind kind, int precond, const Op& op, const Precon
 
 template <class Op>
 cudaError_t launch_body(SolverKind kind, int precond, const Op& op, const PrecondOps<Op>& pc,
-                        SolverHost& H, const Ctx& c, cudaStream_t s) {
+                        SolverHost& H, const Ctx& c, cudaStream_t s, bool ir = false) {
     const int n4 = H.n4(), g = H.vgrid();
     DevScalars* sc = H.ws.sc;
     cudaError_t e = cudaSuccess;
@@ -205,6 +234,28 @@ cudaError_t launch_body(SolverKind kind, int precond, const Op& op, const Precon
         case kCG:
             e = op.apply(H.v(vP), EpiCgPq{H.v(vQ), H.v(vP), sc, c.ctr + 1, c.part}, s);
             if (e != cudaSuccess) return e;
+            if constexpr (std::is_same<Op, CsrOp>::value) {
+                if (ir) {
+                    const float* dv = precond ? H.dinv : nullptr;
+                    launch_k(cg_update_xr_ir, dim3(g), dim3(kNT), 0, s, H.x64(), H.v(vR),
+                             static_cast<const float*>(H.v(vP)), static_cast<const float*>(H.v(vQ)), dv,
+                             H.n, c);
+                    // FP64 true residual when a replacement is due (returns at once otherwise)
+                    const CsrDev view = op.A->view();
+                    const size_t smem = spmv_smem_bytes<double>(view);
+                    smem_optin_k(spmv_tiles<double, double, false, EpiReplace>, smem);
+                    spmv_tiles<double, double, false, EpiReplace><<<op.A->plan.grid, kNT, smem, s>>>(
+                        view, H.x64(), EpiReplace{H.b64(), H.v(vR), dv, sc, c.ctr + 4, c.part});
+                    if (precond == MPS_PRECOND_FSAI) {
+                        e = pc.G->apply(H.v(vR), EpiFsai1{H.v(vW), sc, c.ctr + 3, c.part}, s);
+                        if (e != cudaSuccess) return e;
+                        e = pc.Gt->apply(H.v(vW), EpiFsai2{H.v(vP), sc}, s);
+                        if (e != cudaSuccess) return e;
+                    }
+                    launch_k(cg_update_p, dim3(g), dim3(kNT), 0, s, H.v4(vP), H.v4(vR), dinv4, n4, c);
+                    break;
+                }
+            }
             launch_k(cg_update_xr, dim3(g), dim3(kNT), 0, s, H.v4(vX), H.v4(vR), H.v4(vP), H.v4(vQ),
                                            precond ? dinv4 : nullptr, n4, c);
             if (precond == MPS_PRECOND_FSAI) {
@@ -238,7 +289,7 @@ cudaError_t launch_body(SolverKind kind, int precond, const Op& op, const Precon
 // Capture: [init kernels] -> WHILE(cond) { body kernels }.
 template <class Op>
 cudaError_t build_graph(SolverKind kind, int precond, const Op& op, const PrecondOps<Op>& pc,
-                        SolverHost& H, GraphCache& gc) {
+                        SolverHost& H, GraphCache& gc, bool ir = false) {
     cudaStream_t cs = H.cap;
     cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
@@ -253,7 +304,7 @@ cudaError_t build_graph(SolverKind kind, int precond, const Op& op, const Precon
     if ((e = cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd)) != cudaSuccess) goto abort;
     if ((e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault)) != cudaSuccess)
         goto abort;
-    if ((e = launch_init(kind, precond, op, pc, H, H.ctx(h, 1), cs)) != cudaSuccess) goto abort;
+    if ((e = launch_init(kind, precond, op, pc, H, H.ctx(h, 1), cs, ir)) != cudaSuccess) goto abort;
     if ((e = cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd)) != cudaSuccess) goto abort;
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = h;
@@ -270,7 +321,7 @@ cudaError_t build_graph(SolverKind kind, int precond, const Op& op, const Precon
         cudaGraphDestroy(g);
         return e;
     }
-    e = launch_body(kind, precond, op, pc, H, H.ctx(h, 1), cs);
+    e = launch_body(kind, precond, op, pc, H, H.ctx(h, 1), cs, ir);
     {
         cudaGraph_t b2 = nullptr;
         cudaError_t e2 = cudaStreamEndCapture(cs, &b2);
@@ -298,14 +349,22 @@ abort:
 }
 
 // Run one solve: b (device, n floats) -> x (device, n floats).
+// Reliable-update mode (CG on a CSR only): d_b64 -> d_x64 in FP64, d_b/d_x
+// unused; *replaced receives the number of residual replacements.
 template <class Op>
 mps_status run_solve(SolverKind kind, const Op& op, const PrecondOps<Op>& pc, SolverHost& H,
                      const float* d_b, float* d_x, const mps_solve_opts* o_in,
-                     mps_solve_info* info, cudaStream_t s, int variant = 0) {
+                     mps_solve_info* info, cudaStream_t s, int variant = 0,
+                     const double* d_b64 = nullptr, double* d_x64 = nullptr, double delta = 0.0,
+                     int* replaced = nullptr) {
     mps_solve_opts o;
     mps_solve_opts_default(&o);
     if (o_in) o = *o_in;
+    const bool ir = d_b64 != nullptr;
+    if (ir && (kind != kCG || o.reference_compat || !std::is_same<Op, CsrOp>::value))
+        return fail(MPS_ERR_ARG, "reliable updates run CG on a CSR matrix");
     SolveParams& P = *H.h_params;
+    P.delta = delta;
     P.tol = o.tol > 0 ? o.tol : 1e-6;
     P.omega = o.omega != 0 ? o.omega : 0.01;
     P.max_iter = o.max_iter > 0 ? o.max_iter : 2000;
@@ -314,34 +373,42 @@ mps_status run_solve(SolverKind kind, const Op& op, const PrecondOps<Op>& pc, So
     P.stall_window = o.stall_window > 0 ? o.stall_window : 400;
     const int precond = P.precond;
     MPS_CUDA(cudaMemcpyAsync(H.ws.d_params, H.h_params, sizeof(SolveParams), cudaMemcpyHostToDevice, s));
-    MPS_CUDA(cudaMemcpyAsync(H.v(vB), d_b, (size_t)H.n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    if (ir) {
+        MPS_CUDA(H.ensure_ir());
+        MPS_CUDA(cudaMemcpyAsync(H.b64(), d_b64, (size_t)H.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    } else {
+        MPS_CUDA(cudaMemcpyAsync(H.v(vB), d_b, (size_t)H.n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    }
     if (!o.host_loop) {
-        GraphCache& gc = H.graphs[(kind * 4 + precond) * 2 + (variant & 1)];
+        GraphCache& gc = ir ? H.graphs_ir[precond & 3] : H.graphs[(kind * 4 + precond) * 2 + (variant & 1)];
         if (!gc.exec) {
             // captured once per (solver, preconditioner) on the handle's
             // private stream; the graph only references handle-owned buffers
-            cudaError_t e = build_graph(kind, precond, op, pc, H, gc);
+            cudaError_t e = build_graph(kind, precond, op, pc, H, gc, ir);
             if (e != cudaSuccess && pdl_enabled()) {   // retry with plain stream order
                 cudaGetLastError();
                 pdl_suspend(true);
-                e = build_graph(kind, precond, op, pc, H, gc);
+                e = build_graph(kind, precond, op, pc, H, gc, ir);
                 pdl_suspend(false);
             }
             if (e != cudaSuccess) return cuda_fail(e, "solver graph capture");
         }
         MPS_CUDA(cudaGraphLaunch(gc.exec, s));
     } else {
-        MPS_CUDA(launch_init(kind, precond, op, pc, H, H.ctx({}, 0), s));
+        MPS_CUDA(launch_init(kind, precond, op, pc, H, H.ctx({}, 0), s, ir));
         const int per_poll = 16;
         for (long it = 0;; it += per_poll) {
-            for (int k = 0; k < per_poll; ++k) MPS_CUDA(launch_body(kind, precond, op, pc, H, H.ctx({}, 0), s));
+            for (int k = 0; k < per_poll; ++k)
+                MPS_CUDA(launch_body(kind, precond, op, pc, H, H.ctx({}, 0), s, ir));
             MPS_CUDA(cudaMemcpyAsync(H.ws.h_sc, H.ws.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
             MPS_CUDA(cudaStreamSynchronize(s));
             if (H.ws.h_sc->done) break;
             if (it > 100000000L) return fail(MPS_ERR_TIMEOUT, "host loop did not stop");
         }
     }
-    {
+    if (ir) {
+        MPS_CUDA(cudaMemcpyAsync(d_x64, H.x64(), (size_t)H.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    } else {
         const int nb = (H.n + 255) / 256;
         launch_k(copy_result, dim3(nb < 1184 ? (nb ? nb : 1) : 1184), dim3(256), 0, s, H.v(vX),
                  static_cast<const float*>(H.v(vXAlt)), H.v(vXAlt), d_x, H.n,
@@ -361,6 +428,7 @@ mps_status run_solve(SolverKind kind, const Op& op, const PrecondOps<Op>& pc, So
         const double num = kind == kCG ? r.rr : r.rnorm2;
         info->rel_resid = r.bnorm2 > 0 ? sqrt(num / r.bnorm2) : sqrt(num);
     }
+    if (replaced) *replaced = r.replaced;
     if (r.err & kErrNotFinite) return fail(MPS_ERR_NOT_FINITE, "right-hand side holds NaN or Inf");
     if (r.err & kErrTimeout) return fail(MPS_ERR_TIMEOUT, "solver loop stopped by its watchdog");
     return MPS_OK;

@@ -40,6 +40,11 @@ struct DevScalars {
     int restart;        // next direction update restarts (beta = 0)
     int guard;          // loop bodies executed (watchdog)
     int guard_limit;    // watchdog bound: a loop never runs more bodies than this
+    // reliable updates (mixed-precision CG): FP64 solution, residual replacement
+    double rr_ref;      // largest recurrence ||r||^2 since the last replacement
+    double delta2;      // replace when ||r||^2 < delta2 * rr_ref (or at the target)
+    int replace;        // a replacement is due in this iteration
+    int replaced;       // replacements so far
 };
 
 // Parameters copied host->device before each solve.
@@ -50,6 +55,7 @@ struct SolveParams {
     int compat;
     int precond;
     int stall_window;
+    double delta;       // reliable updates: residual drop between replacements
 };
 
 // ---- CSR views ---------------------------------------------------------------

@@ -77,6 +77,9 @@ __device__ __forceinline__ void loop_watchdog(DevScalars* s) {
 // ============================ CG / PCG =====================================
 // Counter slots: 0 init, 1 pq, 2 xr, 3 G-apply, 4..7 BiCGSTAB, 8 Richardson.
 
+static __device__ void cg_init_scalars(const Ctx& c, const SolveParams* __restrict__ prm, int n,
+                                       int mode, double bb, double bzb);
+
 // x = 0, r = b, p = M b; rr = b.b, rz = b.Mb; stop flags reset.
 static __global__ void __launch_bounds__(kNT)
 cg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restrict__ r,
@@ -101,8 +104,13 @@ cg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restrict
     double tot[2];
     if (!reduce_partials<2>(c, 0, acc, tot)) return;
     if (threadIdx.x != 0) return;
+    cg_init_scalars(c, prm, n, mode, tot[0], tot[1]);
+}
+
+// Scalars of a CG / PCG start: ||b||^2 = bb, b.D^-1 b = bzb.
+static __device__ void cg_init_scalars(const Ctx& c, const SolveParams* __restrict__ prm, int n,
+                                       int mode, double bb, double bzb) {
     DevScalars* s = c.sc;
-    const double bb = tot[0];
     s->n = n;
     s->compat = prm->compat;
     s->max_iter = prm->compat ? (n < 1000 ? n : 1000) : prm->max_iter;
@@ -118,7 +126,7 @@ cg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restrict
     s->restart = (mode == 2) ? 1 : 0;   // the first G-apply starts the direction
     s->bnorm2 = bb;
     s->rr = bb;
-    s->rz = (mode == 1) ? tot[1] : bb;
+    s->rz = (mode == 1) ? bzb : bb;
     s->tol2 = prm->tol * prm->tol * bb;
     s->best_rr = 1e300;
     s->best_iter = 0;
@@ -126,6 +134,10 @@ cg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restrict
     s->rz_jac = 0.0;
     s->guard = 0;
     s->guard_limit = s->max_iter + 8;
+    s->rr_ref = bb;
+    s->delta2 = prm->delta * prm->delta;
+    s->replace = 0;
+    s->replaced = 0;
     if (!isfinite(bb)) {
         s->err = kErrNotFinite;
         s->done = 1;
@@ -170,6 +182,20 @@ struct EpiCgPq {
     }
 };
 
+// beta and rz of the next direction (no preconditioner / Jacobi; the FSAI
+// step sets them from w.w itself).
+static __device__ void cg_direction(DevScalars* s, double rr_new, double rz_jac) {
+    s->rz_jac = rz_jac;
+    if (s->mode == 1) {
+        s->beta = s->restart ? 0.0 : rz_jac / s->rz;
+        s->rz = rz_jac;
+        s->restart = 0;
+    } else if (s->mode == 0) {
+        s->beta = rr_new / s->rz;
+        s->rz = rr_new;
+    }
+}
+
 static __device__ void cg_finalize_xr(DevScalars* s, double rr_new, double rz_jac) {
     const int it = ++s->iter;
     const double rr_old = s->rr;
@@ -200,15 +226,7 @@ static __device__ void cg_finalize_xr(DevScalars* s, double rr_new, double rz_ja
         s->done = 1;
         return;
     }
-    s->rz_jac = rz_jac;
-    if (s->mode == 1) {
-        s->beta = s->restart ? 0.0 : rz_jac / s->rz;
-        s->rz = rz_jac;
-        s->restart = 0;
-    } else if (s->mode == 0) {
-        s->beta = rr_new / s->rz;
-        s->rz = rr_new;
-    }
+    cg_direction(s, rr_new, rz_jac);
 }
 
 // x += alpha p ; r -= alpha q ; rr = r.r (and r.D^-1 r when a diagonal exists)
@@ -231,6 +249,125 @@ cg_update_xr(float4* __restrict__ x, float4* __restrict__ r, const float4* __res
     if (!reduce_partials<2>(c, 2, acc, tot)) return;
     if (threadIdx.x == 0) cg_finalize_xr(c.sc, tot[0], tot[1]);
 }
+
+// ---- reliable updates (mixed-precision CG) ----------------------------------
+// The FP32 recurrences run as above; x is accumulated in FP64, and whenever
+// the recurrence residual has dropped by delta since the last replacement (or
+// reaches the target) r is replaced by the FP64 true residual b - A x
+// (Sleijpen & van der Vorst's reliable updates).  The solve stops only on a
+// replaced, i.e. true, residual.
+
+// x = 0 (FP64), r = (float)b, p = M r; bb = ||b||^2 in FP64.
+static __global__ void __launch_bounds__(kNT)
+cg_init_ir(const double* __restrict__ b, double* __restrict__ x, float* __restrict__ r,
+           float* __restrict__ p, const float* __restrict__ dinv, int n,
+           const SolveParams* __restrict__ prm, Ctx c) {
+    pdl_begin();
+    const int mode = prm->precond;
+    double acc[2] = {0.0, 0.0};
+    MPS_GRID_STRIDE(i, n) {
+        const double bd = b[i];
+        const float bf = (float)bd;
+        x[i] = 0.0;
+        r[i] = bf;
+        float z = bf;
+        if (mode == 1) {
+            z = bf * dinv[i];
+            acc[1] += (double)bf * bf * dinv[i];
+        }
+        if (mode != 2) p[i] = z;
+        acc[0] += bd * bd;
+    }
+    double tot[2];
+    if (!reduce_partials<2>(c, 0, acc, tot)) return;
+    if (threadIdx.x != 0) return;
+    cg_init_scalars(c, prm, n, mode, tot[0], tot[1]);
+}
+
+static __device__ void cg_finalize_ir(DevScalars* s, double rr_new, double rz_jac) {
+    const int it = ++s->iter;
+    s->rr = rr_new;
+    if (!isfinite(rr_new)) {
+        s->breakdown = 1;
+        s->done = 1;
+        return;
+    }
+    if (rr_new > s->rr_ref) s->rr_ref = rr_new;
+    if (rr_new <= s->tol2 || rr_new < s->delta2 * s->rr_ref) {
+        s->replace = 1;                  // the replacement step sets the direction
+        s->rz_jac = rz_jac;
+        return;
+    }
+    if (it >= s->max_iter) {
+        s->done = 1;
+        return;
+    }
+    cg_direction(s, rr_new, rz_jac);
+}
+
+// x += alpha p (FP64) ; r -= alpha q ; rr = r.r, r.D^-1 r
+static __global__ void __launch_bounds__(kNT)
+cg_update_xr_ir(double* __restrict__ x, float* __restrict__ r, const float* __restrict__ p,
+                const float* __restrict__ q, const float* __restrict__ dinv, int n, Ctx c) {
+    pdl_begin();
+    if (c.sc->done) return;
+    const double a = c.sc->alpha;
+    const float af = (float)a;
+    double acc[2] = {0.0, 0.0};
+    MPS_GRID_STRIDE(i, n) {
+        const float pv = p[i];
+        x[i] = fma(a, (double)pv, x[i]);
+        const float rv = fmaf(-af, q[i], r[i]);
+        r[i] = rv;
+        acc[0] += (double)rv * rv;
+        if (dinv) acc[1] += (double)rv * rv * dinv[i];
+    }
+    double tot[2];
+    if (!reduce_partials<2>(c, 2, acc, tot)) return;
+    if (threadIdx.x == 0) cg_finalize_ir(c.sc, tot[0], tot[1]);
+}
+
+// Replacement (runs only when due): r = (float)(b - A x) with FP64 gathers of
+// x and FP64 sums; ||b - A x||^2 and r.D^-1 r; then the stop test and the
+// next direction.
+struct EpiReplace {
+    static constexpr int NS = 2;
+    const double* b;
+    float* r;
+    const float* dinv;
+    DevScalars* sc;
+    unsigned* counter;
+    double* partials;
+    __device__ bool active() const { return !sc->done && sc->replace; }
+    __device__ void tick() const {}
+    __device__ void on_skip() const {}
+    __device__ void row(int i, double s, double* acc) const {
+        const double rt = b[i] - s;
+        const float rf = (float)rt;
+        r[i] = rf;
+        acc[0] += rt * rt;
+        acc[1] += (double)rf * rf * (dinv ? dinv[i] : 1.f);
+    }
+    __device__ void finalize(const double* tot) const {
+        DevScalars* s = sc;
+        s->replace = 0;
+        ++s->replaced;
+        const double rr = tot[0];
+        s->rr = rr;
+        s->rr_ref = rr;
+        if (!isfinite(rr)) {
+            s->breakdown = 1;
+            s->done = 1;
+        } else if (rr <= s->tol2) {
+            s->converged = 1;
+            s->done = 1;
+        } else if (s->iter >= s->max_iter) {
+            s->done = 1;
+        } else {
+            cg_direction(s, rr, tot[1]);
+        }
+    }
+};
 
 // p = z + beta p with z = r (no preconditioner) or D^-1 r (Jacobi).  Last
 // kernel of a CG iteration: writes the WHILE condition.
@@ -353,6 +490,10 @@ bicg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restri
     s->beta = 0.0;
     s->guard = 0;
     s->guard_limit = s->max_iter + 8;
+    s->rr_ref = bb;
+    s->delta2 = prm->delta * prm->delta;
+    s->replace = 0;
+    s->replaced = 0;
     if (!isfinite(bb)) {
         s->err = kErrNotFinite;
         s->done = 1;

@@ -243,7 +243,7 @@ public:
 
     py::dict cg_mixed(torch::Tensor b, torch::Tensor x, double tol, double inner_tol,
                       int64_t max_outer, int64_t max_inner, int64_t value_bits,
-                      const std::string& precond, bool host_loop) {
+                      const std::string& precond, bool host_loop, const std::string& ir_mode) {
         c10::cuda::CUDAGuard g(device_);
         TORCH_CHECK(b.numel() >= n_rows_ && x.numel() >= n_cols_, "b / x too short");
         auto bd = on_device(b, torch::kFloat64, "b");
@@ -258,6 +258,10 @@ public:
         o.value_bits = (int32_t)value_bits;
         o.precond = precond_code(precond);
         o.host_loop = host_loop ? 1 : 0;
+        if (ir_mode == "auto" || ir_mode.empty()) o.ir_mode = MPS_IR_AUTO;
+        else if (ir_mode == "restart") o.ir_mode = MPS_IR_RESTART;
+        else if (ir_mode == "replace") o.ir_mode = MPS_IR_REPLACE;
+        else throw std::invalid_argument("ir_mode must be 'auto', 'restart' or 'replace'");
         mps_ir_info info{};
         mps_status s;
         {
@@ -616,7 +620,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
              py::arg("host_loop") = false)
         .def("cg_mixed", &CsrTensor::cg_mixed, py::arg("b"), py::arg("x"), py::arg("tol") = 1e-10,
              py::arg("inner_tol") = 1e-3, py::arg("max_outer") = 50, py::arg("max_inner") = 2000,
-             py::arg("value_bits") = 32, py::arg("precond") = "none", py::arg("host_loop") = false)
+             py::arg("value_bits") = 32, py::arg("precond") = "none", py::arg("host_loop") = false,
+             py::arg("ir_mode") = "auto")
         .def("set_fsai", &CsrTensor::set_fsai, py::arg("row_ptr"), py::arg("col_ind"),
              py::arg("values"))
         .def("attach_fsai", &CsrTensor::attach_fsai, py::arg("model"))
