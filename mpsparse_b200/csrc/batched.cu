@@ -91,8 +91,40 @@ __device__ __forceinline__ float row_dot(const int* __restrict__ rp, const int* 
     return s;
 }
 
+// Rows i and j (j valid when has_j) of A times x, with up to 8 independent
+// gathers in flight per thread: a group spends most of an iteration waiting
+// on gathers, so two rows' chains are interleaved.  Summation order within a
+// row is the same as row_dot's.
+__device__ __forceinline__ void row_dot2(const int* __restrict__ rp, const int* __restrict__ ci,
+                                         const float* __restrict__ v, const float* x, int i, int j,
+                                         bool has_j, float& s0, float& s1) {
+    const int b0 = __ldg(rp + i), e0 = __ldg(rp + i + 1);
+    const int b1 = has_j ? __ldg(rp + j) : 0, e1 = has_j ? __ldg(rp + j + 1) : 0;
+    s0 = 0.f;
+    s1 = 0.f;
+    const int len = max(e0 - b0, e1 - b1);
+    for (int k = 0; k < len; k += 4) {
+        float x0[4], x1[4], v0[4], v1[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const bool in0 = b0 + k + u < e0, in1 = b1 + k + u < e1;
+            const int c0 = in0 ? __ldg(ci + b0 + k + u) : 0;
+            const int c1 = in1 ? __ldg(ci + b1 + k + u) : 0;
+            v0[u] = in0 ? __ldg(v + b0 + k + u) : 0.f;
+            v1[u] = in1 ? __ldg(v + b1 + k + u) : 0.f;
+            x0[u] = in0 ? x[c0] : 0.f;
+            x1[u] = in1 ? x[c1] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (b0 + k + u < e0) s0 = fmaf(v0[u], x0[u], s0);
+            if (b1 + k + u < e1) s1 = fmaf(v1[u], x1[u], s1);
+        }
+    }
+}
+
 template <int WPS>
-__global__ void __launch_bounds__(kBatchNT)
+__global__ void __launch_bounds__(kBatchNT, 2)
 batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchOut out, double tol,
           int max_iter, int stall_window, unsigned* queue) {
     constexpr int GS = WPS * 32;
@@ -148,10 +180,16 @@ batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchO
         }
         while (!conv && it < max_iter) {
             double a[1] = {0.0};
-            for (int i = lo + lt; i < hi; i += GS) {
-                const float qv = row_dot(B.rp, B.ci, B.v, B.p, i);
-                B.q[i] = qv;
-                a[0] += (double)B.p[i] * qv;
+            for (int i = lo + lt; i < hi; i += 2 * GS) {
+                const int j = i + GS;
+                float q0, q1;
+                row_dot2(B.rp, B.ci, B.v, B.p, i, j, j < hi, q0, q1);
+                B.q[i] = q0;
+                a[0] += (double)B.p[i] * q0;
+                if (j < hi) {
+                    B.q[j] = q1;
+                    a[0] += (double)B.p[j] * q1;
+                }
             }
             group_reduce<WPS, 1>(a, red[g], g, lt);
             if (!(a[0] > 0.0)) break;             // breakdown (not SPD)
@@ -174,10 +212,16 @@ batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchO
             double beta;
             if (mode == 2) {
                 double d[1] = {0.0};
-                for (int i = lo + lt; i < hi; i += GS) {
-                    const float wi = row_dot(B.grp, B.gci, B.gv, B.r, i);
-                    B.w[i] = wi;
-                    d[0] += (double)wi * wi;
+                for (int i = lo + lt; i < hi; i += 2 * GS) {
+                    const int j = i + GS;
+                    float w0, w1;
+                    row_dot2(B.grp, B.gci, B.gv, B.r, i, j, j < hi, w0, w1);
+                    B.w[i] = w0;
+                    d[0] += (double)w0 * w0;
+                    if (j < hi) {
+                        B.w[j] = w1;
+                        d[0] += (double)w1 * w1;
+                    }
                 }
                 group_reduce<WPS, 1>(d, red[g], g, lt);
                 if (stall_window > 0 && !(d[0] < 0.25 * best) && it - best_it >= stall_window) {
@@ -194,8 +238,13 @@ batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchO
                 beta = d[0] / rz;
                 rz = d[0];
                 const float bf = (float)beta;
-                for (int i = lo + lt; i < hi; i += GS)
-                    B.p[i] = fmaf(bf, B.p[i], row_dot(B.gtrp, B.gtci, B.gtv, B.w, i));
+                for (int i = lo + lt; i < hi; i += 2 * GS) {
+                    const int j = i + GS;
+                    float z0, z1;
+                    row_dot2(B.gtrp, B.gtci, B.gtv, B.w, i, j, j < hi, z0, z1);
+                    B.p[i] = fmaf(bf, B.p[i], z0);
+                    if (j < hi) B.p[j] = fmaf(bf, B.p[j], z1);
+                }
             } else {
                 const double rzn = mode == 1 ? c[1] : c[0];
                 beta = rzn / rz;
