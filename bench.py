@@ -54,53 +54,83 @@ def peaks():
 
 # ---------------------------------------------------------------- clocks ----
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock, max clock, power and clock-event reasons of the GPU the run
+    uses, sampled every 200 ms in a background thread through NVML (queries
+    of the driver that do not stall the CUDA stream the way a polling
+    nvidia-smi process does); nvidia-smi is the fallback."""
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
+    def __init__(self, dev: int):
+        self.dev = dev
+        self.rows = []
+        self.stop = threading.Event()
+        self.thread = None
         self.proc = None
         self.path = None
 
+    def _bus_id(self):
+        import torch
+        p = torch.cuda.get_device_properties(self.dev)
+        return f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+
+    def _nvml_loop(self, nv, h):
+        while not self.stop.is_set():
+            try:
+                self.rows.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                                  nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM),
+                                  nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
     def __enter__(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByPciBusId(self._bus_id().encode())
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                ["nvidia-smi", "-i", self._bus_id(), "--query-gpu=clocks.sm,clocks.max.sm,"
+                 "clocks_event_reasons.active", "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+            for line in open(self.path):
+                parts = [q.strip() for q in line.split(",")]
+                try:
+                    self.rows.append((float(parts[0]), float(parts[1]), int(parts[2], 16)))
+                except Exception:
+                    pass
 
     def summary(self):
-        rows = []
-        try:
-            for line in open(self.path):
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        except Exception:
-            pass
-        if not rows:
+        if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        load = [s for s in sm if mx and s > 0.3 * max(mx)] or sm
-        return {"sm_mhz": statistics.median(load) if load else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+        sm = [r[0] for r in self.rows]
+        mx = max(r[1] for r in self.rows)
+        reasons = sorted({name for r in self.rows for name, bit in self.REASONS if r[2] & bit})
+        load = [v for v in sm if v > 0.3 * mx] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.rows), "source": "nvml" if self.proc is None else "nvidia-smi"}
 
 
 # ------------------------------------------------------------- systems -----
@@ -207,26 +237,26 @@ def run_ours(args, rank, world, dev):
         torch.distributed.barrier()
     torch.cuda.synchronize()
     with ClockSampler(dev) as clk:
-        time.sleep(1.0)                       # let the sampler start before timing
+        time.sleep(0.5)                       # let the sampler start before timing
         t_wall0 = time.perf_counter()
         torch.cuda.nvtx.range_push("timed")   # profilers can filter on this range
         times, infos, xs = timed(headline)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
         t_wall = time.perf_counter() - t_wall0
-    if world > 1:
-        torch.distributed.barrier()
+        if world > 1:
+            torch.distributed.barrier()
+        # plain CG and Jacobi-PCG on the same systems (the comparison the metric names)
+        ptimes, pinfos, pxs = timed(solve_plain)
+        jtimes, jinfos, jxs = timed(solve_jacobi)
     clocks = clk.summary()
     # verification (untimed): FP64 true residual of every timed solve
     resid = []
     for k, x in enumerate(xs):
         coo, A, b = systems[warm + k]
         resid.append(true_residual_gpu(A.csr(), b, x))
-    # plain CG on the same systems (the comparison the metric names)
-    ptimes, pinfos, pxs = timed(solve_plain)
     presid = [true_residual_gpu(systems[warm + k][1].csr(), systems[warm + k][2], x)
               for k, x in enumerate(pxs)]
-    jtimes, jinfos, jxs = timed(solve_jacobi)
 
     total_ms = sum(times)
     if world > 1:
@@ -349,12 +379,19 @@ def batched_c5(args, dev):
     rn = torch.zeros(S.n_systems, dtype=torch.float64, device=dev).index_add_(0, seg, r * r)
     bn = torch.zeros(S.n_systems, dtype=torch.float64, device=dev).index_add_(0, seg, b.double() ** 2)
     rel = (rn / bn).sqrt().cpu().numpy()
+    # FP32 attainable accuracy of each system (x is returned in FP32):
+    # 16 * eps32 * || |A| |x| || / ||b||
+    Mabs = torch.sparse_csr_tensor(rp.long(), ci.long(), v.double().abs(), (S.n, S.n))
+    ax = (Mabs @ x.double().abs().unsqueeze(1)).squeeze(1)
+    fn = torch.zeros(S.n_systems, dtype=torch.float64, device=dev).index_add_(0, seg, ax * ax)
+    floor = (16 * 2.0 ** -24 * fn.sqrt() / bn.sqrt()).cpu().numpy()
     ms = statistics.median(times)
     return {"workload": f"{S.n_systems} SPD systems, n log-uniform [1024, 65536], half 2D "
                         "log-normal diffusion (sigma 1, corr 8), half graph Laplacians + 0.01 I",
             "rows": S.n, "nnz": int(S.nnz.sum()), "ms": ms,
             "solves_per_s": S.n_systems / (ms * 1e-3), "converged": int(cv.sum()),
-            "true_resid_max": float(rel.max()), "fp32_floor_note": "FP64-checked per system",
+            "true_resid_max": float(rel.max()),
+            "systems_within_tol_or_fp32_floor": int((rel <= np.maximum(2e-6, floor)).sum()),
             "iters_mean": {"grid": float(it[kinds == 0].mean()), "graph": float(it[kinds == 1].mean())},
             "precond_choice": {str(k): v["chosen"] for k, v in choice.items()},
             "warps_per_system": tune["warps_per_system"], "launches_per_solve": 1}
@@ -369,8 +406,9 @@ def spmv_c3(args, dev):
     m = args.c3_grid
     coo = W.lognormal_diffusion_3d(m, 1.0, 8.0, 0)
     e = torch.empty(0)
-    A = mps.spmv.csr_tensor(torch.from_numpy(coo.keys()), torch.from_numpy(coo.vals), e, e, e,
-                            coo.n, coo.n, fill_outputs=False)
+    keys_d = torch.from_numpy(coo.keys()).to(dev)
+    vals_d = torch.from_numpy(coo.vals).to(dev)
+    A = mps.spmv.csr_tensor(keys_d, vals_d, e, e, e, coo.n, coo.n, fill_outputs=False)
     n, nnz = coo.n, coo.nnz
     del coo
     x = torch.randn(n, device=dev)
@@ -390,9 +428,46 @@ def spmv_c3(args, dev):
     ms = statistics.median(a.elapsed_time(b) for a, b in evs)
     bytes_alg = 8 * nnz + 4 * (n + 1) + 4 * n + 4 * n
     gbs = bytes_alg / (ms * 1e-3) / 1e9
-    return {"workload": f"{m}^3 7-pt log-normal diffusion", "n": n, "nnz": nnz,
-            "bytes_per_launch": bytes_alg, "ms": ms, "gbs": gbs, "launches": reps,
-            "plan": {k: plan[k] for k in ("tile_nnz", "stages", "evict_first")}}
+    out = {"workload": f"{m}^3 7-pt log-normal diffusion", "n": n, "nnz": nnz,
+           "bytes_per_launch": bytes_alg, "ms": ms, "gbs": gbs, "launches": reps,
+           "plan": {k: plan[k] for k in ("tile_nnz", "stages", "evict_first")}}
+    if not args.only_spmv:
+        out["vendor"] = vendor_baselines(A, keys_d, vals_d, x, n, nnz, bytes_alg, stream)
+    return out
+
+
+def _event_ms(fn, stream, reps):
+    import torch
+    ts = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    return statistics.median(ts)
+
+
+def vendor_baselines(A, keys, vals, x, n, nnz, bytes_alg, stream):
+    """Library kernels on the same B200 and matrix: cuSPARSE SpMV (through
+    torch's CSR addmv) and CUB's radix sort of the packed keys (torch.sort),
+    beside this library's SpMV and COO -> CSR (sort + row_ptr + tile plan)."""
+    import torch
+    import mpsparse_b200 as mps
+    rp, ci, v = A.csr()
+    M = torch.sparse_csr_tensor(rp, ci, v, (n, n))
+    for _ in range(3):
+        torch.mv(M, x)
+    sp_ms = _event_ms(lambda: torch.mv(M, x), stream, 20)
+    del M
+    sort_ms = _event_ms(lambda: torch.sort(keys), stream, 3)
+    e = torch.empty(0)
+    ours_ms = _event_ms(lambda: mps.spmv.csr_tensor(keys, vals, e, e, e, n, n, fill_outputs=False),
+                        stream, 3)
+    return {"cusparse_spmv_ms": sp_ms, "cusparse_spmv_gbs": bytes_alg / (sp_ms * 1e-3) / 1e9,
+            "cub_sort_keys_ms": sort_ms, "ours_coo_to_csr_ms": ours_ms,
+            "ours_coo_to_csr_gbs_onepass_model": (20 * nnz + 4 * (n + 1)) / (ours_ms * 1e-3) / 1e9}
 
 
 # --------------------------------------------------------- CPU baselines ---

@@ -113,12 +113,39 @@ bcsr_tiles(BcsrDev A, const float* __restrict__ x, Epi epi) {
             const int br = bs + lr / B, k = lr % B;
             const int jb = A.rp[br], je = A.rp[br + 1];
             float s = 0.f;
-            if (use_smem) {
-                const float* base = buf[b] + (size_t)(jb - j0) * BB + k * B;
-                for (int j = jb; j < je; ++j, base += BB) s += block_row_dot<B>(base, x, A.ci[j]);
-            } else {
-                for (int j = jb; j < je; ++j)
-                    s += block_row_dot<B>(A.v + (size_t)j * BB + k * B, x, A.ci[j]);
+            // UJ blocks per round: their column indices and x segments are
+            // all requested before the first product, so a block row costs
+            // ceil(blocks / UJ) gather round trips instead of one per block.
+            constexpr int UJ = B == 4 ? 8 : 4;
+            for (int j = jb; j < je; j += UJ) {
+                int cj[UJ];
+#pragma unroll
+                for (int u = 0; u < UJ; ++u) cj[u] = j + u < je ? __ldg(A.ci + j + u) : -1;
+                float4 xv[UJ][B / 4];
+#pragma unroll
+                for (int u = 0; u < UJ; ++u)
+#pragma unroll
+                    for (int q = 0; q < B / 4; ++q)
+                        xv[u][q] = cj[u] >= 0
+                                       ? __ldg(reinterpret_cast<const float4*>(x + (size_t)cj[u] * B) + q)
+                                       : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int u = 0; u < UJ; ++u) {
+                    if (cj[u] < 0) break;
+                    const float* row = use_smem ? buf[b] + (size_t)(j + u - j0) * BB + k * B
+                                                : A.v + (size_t)(j + u) * BB + k * B;
+                    const float4* r4 = reinterpret_cast<const float4*>(row);
+                    float bsum = 0.f;
+#pragma unroll
+                    for (int q = 0; q < B / 4; ++q) {
+                        const float4 a = r4[q];
+                        bsum = fmaf(a.x, xv[u][q].x, bsum);
+                        bsum = fmaf(a.y, xv[u][q].y, bsum);
+                        bsum = fmaf(a.z, xv[u][q].z, bsum);
+                        bsum = fmaf(a.w, xv[u][q].w, bsum);
+                    }
+                    s += bsum;
+                }
             }
             epi.row(br * B + k, s, acc);
         }
