@@ -216,17 +216,17 @@ mps_status mps_bcsr_create_from_keys(const uint64_t* d_keys, const float* d_vals
     unsigned *idx = nullptr, *eidx = nullptr, *cnt = nullptr, *bsum = nullptr, *d_err = nullptr;
     int *erp = nullptr, *ebc = nullptr;
     const size_t nz = nnz ? nnz : 1;
-    MPS_CUDA(cudaMallocAsync(&bkeys, nz * 8, s));
-    MPS_CUDA(cudaMallocAsync(&idx, nz * 4, s));
-    MPS_CUDA(cudaMallocAsync(&eidx, nz * 4, s));
-    MPS_CUDA(cudaMallocAsync(&ebc, nz * 4, s));
-    MPS_CUDA(cudaMallocAsync(&erp, ((size_t)nbr + 1) * 4, s));
-    MPS_CUDA(cudaMallocAsync(&cnt, ((size_t)nbr + 1) * 4, s));
-    MPS_CUDA(cudaMallocAsync(&bsum, (((size_t)nbr + 2048) / 2048 + 1) * 4, s));
-    MPS_CUDA(cudaMallocAsync(&d_err, 4, s));
+    MPS_CUDA(stream_alloc(&bkeys, nz * 8, s));
+    MPS_CUDA(stream_alloc(&idx, nz * 4, s));
+    MPS_CUDA(stream_alloc(&eidx, nz * 4, s));
+    MPS_CUDA(stream_alloc(&ebc, nz * 4, s));
+    MPS_CUDA(stream_alloc(&erp, ((size_t)nbr + 1) * 4, s));
+    MPS_CUDA(stream_alloc(&cnt, ((size_t)nbr + 1) * 4, s));
+    MPS_CUDA(stream_alloc(&bsum, (((size_t)nbr + 2048) / 2048 + 1) * 4, s));
+    MPS_CUDA(stream_alloc(&d_err, 4, s));
     MPS_CUDA(cudaMemsetAsync(d_err, 0, 4, s));
     int* brp = nullptr;
-    MPS_CUDA(cudaMallocAsync(&brp, ((size_t)nbr + 1) * 4, s));
+    MPS_CUDA(stream_alloc(&brp, ((size_t)nbr + 1) * 4, s));
     if (nnz)
         block_keys_kernel<<<grid1(nnz), 256, 0, s>>>(reinterpret_cast<const unsigned long long*>(d_keys),
                                                       nnz, (int)block, n_rows, n_cols, bkeys, idx, d_err);

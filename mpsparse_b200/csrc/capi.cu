@@ -1,4 +1,6 @@
 // capi.cu -- extern "C" entry points (include/mpsparse.h) for CSR handles.
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -19,6 +21,26 @@ mps_status cuda_fail(cudaError_t e, const char* what) {
     g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
     return e == cudaErrorMemoryAllocation ? MPS_ERR_OOM : MPS_ERR_CUDA;
 }
+cudaMemPool_t lib_pool() {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = pools.find(d);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = d;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[d] = pool;
+    return pool;
+}
+
 int num_sms() {
     static int sms = 0;
     if (!sms) {
@@ -208,7 +230,7 @@ mps_status mps_coo_to_csr(const uint64_t* d_keys, const float* d_vals, uint64_t 
     if (!d_row_ptr || (nnz && (!d_keys || !d_vals || !d_col_ind || !d_out_vals)))
         return fail(MPS_ERR_ARG, "null pointer");
     unsigned* d_err = nullptr;
-    MPS_CUDA(cudaMallocAsync(&d_err, sizeof(unsigned), s));
+    MPS_CUDA(stream_alloc(&d_err, sizeof(unsigned), s));
     MPS_CUDA(cudaMemsetAsync(d_err, 0, sizeof(unsigned), s));
     cudaError_t e = sort_to_csr(d_keys, reinterpret_cast<const uint32_t*>(d_vals), nnz, n_rows,
                                 n_cols, d_row_ptr, d_col_ind, reinterpret_cast<uint32_t*>(d_out_vals),
@@ -384,7 +406,7 @@ mps_status mps_csr_set_fsai(mps_csr* h, const int32_t* d_g_row_ptr, const int32_
     MPS_CUDA(spmv_plan_build(h->G, 0, s));
     // G^T through the same radix sort on (col<<32 | row) keys.
     unsigned long long* keys = nullptr;
-    MPS_CUDA(cudaMallocAsync(&keys, (g_nnz ? g_nnz : 1) * 8, s));
+    MPS_CUDA(stream_alloc(&keys, (g_nnz ? g_nnz : 1) * 8, s));
     MPS_CUDA(transpose_keys_launch(h->G, keys, s));
     st = build_from_keys(h->Gt, reinterpret_cast<const uint64_t*>(keys),
                          reinterpret_cast<const uint32_t*>(h->G.v), g_nnz, n, n, h->d_err, s);
@@ -472,7 +494,7 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
         MPS_CUDA(to_bf16_launch(h->A.v, h->vb, h->A.nnz, s));
     }
     double* scal = nullptr;   // [0] = ||b||^2, [1] = ||r||^2
-    MPS_CUDA(cudaMallocAsync(&scal, 2 * sizeof(double), s));
+    MPS_CUDA(stream_alloc(&scal, 2 * sizeof(double), s));
     float* r32 = H.v(vTmp0);
     float* d32 = H.v(vTmp1);
     const int g = H.vgrid();

@@ -249,10 +249,11 @@ cudaError_t launch_body(SolverKind kind, int precond, const Op& op, const Precon
                     if (precond == MPS_PRECOND_FSAI) {
                         e = pc.G->apply(H.v(vR), EpiFsai1{H.v(vW), sc, c.ctr + 3, c.part}, s);
                         if (e != cudaSuccess) return e;
-                        e = pc.Gt->apply(H.v(vW), EpiFsai2{H.v(vP), sc}, s);
+                        e = pc.Gt->apply(H.v(vW), EpiFsai2{H.v(vP), sc, nullptr, nullptr, H.v(vR), H.dinv, c, 1}, s);
                         if (e != cudaSuccess) return e;
+                    } else {
+                        launch_k(cg_update_p, dim3(g), dim3(kNT), 0, s, H.v4(vP), H.v4(vR), dinv4, n4, c);
                     }
-                    launch_k(cg_update_p, dim3(g), dim3(kNT), 0, s, H.v4(vP), H.v4(vR), dinv4, n4, c);
                     break;
                 }
             }
@@ -261,10 +262,11 @@ cudaError_t launch_body(SolverKind kind, int precond, const Op& op, const Precon
             if (precond == MPS_PRECOND_FSAI) {
                 e = pc.G->apply(H.v(vR), EpiFsai1{H.v(vW), sc, c.ctr + 3, c.part}, s);
                 if (e != cudaSuccess) return e;
-                e = pc.Gt->apply(H.v(vW), EpiFsai2{H.v(vP), sc}, s);
+                e = pc.Gt->apply(H.v(vW), EpiFsai2{H.v(vP), sc, nullptr, nullptr, H.v(vR), H.dinv, c, 1}, s);
                 if (e != cudaSuccess) return e;
+            } else {
+                launch_k(cg_update_p, dim3(g), dim3(kNT), 0, s, H.v4(vP), H.v4(vR), dinv4, n4, c);
             }
-            launch_k(cg_update_p, dim3(g), dim3(kNT), 0, s, H.v4(vP), H.v4(vR), dinv4, n4, c);
             break;
         case kBiCG:
             launch_k(bicg_update_p, dim3(g), dim3(kNT), 0, s, H.v4(vP), H.v4(vR), H.v4(vQ), n4, c);

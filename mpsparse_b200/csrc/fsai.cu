@@ -282,8 +282,8 @@ static mps_status fsai_prepare(mps_csr* h, cudaStream_t s) {
     if (A.n_rows != A.n_cols) return fail(MPS_ERR_ARG, "FSAI needs a square matrix");
     unsigned* cnt = nullptr;
     unsigned* bsum = nullptr;
-    MPS_CUDA(cudaMallocAsync(&cnt, ((size_t)n + 1) * 4, s));
-    MPS_CUDA(cudaMallocAsync(&bsum, (((size_t)n + 2048) / 2048 + 1) * 4, s));
+    MPS_CUDA(stream_alloc(&cnt, ((size_t)n + 1) * 4, s));
+    MPS_CUDA(stream_alloc(&bsum, (((size_t)n + 2048) / 2048 + 1) * 4, s));
     g_count_kernel<<<g1(n), 256, 0, s>>>(A.rp, A.ci, n, cnt);
     csr_free(h->G);
     csr_free(h->Gt);
@@ -291,7 +291,7 @@ static mps_status fsai_prepare(mps_csr* h, cudaStream_t s) {
     h->H.drop_graphs();
     // the pattern size is needed on the host for the allocations
     int32_t* grp_tmp = nullptr;
-    MPS_CUDA(cudaMallocAsync(&grp_tmp, ((size_t)n + 1) * 4, s));
+    MPS_CUDA(stream_alloc(&grp_tmp, ((size_t)n + 1) * 4, s));
     MPS_CUDA(exclusive_scan_rows(cnt, n, grp_tmp, bsum, s));
     int nnz_g = 0;
     MPS_CUDA(cudaMemcpyAsync(&nnz_g, grp_tmp + n, 4, cudaMemcpyDeviceToHost, s));
@@ -315,8 +315,8 @@ static mps_status fsai_prepare(mps_csr* h, cudaStream_t s) {
     // G^T: sort (col << 32 | row) keys with the G index as payload
     unsigned long long* keys = nullptr;
     uint32_t* idx = nullptr;
-    MPS_CUDA(cudaMallocAsync(&keys, nz * 8, s));
-    MPS_CUDA(cudaMallocAsync(&idx, nz * 4, s));
+    MPS_CUDA(stream_alloc(&keys, nz * 8, s));
+    MPS_CUDA(stream_alloc(&idx, nz * 4, s));
     MPS_CUDA(transpose_keys_launch(h->G, keys, s));
     {
         std::vector<uint32_t> iota((size_t)nnz_g);
@@ -515,7 +515,7 @@ mps_status mps_fsai_mlp_forward(const mps_fsai_model* m, const float* d_X, uint6
                                 cudaStream_t s) {
     if (!m || !d_X || !d_out) return fail(MPS_ERR_ARG, "null argument");
     __nv_bfloat16* xb = nullptr;
-    MPS_CUDA(cudaMallocAsync(&xb, (N + 1) * kNF * 2, s));
+    MPS_CUDA(stream_alloc(&xb, (N + 1) * kNF * 2, s));
     MPS_CUDA(to_bf16_launch(d_X, xb, N * kNF, s));
     MPS_CUDA(mlp_forward_launch(m->packed, xb, (long)N, d_out, m->err, s));
     cudaFreeAsync(xb, s);
@@ -526,7 +526,7 @@ mps_status mps_fsai_mlp_backward(const mps_fsai_model* m, const float* d_X, cons
                                  uint64_t N, float* d_grad, cudaStream_t s) {
     if (!m || !d_X || !d_dout || !d_grad) return fail(MPS_ERR_ARG, "null argument");
     __nv_bfloat16* xb = nullptr;
-    MPS_CUDA(cudaMallocAsync(&xb, (N + 1) * kNF * 2, s));
+    MPS_CUDA(stream_alloc(&xb, (N + 1) * kNF * 2, s));
     MPS_CUDA(to_bf16_launch(d_X, xb, N * kNF, s));
     MPS_CUDA(cudaMemsetAsync(d_grad, 0, kNParam * 4, s));
     MPS_CUDA(mlp_backward_launch(m->packed, xb, d_dout, (long)N, d_grad, m->err, s));

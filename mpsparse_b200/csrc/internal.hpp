@@ -22,6 +22,18 @@ mps_status cuda_fail(cudaError_t e, const char* what);
 
 int num_sms();
 
+// Stream-ordered scratch allocations of the library come from one memory
+// pool per device that keeps its memory after frees (release threshold at
+// the maximum): a large sort's temporary buffers are mapped once, not on
+// every call.  The pool holds at most the library's peak scratch footprint.
+cudaMemPool_t lib_pool();
+template <class T>
+inline cudaError_t stream_alloc(T** p, size_t bytes, cudaStream_t s) {
+    cudaMemPool_t pool = lib_pool();
+    if (!pool) return cudaErrorMemoryAllocation;
+    return cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, pool, s);
+}
+
 // ---- device scalar block of one solve --------------------------------------
 // One instance lives in device memory per handle; the host mirrors it into
 // pinned memory at the end of a solve.

@@ -430,18 +430,37 @@ struct EpiFsai1 {
 };
 
 // FSAI step 2: p = G^T w + beta p
+// As the last kernel of an FSAI-PCG iteration (`body`) it also takes
+// cg_update_p's place: it runs the loop watchdog and writes the WHILE
+// condition at its start (the stop decision is final by then), and after a
+// stall fallback it updates p = D^-1 r + beta p instead (the G^T w row sum is
+// then unused).
 struct EpiFsai2 {
     static constexpr int NS = 0;
     float* p;
     DevScalars* sc;
     unsigned* counter = nullptr;
     double* partials = nullptr;
-    __device__ bool active() const { return !sc->done && sc->mode == 2; }
-    __device__ void tick() const {}
+    const float* r = nullptr;      // body only
+    const float* dinv = nullptr;
+    Ctx c = {};
+    int body = 0;
+    __device__ bool active() const { return !sc->done && (body ? sc->mode >= 1 : sc->mode == 2); }
+    __device__ void tick() const {
+        if (body) {
+            loop_watchdog(sc);
+            set_cond(c, !sc->done);
+        }
+    }
     __device__ void on_skip() const {}
-    __device__ void row(int r, float s, double*) const {
+    __device__ void row(int i, float s, double*) const {
         const float beta = (float)__ldcg(&sc->beta);
-        p[r] = fmaf(beta, p[r], s);
+        if (!body || __ldcg(&sc->mode) == 2) {
+            p[i] = fmaf(beta, p[i], s);
+        } else {
+            const float z = r[i] * dinv[i];
+            p[i] = beta != 0.f ? fmaf(beta, p[i], z) : z;
+        }
     }
     __device__ void finalize(const double*) const {}
 };

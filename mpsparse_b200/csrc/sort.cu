@@ -337,7 +337,7 @@ cudaError_t sort_to_csr(const uint64_t* keys, const uint32_t* payload, uint64_t 
     const size_t o_k0 = carve(nnz * 8), o_k1 = carve(nnz * 8), o_v0 = carve(nnz * 4),
                  o_v1 = carve(nnz * 4);
     unsigned char* tmp = nullptr;
-    cudaError_t e = cudaMallocAsync(&tmp, off, s);
+    cudaError_t e = stream_alloc(&tmp, off, s);
     if (e != cudaSuccess) return e;
     unsigned* hist = (unsigned*)(tmp + o_hist);
     unsigned* base = (unsigned*)(tmp + o_base);

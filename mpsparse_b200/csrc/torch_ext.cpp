@@ -561,13 +561,19 @@ void coo_csr_fn(torch::Tensor keys, torch::Tensor values, torch::Tensor row_ptr,
     c10::cuda::CUDAGuard g(k.get_device());
     auto opt = k.options();
     const int64_t nnz = k.numel();
-    auto rp = torch::empty({num_rows + 1}, opt.dtype(torch::kInt32));
-    auto ci = torch::empty({std::max<int64_t>(nnz, 1)}, opt.dtype(torch::kInt32));
-    auto ov = torch::empty({std::max<int64_t>(nnz, 1)}, opt.dtype(torch::kFloat32));
+    // Device outputs are written in place; host outputs through temporaries.
+    auto direct = [&](const torch::Tensor& t) {
+        return t.is_cuda() && t.is_contiguous() && t.get_device() == k.get_device();
+    };
+    const bool in_place = nnz > 0 && direct(row_ptr) && direct(col_ind) && direct(out_vals);
+    auto rp = in_place ? row_ptr : torch::empty({num_rows + 1}, opt.dtype(torch::kInt32));
+    auto ci = in_place ? col_ind : torch::empty({std::max<int64_t>(nnz, 1)}, opt.dtype(torch::kInt32));
+    auto ov = in_place ? out_vals : torch::empty({std::max<int64_t>(nnz, 1)}, opt.dtype(torch::kFloat32));
     check(mps_coo_to_csr(reinterpret_cast<const uint64_t*>(k.data_ptr<int64_t>()), v.data_ptr<float>(),
                          (uint64_t)nnz, (uint32_t)num_rows, (uint32_t)num_cols, rp.data_ptr<int32_t>(),
                          ci.data_ptr<int32_t>(), ov.data_ptr<float>(), cur_stream()),
           "coo_csr");
+    if (in_place) return;
     row_ptr.copy_(rp);
     if (nnz) {
         col_ind.copy_(ci.narrow(0, 0, nnz));
