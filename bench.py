@@ -279,10 +279,11 @@ def run_ours(args, rank, world, dev):
         "value": total_ms / (steps * world),
         "iters_mean": statistics.mean(iters),
         "true_resid_max": max(resid),
-        "plain_cg": {"ms_per_solve": statistics.mean(ptimes),
+        "step_ms": [round(t, 3) for t in times],
+        "plain_cg": {"ms_per_solve": statistics.mean(ptimes), "step_ms": [round(t, 3) for t in ptimes],
                      "iters_mean": statistics.mean(i["iters"] for i in pinfos),
                      "true_resid_max": max(presid)},
-        "jacobi_pcg": {"ms_per_solve": statistics.mean(jtimes),
+        "jacobi_pcg": {"ms_per_solve": statistics.mean(jtimes), "step_ms": [round(t, 3) for t in jtimes],
                        "iters_mean": statistics.mean(i["iters"] for i in jinfos)},
         "outer_mean": statistics.mean(i.get("outer", 0) for i in infos),
         "setup_ms_first_solve": setup_ms,
@@ -609,6 +610,7 @@ def main():
                 "config": {"workload": WORKLOAD, "solver": res["solver"], "tol": TOL,
                            "l2": "flushed between steps (256 MB write)",
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                "step_ms": res["step_ms"],
                 "iters_mean": res["iters_mean"], "outer_mean": res["outer_mean"],
                 "true_resid_max": res["true_resid_max"],
                 "setup_ms_first_solve": res["setup_ms_first_solve"],
