@@ -263,12 +263,20 @@ mps_status mps_batch_attach_fsai(mps_batch* B, const mps_fsai_model* m, cudaStre
  * (the system is not solved: x untouched, iters 0, converged 0, relres -1). */
 #define MPS_BATCH_SKIP 3
 mps_status mps_batch_set_precond(mps_batch* B, const int8_t* h_kind);
-/* Autotuner: time the candidate warps-per-system (1, 2, 4, 8, 16) on a sample
- * spanning the batch's sizes and keep the fastest (h_ms: 5 timings, may be
- * NULL). */
+/* Autotuner: times whole-batch solves with 32, 16, 8, 4, 2, 1 warps per
+ * system (stopping once the time grows) and then the cluster path for the
+ * largest systems, and keeps the fastest (h_ms: the 6 timings for 1, 2, 4,
+ * 8, 16, 32 warps, 0 where not timed; may be NULL).  Overwrites no caller
+ * buffer. */
 mps_status mps_batch_autotune(mps_batch* B, const float* d_b, double tol, int32_t max_iter,
                               int32_t* h_chosen_wps, float* h_ms, cudaStream_t stream);
 int32_t mps_batch_warps_per_system(const mps_batch* B);
+/* How many of the batch's largest systems (only systems of 16,384 rows and
+ * more qualify) are solved by a thread-block cluster each (chosen by
+ * mps_batch_autotune); 0 when the cluster path is off. */
+int32_t mps_batch_uses_clusters(const mps_batch* B);
+/* Set that number by hand (-1: every qualifying system, 0: off). */
+mps_status mps_batch_set_clusters(mps_batch* B, int32_t n_systems);
 /* Solve all systems: per-system iteration count, converged flag (the
  * convergence mask) and recurrence relative residual. */
 mps_status mps_batch_cg(mps_batch* B, const float* d_b, float* d_x, double tol, int32_t max_iter,

@@ -93,8 +93,8 @@ class BatchedSolver:
 
     def autotune(self, b, tol=1e-6, max_iter=20000):
         wps, ms = self.impl.autotune(b, tol, max_iter)
-        return {"warps_per_system": int(wps),
-                "candidates_ms": dict(zip((1, 2, 4, 8, 16), (float(t) for t in ms)))}
+        return {"warps_per_system": int(wps), "systems_on_clusters": int(self.impl.uses_clusters),
+                "candidates_ms": dict(zip((1, 2, 4, 8, 16, 32), (float(t) for t in ms)))}
 
     def solve(self, b, x, tol=1e-6, max_iter=20000):
         """x (CUDA float32, total_rows) is overwritten.  Returns (iters,

@@ -11,9 +11,15 @@
 // the same stall watch and Jacobi fallback as the single-system solver), and a
 // convergence record (iterations, converged flag, relative residual) -- the
 // per-system convergence mask.  WPS (warps per system, hence rows per warp)
-// is chosen by the autotuner, which times candidate launches on a sample of
-// the batch.  No reference counterpart (the reference solves one system per
+// is chosen by the autotuner, which times whole-batch launches.  Systems of
+// at least kBigRows rows can instead be solved by a whole thread-block
+// cluster each (8 CTAs, 4096 threads; cluster barriers and distributed
+// shared memory for the reductions) in a second persistent kernel beside the
+// warp groups; the autotuner keeps that path only when the batch is faster
+// with it.  No reference counterpart (the reference solves one system per
 // call).
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <chrono>
 #include <numeric>
@@ -82,22 +88,99 @@ __device__ __forceinline__ void group_reduce(double* v, double (*red)[4], int g,
     group_sync<WPS>(g);
 }
 
-__device__ __forceinline__ float row_dot(const int* __restrict__ rp, const int* __restrict__ ci,
-                                         const float* __restrict__ v, const float* __restrict__ x,
-                                         int r) {
-    float s = 0.f;
-    const int e = rp[r + 1];
-    for (int k = rp[r]; k < e; ++k) s = fmaf(v[k], x[ci[k]], s);
-    return s;
-}
+// A solving group: WPS warps of one 512-thread CTA (WarpGroup), or the
+// whole of a CS-CTA thread-block cluster (ClusterGroup, for the largest
+// systems).  Both provide the group size, the thread's rank in the group, a
+// group barrier, a fixed-order FP64 all-reduce and the queue pop.
+struct GroupShared {
+    double red[32][4];                 // per-warp partial sums (up to 1024 threads)
+    double cred[2][16][4];             // cluster: per-CTA partials (double-buffered)
+    int next[32];
+    int flip;
+};
 
-// Rows i and j (j valid when has_j) of A times x, with up to 8 independent
-// gathers in flight per thread: a group spends most of an iteration waiting
-// on gathers, so two rows' chains are interleaved.  Summation order within a
-// row is the same as row_dot's.
-__device__ __forceinline__ void row_dot2(const int* __restrict__ rp, const int* __restrict__ ci,
-                                         const float* __restrict__ v, const float* x, int i, int j,
-                                         bool has_j, float& s0, float& s1) {
+template <int WPS>
+struct WarpGroup {
+    static constexpr int GS = WPS * 32;
+    int g, lt;
+    __device__ WarpGroup() : g(threadIdx.x / GS), lt(threadIdx.x % GS) {}
+    __device__ void sync() const { group_sync<WPS>(g); }
+    template <int NS>
+    __device__ void reduce(double* v, GroupShared& sh) const {
+        group_reduce<WPS, NS>(v, reinterpret_cast<double(*)[4]>(&sh.red[g * WPS][0]), g, lt);
+    }
+    __device__ int pop(unsigned* queue, GroupShared& sh) const {
+        if (lt == 0) sh.next[g] = (int)atomicAdd(queue, 1u);
+        sync();
+        const int q = sh.next[g];
+        sync();
+        return q;
+    }
+    __device__ float gather(const float* x, int c) const { return x[c]; }
+};
+
+template <int CS>
+struct ClusterGroup {
+    static constexpr int GS = CS * kBatchNT;
+    int lt;
+    unsigned rank;
+    __device__ ClusterGroup() {
+        rank = cooperative_groups::this_cluster().block_rank();
+        lt = (int)rank * kBatchNT + threadIdx.x;
+    }
+    __device__ void sync() const { cooperative_groups::this_cluster().sync(); }
+    template <int NS>
+    __device__ void reduce(double* v, GroupShared& sh) const {
+        auto cl = cooperative_groups::this_cluster();
+        // CTA sums in a fixed order
+#pragma unroll
+        for (int i = 0; i < NS; ++i) v[i] = warp_sum(v[i]);
+        const int w = threadIdx.x >> 5;
+        if ((threadIdx.x & 31) == 0)
+#pragma unroll
+            for (int i = 0; i < NS; ++i) sh.red[w][i] = v[i];
+        __syncthreads();
+        const int buf = sh.flip;
+        if (threadIdx.x == 0) {
+            double* dst = cl.map_shared_rank(&sh.cred[buf][rank][0], 0);
+#pragma unroll
+            for (int i = 0; i < NS; ++i) {
+                double s = 0.0;
+                for (int k = 0; k < kBatchNT / 32; ++k) s += sh.red[k][i];
+                dst[i] = s;
+            }
+        }
+        cl.sync();   // partials of every CTA are in CTA 0's shared memory
+        const double* src = cl.map_shared_rank(&sh.cred[buf][0][0], 0);
+#pragma unroll
+        for (int i = 0; i < NS; ++i) {
+            double s = 0.0;
+#pragma unroll
+            for (int k = 0; k < CS; ++k) s += src[k * 4 + i];
+            v[i] = s;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) sh.flip = buf ^ 1;
+        __syncthreads();
+    }
+    __device__ int pop(unsigned* queue, GroupShared& sh) const {
+        auto cl = cooperative_groups::this_cluster();
+        if (rank == 0 && threadIdx.x == 0) sh.next[0] = (int)atomicAdd(queue, 1u);
+        cl.sync();
+        const int q = *cl.map_shared_rank(&sh.next[0], 0);
+        cl.sync();   // rank 0 may overwrite next[0] only after every CTA read it
+        return q;
+    }
+    // vectors written by other CTAs of the cluster: read through L2
+    __device__ float gather(const float* x, int c) const { return __ldcg(x + c); }
+};
+
+// Rows i and j of a CSR times x through the group's gather (see row_dot2).
+template <class Grp>
+__device__ __forceinline__ void grp_dot2(const Grp& G, const int* __restrict__ rp,
+                                         const int* __restrict__ ci, const float* __restrict__ v,
+                                         const float* x, int i, int j, bool has_j, float& s0,
+                                         float& s1) {
     const int b0 = __ldg(rp + i), e0 = __ldg(rp + i + 1);
     const int b1 = has_j ? __ldg(rp + j) : 0, e1 = has_j ? __ldg(rp + j + 1) : 0;
     s0 = 0.f;
@@ -112,8 +195,8 @@ __device__ __forceinline__ void row_dot2(const int* __restrict__ rp, const int* 
             const int c1 = in1 ? __ldg(ci + b1 + k + u) : 0;
             v0[u] = in0 ? __ldg(v + b0 + k + u) : 0.f;
             v1[u] = in1 ? __ldg(v + b1 + k + u) : 0.f;
-            x0[u] = in0 ? x[c0] : 0.f;
-            x1[u] = in1 ? x[c1] : 0.f;
+            x0[u] = in0 ? G.gather(x, c0) : 0.f;
+            x1[u] = in1 ? G.gather(x, c1) : 0.f;
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -123,20 +206,17 @@ __device__ __forceinline__ void row_dot2(const int* __restrict__ rp, const int* 
     }
 }
 
-template <int WPS>
-__global__ void __launch_bounds__(kBatchNT, 2)
-batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchOut out, double tol,
-          int max_iter, int stall_window, unsigned* queue) {
-    constexpr int GS = WPS * 32;
-    constexpr int NG = kBatchNT / GS;
-    __shared__ double red[NG][WPS][4];
-    __shared__ int s_next[NG];
-    const int g = threadIdx.x / GS, lt = threadIdx.x % GS;
+// PCG on the systems the queue hands out, one system per group at a time.
+template <class Grp>
+__device__ __forceinline__ void batch_pcg_body(const BatchDev& B, const float* __restrict__ b,
+                                               float* __restrict__ x, const BatchOut& out, double tol,
+                                               int max_iter, int stall_window, unsigned* queue,
+                                               GroupShared& sh) {
+    const Grp G;
+    constexpr int GS = Grp::GS;
+    const int lt = G.lt;
     for (;;) {
-        if (lt == 0) s_next[g] = (int)atomicAdd(queue, 1u);
-        group_sync<WPS>(g);
-        const int qi = s_next[g];
-        group_sync<WPS>(g);
+        const int qi = G.pop(queue, sh);
         if (qi >= B.n_sys) break;
         const int sys = B.order[qi];
         const int lo = B.row_off[sys], hi = B.row_off[sys + 1];
@@ -150,7 +230,7 @@ batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchO
             continue;
         }
         // init: x = 0, r = b, p = M b
-        double acc[3] = {0.0, 0.0, 0.0};
+        double acc[2] = {0.0, 0.0};
         for (int i = lo + lt; i < hi; i += GS) {
             const float bi = b[i];
             x[i] = 0.f;
@@ -160,7 +240,7 @@ batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchO
             acc[0] += (double)bi * bi;
             acc[1] += (double)bi * z;
         }
-        group_reduce<WPS, 2>(acc, red[g], g, lt);
+        G.template reduce<2>(acc, sh);
         const double bb = acc[0];
         double rz = acc[1], rr = bb;
         const double thresh = tol * tol * bb;
@@ -168,22 +248,34 @@ batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchO
         double best = 1e300;
         if (!conv && mode == 2) {                 // p = G^T G b
             double a2[1] = {0.0};
-            for (int i = lo + lt; i < hi; i += GS) {
-                const float wi = row_dot(B.grp, B.gci, B.gv, B.r, i);
-                B.w[i] = wi;
-                a2[0] += (double)wi * wi;
+            for (int i = lo + lt; i < hi; i += 2 * GS) {
+                const int j = i + GS;
+                float w0, w1;
+                grp_dot2(G, B.grp, B.gci, B.gv, B.r, i, j, j < hi, w0, w1);
+                B.w[i] = w0;
+                a2[0] += (double)w0 * w0;
+                if (j < hi) {
+                    B.w[j] = w1;
+                    a2[0] += (double)w1 * w1;
+                }
             }
-            group_reduce<WPS, 1>(a2, red[g], g, lt);
+            G.template reduce<1>(a2, sh);
             rz = a2[0];
-            for (int i = lo + lt; i < hi; i += GS) B.p[i] = row_dot(B.gtrp, B.gtci, B.gtv, B.w, i);
-            group_sync<WPS>(g);
+            for (int i = lo + lt; i < hi; i += 2 * GS) {
+                const int j = i + GS;
+                float z0, z1;
+                grp_dot2(G, B.gtrp, B.gtci, B.gtv, B.w, i, j, j < hi, z0, z1);
+                B.p[i] = z0;
+                if (j < hi) B.p[j] = z1;
+            }
+            G.sync();
         }
         while (!conv && it < max_iter) {
             double a[1] = {0.0};
             for (int i = lo + lt; i < hi; i += 2 * GS) {
                 const int j = i + GS;
                 float q0, q1;
-                row_dot2(B.rp, B.ci, B.v, B.p, i, j, j < hi, q0, q1);
+                grp_dot2(G, B.rp, B.ci, B.v, B.p, i, j, j < hi, q0, q1);
                 B.q[i] = q0;
                 a[0] += (double)B.p[i] * q0;
                 if (j < hi) {
@@ -191,7 +283,7 @@ batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchO
                     a[0] += (double)B.p[j] * q1;
                 }
             }
-            group_reduce<WPS, 1>(a, red[g], g, lt);
+            G.template reduce<1>(a, sh);
             if (!(a[0] > 0.0)) break;             // breakdown (not SPD)
             const float alpha = (float)(rz / a[0]);
             double c[2] = {0.0, 0.0};
@@ -202,7 +294,7 @@ batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchO
                 c[0] += (double)ri * ri;
                 c[1] += (double)ri * ri * B.dinv[i];
             }
-            group_reduce<WPS, 2>(c, red[g], g, lt);
+            G.template reduce<2>(c, sh);
             ++it;
             rr = c[0];
             if (rr <= thresh) {
@@ -215,7 +307,7 @@ batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchO
                 for (int i = lo + lt; i < hi; i += 2 * GS) {
                     const int j = i + GS;
                     float w0, w1;
-                    row_dot2(B.grp, B.gci, B.gv, B.r, i, j, j < hi, w0, w1);
+                    grp_dot2(G, B.grp, B.gci, B.gv, B.r, i, j, j < hi, w0, w1);
                     B.w[i] = w0;
                     d[0] += (double)w0 * w0;
                     if (j < hi) {
@@ -223,12 +315,12 @@ batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchO
                         d[0] += (double)w1 * w1;
                     }
                 }
-                group_reduce<WPS, 1>(d, red[g], g, lt);
+                G.template reduce<1>(d, sh);
                 if (stall_window > 0 && !(d[0] < 0.25 * best) && it - best_it >= stall_window) {
                     mode = 1;                     // stalled: Jacobi from here, restart p
                     rz = c[1];
                     for (int i = lo + lt; i < hi; i += GS) B.p[i] = B.r[i] * B.dinv[i];
-                    group_sync<WPS>(g);
+                    G.sync();
                     continue;
                 }
                 if (d[0] < 0.25 * best) {
@@ -241,7 +333,7 @@ batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchO
                 for (int i = lo + lt; i < hi; i += 2 * GS) {
                     const int j = i + GS;
                     float z0, z1;
-                    row_dot2(B.gtrp, B.gtci, B.gtv, B.w, i, j, j < hi, z0, z1);
+                    grp_dot2(G, B.gtrp, B.gtci, B.gtv, B.w, i, j, j < hi, z0, z1);
                     B.p[i] = fmaf(bf, B.p[i], z0);
                     if (j < hi) B.p[j] = fmaf(bf, B.p[j], z1);
                 }
@@ -255,14 +347,46 @@ batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchO
                     B.p[i] = fmaf(bf, B.p[i], z);
                 }
             }
-            group_sync<WPS>(g);
+            G.sync();
         }
         if (lt == 0) {
             out.iters[sys] = it;
             out.converged[sys] = conv;
             out.relres[sys] = bb > 0.0 ? (float)sqrt(rr / bb) : 0.f;
         }
+        G.sync();   // the next pop must not race this system's last reads
     }
+}
+
+template <int WPS>
+__global__ void __launch_bounds__(kBatchNT, 2)
+batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchOut out, double tol,
+          int max_iter, int stall_window, unsigned* queue) {
+    __shared__ GroupShared sh;
+    batch_pcg_body<WarpGroup<WPS>>(B, b, x, out, tol, max_iter, stall_window, queue, sh);
+}
+
+// 32 warps per system: one 1024-thread CTA per system.
+__global__ void __launch_bounds__(1024, 1)
+batch_pcg_cta(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchOut out,
+              double tol, int max_iter, int stall_window, unsigned* queue) {
+    __shared__ GroupShared sh;
+    batch_pcg_body<WarpGroup<32>>(B, b, x, out, tol, max_iter, stall_window, queue, sh);
+}
+
+// One cluster of kClusterCTAs CTAs per system (launched with the cluster
+// dimension attribute); every CTA of a cluster runs the same control flow,
+// so every cluster barrier is reached by all of them.
+constexpr int kClusterCTAs = 8;
+
+__global__ void __launch_bounds__(kBatchNT, 2)
+batch_pcg_cluster(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchOut out,
+                  double tol, int max_iter, int stall_window, unsigned* queue) {
+    __shared__ GroupShared sh;
+    if (threadIdx.x == 0) sh.flip = 0;
+    cooperative_groups::this_cluster().sync();
+    batch_pcg_body<ClusterGroup<kClusterCTAs>>(B, b, x, out, tol, max_iter, stall_window, queue, sh);
+    cooperative_groups::this_cluster().sync();   // no CTA leaves while another reads its memory
 }
 
 using BatchKernel = void (*)(BatchDev, const float*, float*, BatchOut, double, int, int, unsigned*);
@@ -273,9 +397,12 @@ BatchKernel batch_kernel(int wps) {
         case 2: return batch_pcg<2>;
         case 4: return batch_pcg<4>;
         case 8: return batch_pcg<8>;
-        default: return batch_pcg<16>;
+        case 16: return batch_pcg<16>;
+        default: return batch_pcg_cta;
     }
 }
+
+int batch_threads(int wps) { return wps >= 32 ? 1024 : kBatchNT; }
 
 }  // namespace
 }  // namespace mps
@@ -288,22 +415,30 @@ struct mps_batch {
     std::vector<int> row_off;      // host copy
     int* d_row_off = nullptr;
     int* d_order = nullptr;
-    int* d_sample_order = nullptr;
-    int n_sample = 0;
     signed char* d_kind = nullptr;
     float* d_work = nullptr;       // r, p, q, w
-    unsigned* d_queue = nullptr;
-    int wps = 4;
+    unsigned* d_queue = nullptr;   // [0] warp groups, [1] clusters
+    int wps = 16;
+    // systems with at least kBigRows rows go to one thread-block cluster each
+    int n_big = 0;
+    int clusters = 0;              // the cluster kernel takes this many of the largest systems
+    cudaStream_t side = nullptr;   // the cluster kernel's branch
+    cudaEvent_t fork = nullptr, join = nullptr;
     // one-launch graph of the last call: [queue reset, persistent kernel]
     cudaGraphExec_t exec = nullptr;
     const void* exec_key[5] = {};
     int exec_wps = 0;
+    int exec_clusters = -1;
     double exec_tol = -1.0;
     int exec_max_iter = -1;
     cudaStream_t cap = nullptr;
 };
 
-static BatchDev batch_view(mps_batch* B, bool sample) {
+// Rows from which a system is solved by a cluster of kClusterCTAs CTAs
+// (4096 threads, at least 4 rows each) rather than by warps of one CTA.
+constexpr int kBigRows = 16384;
+
+static BatchDev batch_view(mps_batch* B) {
     mps_csr* h = B->A;
     const size_t n = h->A.n_rows;
     BatchDev d{};
@@ -320,9 +455,9 @@ static BatchDev batch_view(mps_batch* B, bool sample) {
     }
     d.dinv = h->H.dinv;
     d.row_off = B->d_row_off;
-    d.order = sample ? B->d_sample_order : B->d_order;
+    d.order = B->d_order;
     d.kind = B->d_kind;
-    d.n_sys = sample ? B->n_sample : B->n_sys;
+    d.n_sys = B->n_sys;
     d.r = B->d_work;
     d.p = B->d_work + (n + 4);
     d.q = B->d_work + 2 * (n + 4);
@@ -330,15 +465,53 @@ static BatchDev batch_view(mps_batch* B, bool sample) {
     return d;
 }
 
-static mps_status batch_launch(mps_batch* B, int wps, bool sample, const float* b, float* x,
+// One batch: the largest systems (queue order front) on clusters in a side
+// branch, the rest on warp groups, both persistent and fed by their queues.
+static mps_status batch_launch(mps_batch* B, int wps, const float* b, float* x,
                                double tol, int max_iter, int stall_window, BatchOut out,
-                               cudaStream_t s) {
-    BatchKernel k = batch_kernel(wps);
-    int per_sm = resident_ctas(reinterpret_cast<const void*>(k), kBatchNT, 0);
-    const int grid = num_sms() * (per_sm > 0 ? per_sm : 1);
-    MPS_CUDA(cudaMemsetAsync(B->d_queue, 0, sizeof(unsigned), s));
-    k<<<grid, kBatchNT, 0, s>>>(batch_view(B, sample), b, x, out, tol, max_iter, stall_window, B->d_queue);
-    MPS_CUDA(cudaGetLastError());
+                               cudaStream_t s, int use_clusters) {
+    BatchDev all = batch_view(B);
+    const int nb = std::min(std::max(use_clusters, 0), B->n_big);
+    MPS_CUDA(cudaMemsetAsync(B->d_queue, 0, 2 * sizeof(unsigned), s));
+    if (nb > 0) {
+        BatchDev big = all;
+        big.n_sys = nb;
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = kClusterCTAs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.blockDim = dim3(kBatchNT);
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cfg.gridDim = dim3(kClusterCTAs);
+        int max_clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&max_clusters, batch_pcg_cluster, &cfg) != cudaSuccess ||
+            max_clusters < 1)
+            return cuda_fail(cudaGetLastError(), "cluster occupancy");
+        // half of the GPU's clusters at most: the warp groups run beside them
+        int nc = std::min(nb, std::max(1, max_clusters / 2));
+        cfg.gridDim = dim3(nc * kClusterCTAs);
+        cfg.stream = B->side;
+        MPS_CUDA(cudaEventRecord(B->fork, s));
+        MPS_CUDA(cudaStreamWaitEvent(B->side, B->fork, 0));
+        MPS_CUDA(cudaLaunchKernelEx(&cfg, batch_pcg_cluster, big, b, x, out, tol, max_iter, stall_window,
+                                    B->d_queue + 1));
+        MPS_CUDA(cudaEventRecord(B->join, B->side));
+    }
+    BatchDev small = all;
+    small.order = all.order + nb;
+    small.n_sys = all.n_sys - nb;
+    if (small.n_sys > 0) {
+        BatchKernel k = batch_kernel(wps);
+        const int nt = batch_threads(wps);
+        int per_sm = resident_ctas(reinterpret_cast<const void*>(k), nt, 0);
+        const int grid = num_sms() * (per_sm > 0 ? per_sm : 1);
+        k<<<grid, nt, 0, s>>>(small, b, x, out, tol, max_iter, stall_window, B->d_queue);
+        MPS_CUDA(cudaGetLastError());
+    }
+    if (nb > 0) MPS_CUDA(cudaStreamWaitEvent(s, B->join, 0));
     return MPS_OK;
 }
 
@@ -368,25 +541,22 @@ mps_status mps_batch_create(const int32_t* d_row_ptr, const int32_t* d_col_ind, 
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
         return (h_row_off[a + 1] - h_row_off[a]) > (h_row_off[b + 1] - h_row_off[b]);
     });
-    // autotuning sample: every k-th system of the size order (spans all sizes)
-    std::vector<int> sample;
-    const int step = std::max(1, n_systems / 64);
-    for (int i = 0; i < n_systems; i += step) sample.push_back(order[i]);
-    B->n_sample = (int)sample.size();
+    auto rows_of = [&](int sy) { return h_row_off[sy + 1] - h_row_off[sy]; };
+    while (B->n_big < n_systems && rows_of(order[B->n_big]) >= kBigRows) ++B->n_big;
     cudaError_t e = cudaSuccess;
     const size_t n = total_rows;
     if (e == cudaSuccess) e = cudaMalloc(&B->d_row_off, (n_systems + 1) * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&B->d_order, n_systems * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&B->d_sample_order, sample.size() * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&B->d_kind, n_systems);
     if (e == cudaSuccess) e = cudaMalloc(&B->d_work, 4 * (n + 4) * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&B->d_queue, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_queue, 2 * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&B->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B->join, cudaEventDisableTiming);
     if (e == cudaSuccess)
         e = cudaMemcpy(B->d_row_off, h_row_off, (n_systems + 1) * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaMemcpy(B->d_order, order.data(), n_systems * sizeof(int), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess)
-        e = cudaMemcpy(B->d_sample_order, sample.data(), sample.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(B->d_kind, 1, n_systems);   // Jacobi by default
     if (e != cudaSuccess) {
         mps_batch_destroy(B);
@@ -410,12 +580,14 @@ mps_status mps_batch_destroy(mps_batch* B) {
     if (B->A) mps_csr_destroy(B->A);
     cudaFree(B->d_row_off);
     cudaFree(B->d_order);
-    cudaFree(B->d_sample_order);
     cudaFree(B->d_kind);
     cudaFree(B->d_work);
     cudaFree(B->d_queue);
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->cap) cudaStreamDestroy(B->cap);
+    if (B->side) cudaStreamDestroy(B->side);
+    if (B->fork) cudaEventDestroy(B->fork);
+    if (B->join) cudaEventDestroy(B->join);
     delete B;
     return MPS_OK;
 }
@@ -442,7 +614,7 @@ mps_status mps_batch_set_precond(mps_batch* B, const int8_t* h_kind) {
 int32_t mps_batch_warps_per_system(const mps_batch* B) { return B ? B->wps : 0; }
 
 mps_status mps_batch_autotune(mps_batch* B, const float* d_b, double tol, int32_t max_iter,
-                              int32_t* h_chosen_wps, float* h_ms /* 5 candidates */, cudaStream_t s) {
+                              int32_t* h_chosen_wps, float* h_ms /* 6 candidates */, cudaStream_t s) {
     if (!B || !d_b) return fail(MPS_ERR_ARG, "null argument");
     const size_t n = B->A->A.n_rows;
     float* xs = nullptr;
@@ -450,27 +622,74 @@ mps_status mps_batch_autotune(mps_batch* B, const float* d_b, double tol, int32_
     MPS_CUDA(cudaMalloc(&xs, n * sizeof(float)));
     MPS_CUDA(cudaMalloc(&it, 3 * B->n_sys * sizeof(int)));
     BatchOut o{it, it + B->n_sys, reinterpret_cast<float*>(it + 2 * B->n_sys)};
-    const int cands[5] = {1, 2, 4, 8, 16};
+    const int cands[6] = {1, 2, 4, 8, 16, 32};
+    if (h_ms)
+        for (int c = 0; c < 6; ++c) h_ms[c] = 0.f;
     float best = 1e30f;
     int best_w = B->wps;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     mps_status st = MPS_OK;
-    for (int c = 0; c < 5 && st == MPS_OK; ++c) {
+    auto time_one = [&](int w, int cl) {
         float ms = 0.f;
-        for (int rep = 0; rep < 2; ++rep) {   // first run warms up
+        for (int rep = 0; rep < 1 && st == MPS_OK; ++rep) {
             cudaEventRecord(e0, s);
-            st = batch_launch(B, cands[c], true, d_b, xs, tol, max_iter, 400, o, s);
+            st = batch_launch(B, w, d_b, xs, tol, max_iter, 400, o, s, cl);
             if (st != MPS_OK) break;
             cudaEventRecord(e1, s);
             cudaEventSynchronize(e1);
             cudaEventElapsedTime(&ms, e0, e1);
         }
+        return ms;
+    };
+    // Timed on the whole batch (the balance between the largest systems'
+    // latency and the bulk's throughput does not survive sampling): warps
+    // per system from 16 down while the time improves, then the cluster
+    // path for the largest systems on or off.
+    (void)time_one(32, 0);                    // warm-up
+    int cl = 0;
+    float prev = 1e30f;
+    for (int c = 5; c >= 0 && st == MPS_OK; --c) {
+        const float ms = time_one(cands[c], 0);
         if (h_ms) h_ms[c] = ms;
         if (ms < best) {
             best = ms;
             best_w = cands[c];
+        }
+        if (ms > prev) break;                 // past the minimum
+        prev = ms;
+    }
+    if (st == MPS_OK && B->n_big > 0) {
+        // the largest systems on clusters: as many as one wave of clusters,
+        // two, four, or all systems above kBigRows
+        int max_clusters = 0;
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = kClusterCTAs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.blockDim = dim3(kBatchNT);
+        cfg.gridDim = dim3(kClusterCTAs);
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        if (cudaOccupancyMaxActiveClusters(&max_clusters, batch_pcg_cluster, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            max_clusters = 0;
+        }
+        const int q = std::max(1, max_clusters / 2);
+        const int ks[4] = {q, 2 * q, 4 * q, B->n_big};
+        int last = 0;
+        for (int i = 0; i < 4 && st == MPS_OK && max_clusters > 0; ++i) {
+            const int k = std::min(ks[i], B->n_big);
+            if (k <= last) continue;
+            last = k;
+            const float ms = time_one(best_w, k);
+            if (ms < best) {
+                best = ms;
+                cl = k;
+            }
         }
     }
     cudaEventDestroy(e0);
@@ -479,7 +698,18 @@ mps_status mps_batch_autotune(mps_batch* B, const float* d_b, double tol, int32_
     cudaFree(it);
     if (st != MPS_OK) return st;
     B->wps = best_w;
+    B->clusters = cl;
     if (h_chosen_wps) *h_chosen_wps = best_w;
+    return MPS_OK;
+}
+
+int32_t mps_batch_uses_clusters(const mps_batch* B) {
+    return B ? std::min(std::max(B->clusters, 0), B->n_big) : 0;
+}
+
+mps_status mps_batch_set_clusters(mps_batch* B, int32_t n_systems) {
+    if (!B) return fail(MPS_ERR_ARG, "null argument");
+    B->clusters = n_systems < 0 ? B->n_big : n_systems;
     return MPS_OK;
 }
 
@@ -493,7 +723,7 @@ mps_status mps_batch_cg(mps_batch* B, const float* d_b, float* d_x, double tol, 
     // The whole batch is one CUDA-graph launch (queue reset + persistent
     // kernel), captured once per set of buffers and reused.
     const void* key[5] = {d_b, d_x, d_iters, d_converged, d_relres};
-    bool same = B->exec && B->exec_wps == B->wps;
+    bool same = B->exec && B->exec_wps == B->wps && B->exec_clusters == B->clusters;
     for (int i = 0; i < 5 && same; ++i) same = key[i] == B->exec_key[i];
     same = same && B->exec_tol == tol && B->exec_max_iter == max_iter;
     if (!same) {
@@ -501,7 +731,7 @@ mps_status mps_batch_cg(mps_batch* B, const float* d_b, float* d_x, double tol, 
         B->exec = nullptr;
         if (!B->cap) MPS_CUDA(cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking));
         MPS_CUDA(cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal));
-        mps_status st = batch_launch(B, B->wps, false, d_b, d_x, tol, max_iter, 400, o, B->cap);
+        mps_status st = batch_launch(B, B->wps, d_b, d_x, tol, max_iter, 400, o, B->cap, B->clusters);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(B->cap, &g);
         if (st != MPS_OK) {
@@ -514,6 +744,7 @@ mps_status mps_batch_cg(mps_batch* B, const float* d_b, float* d_x, double tol, 
         if (e != cudaSuccess) return cuda_fail(e, "batch graph instantiate");
         for (int i = 0; i < 5; ++i) B->exec_key[i] = key[i];
         B->exec_wps = B->wps;
+        B->exec_clusters = B->clusters;
         B->exec_tol = tol;
         B->exec_max_iter = max_iter;
     }

@@ -516,10 +516,10 @@ public:
         c10::cuda::CUDAGuard g(device_);
         auto bd = on_device(b, torch::kFloat32, "b");
         int32_t w = 0;
-        float ms[5];
+        float ms[6];
         check(mps_batch_autotune(h_, bd.data_ptr<float>(), tol, (int32_t)max_iter, &w, ms, cur_stream()),
               "autotune");
-        return {w, std::vector<double>(ms, ms + 5)};
+        return {w, std::vector<double>(ms, ms + 6)};
     }
     std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> cg(torch::Tensor b, torch::Tensor x, double tol,
                                                                int64_t max_iter) {
@@ -538,6 +538,8 @@ public:
         return {it, cv, rr};
     }
     int64_t warps_per_system() const { return mps_batch_warps_per_system(h_); }
+    int64_t uses_clusters() const { return mps_batch_uses_clusters(h_); }
+    void set_clusters(int64_t n) { check(mps_batch_set_clusters(h_, (int32_t)n), "set_clusters"); }
     int64_t num_systems() const { return n_sys_; }
 
 private:
@@ -662,6 +664,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         .def("cg", &BatchSolver::cg, py::arg("b"), py::arg("x"), py::arg("tol") = 1e-6,
              py::arg("max_iter") = 20000)
         .def_property_readonly("warps_per_system", &BatchSolver::warps_per_system)
+        .def_property_readonly("uses_clusters", &BatchSolver::uses_clusters)
+        .def("set_clusters", &BatchSolver::set_clusters, py::arg("n_systems"))
         .def_property_readonly("num_systems", &BatchSolver::num_systems);
 
     py::class_<BcsrTensor>(m, "bcsr_tensor")
