@@ -35,8 +35,11 @@ __host__ __device__ constexpr size_t stream_buf_bytes(int cap, int rcap) {
     return (size_t)cap * 4 + (size_t)cap * (BF16 ? 2 : 4) + (size_t)rcap * 4;
 }
 
+// Two buffers leave room for 6 CTAs per SM (registers capped to match),
+// three for 4: more warps in flight versus a deeper copy pipeline, chosen
+// per matrix by the autotuner.
 template <bool BF16, class Epi, int NB, int NT = kNT>
-__global__ void __launch_bounds__(NT, 4)
+__global__ void __launch_bounds__(NT, NB == 2 ? 6 : 4)
 spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
     static_assert(NB >= 2 && NB <= 4, "2 to 4 stages");
     pdl_begin();

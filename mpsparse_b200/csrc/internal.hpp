@@ -92,8 +92,8 @@ struct SpmvPlan {
     int cap_s = 0;            // staged nonzeros per buffer of the TMA kernel
     int rcap = 0;             // staged row_ptr entries per buffer
     int grid_s = 0;           // persistent CTAs of the TMA kernel
-    int stages = 3;           // TMA pipeline depth (2 or 3)
-    int evict_first = 0;      // L2 evict-first hint on the col_ind/value copies
+    int stages = 2;           // TMA pipeline depth (2 or 3)
+    int evict_first = 1;      // L2 evict-first hint on the col_ind/value copies
     int max_tile_nnz = 0;     // largest tile (nonzeros) and row count of the plan
     int max_tile_rows = 0;
 };
