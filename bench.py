@@ -194,7 +194,8 @@ def run_ours(args, rank, world, dev):
         info = A.cg_mixed(b64[i], x, tol=TOL, inner_tol=args.inner_tol, max_inner=args.max_iter,
                           precond="fsai", host_loop=args.host_loop)
         return x, {"iters": info["inner_iters"], "outer": info["outer_iters"],
-                   "converged": info["converged"], "rel_resid": info["rel_resid"]}
+                   "converged": info["converged"], "rel_resid": info["rel_resid"],
+                   "form": A.fsai_apply()["form"]}
 
     if args.solver == "learned":
         from mpsparse_b200.fsai import LearnedFsai, DEFAULT_WEIGHTS
@@ -265,11 +266,19 @@ def run_ours(args, rank, world, dev):
         total_ms = float(t.item())
     iters = [i["iters"] for i in infos]
     if args.solver == "learned":
-        # per solve: attach (network forward, value map, G^T gather) + ||b||^2 +
-        # outer residuals (outer + 1) + accumulations (outer) + per inner sweep
-        # (init + 2 G-applies, 5 kernels per iteration, result copy)
-        launches = sum(3 + 1 + (i["outer"] + 1) + i["outer"] + i["outer"] * 4 + 5 * i["iters"]
-                       for i in infos)
+        # per solve: attach (network forward, value map, G^T gather, and
+        # G^T G values in product form) + ||b||^2 + init + per iteration 2
+        # kernels (product form: direction + A p, update + M r) or 3 (split:
+        # A p, update + G r, G^T w) + 2 per residual replacement + the FP64
+        # true residual at the end; the product form's graph runs 4
+        # iterations per loop body, so after each replacement (and at the
+        # stop) about 1.5 iterations' kernels return at once: 3 launches
+        def per_solve(i):
+            if i.get("form") == "product":
+                rounds = max(i["outer"], 1)
+                return 4 + 1 + 2 + 2 * i["iters"] + 2 * rounds + 3 * rounds + 1
+            return 3 + 1 + 3 + 3 * i["iters"] + 2 * i["outer"] + 1
+        launches = sum(per_solve(i) for i in infos)
     else:
         launches = sum(2 + 3 * i["iters"] for i in infos)   # init + 3 kernels/iteration + copy
 

@@ -210,6 +210,23 @@ mps_status mps_csr_cg_mixed(mps_csr* A, const double* d_b, double* d_x, const mp
 mps_status mps_csr_set_fsai(mps_csr* A, const int32_t* d_g_row_ptr, const int32_t* d_g_col_ind,
                             const float* d_g_vals, uint64_t g_nnz, cudaStream_t stream);
 
+/* How PCG applies the attached factor: SPLIT = two SpMVs (w = G r, z = G^T w),
+ * PRODUCT = one SpMV with M = G^T G (built on the GPU from G's pattern, then
+ * refreshed from G's values at every attach), AUTO (default) = PRODUCT while
+ * M holds at most ~3.75M nonzeros more than G and G^T together (one kernel
+ * launch per iteration outweighs the extra bytes), else SPLIT.  The setting
+ * applies now to an attached factor and to later ones.  No reference
+ * counterpart. */
+enum { MPS_FSAI_APPLY_AUTO = 0, MPS_FSAI_APPLY_SPLIT = 1, MPS_FSAI_APPLY_PRODUCT = 2 };
+mps_status mps_csr_set_fsai_apply(mps_csr* A, int32_t mode, cudaStream_t stream);
+/* The form in force (MPS_FSAI_APPLY_SPLIT / _PRODUCT, -1: no factor) and
+ * nnz(M) (0 unless PRODUCT). */
+mps_status mps_csr_fsai_apply(const mps_csr* A, int32_t* in_force, uint64_t* nnz_m);
+/* Inspection: M = G^T G in CSR (row_ptr n+1, col_ind / values nnz_m), device
+ * buffers; PRODUCT form only. */
+mps_status mps_csr_fsai_product_get(const mps_csr* A, int32_t* d_row_ptr, int32_t* d_col_ind,
+                                    float* d_vals, cudaStream_t stream);
+
 /* Learned FSAI network: per-nonzero MLP 16 -> 64 -> 64 -> 1 (GELU), BF16
  * weights, FP32 accumulation, run on the tensor cores (tcgen05).  It maps 16
  * local coefficient features of each nonzero (i, j) of tril(A) to the factor

@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(NT, 2)
 bcsr_tiles(BcsrDev A, const float* __restrict__ x, Epi epi) {
     extern __shared__ __align__(128) unsigned char bcsr_smem[];
     __shared__ unsigned long long bar[2];
-    __shared__ double red[NT / 32];
+    __shared__ double red[(Epi::NS > 0 ? Epi::NS : 1) * (NT / 32)];
     __shared__ int last_flag;
     __shared__ int timed_out;
     if (blockIdx.x == 0 && threadIdx.x == 0) epi.tick();
@@ -160,16 +160,14 @@ bcsr_tiles(BcsrDev A, const float* __restrict__ x, Epi epi) {
         mbar_wait_bounded(&bar[tb], par);
     }
     if constexpr (Epi::NS > 0) {
+        block_sum_n<NT, Epi::NS>(acc, red);
+        if (threadIdx.x == 0) {
 #pragma unroll
-        for (int i = 0; i < Epi::NS; ++i) {
-            const double v = block_sum<NT>(acc[i], red);
-            if (threadIdx.x == 0) epi.partials[i * kMaxPartials + blockIdx.x] = v;
+            for (int i = 0; i < Epi::NS; ++i) epi.partials[i * kMaxPartials + blockIdx.x] = acc[i];
         }
         if (arrive_last(epi.counter, &last_flag)) {
             double tot[Epi::NS];
-#pragma unroll
-            for (int i = 0; i < Epi::NS; ++i)
-                tot[i] = sum_partials<NT>(epi.partials + i * kMaxPartials, gridDim.x, red);
+            sum_partials_n<NT, Epi::NS>(epi.partials, kMaxPartials, gridDim.x, red, tot);
             if (threadIdx.x == 0) epi.finalize(tot);
         }
     }

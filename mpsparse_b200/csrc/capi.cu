@@ -52,7 +52,7 @@ int num_sms() {
     return sms;
 }
 
-static mps_status device_error(unsigned err, const char* what) {
+mps_status device_error(unsigned err, const char* what) {
     if (err & kErrRange) return fail(MPS_ERR_RANGE, std::string(what) + ": a key lies outside [0, num_rows) x [0, num_cols)");
     if (err & kErrTimeout) return fail(MPS_ERR_TIMEOUT, std::string(what) + ": a bounded device wait gave up");
     return MPS_OK;
@@ -192,6 +192,7 @@ mps_status mps_csr_create_from_csr(const int32_t* d_row_ptr, const int32_t* d_co
 mps_status mps_csr_destroy(mps_csr* h) {
     if (!h) return MPS_OK;
     csr_free(h->A);
+    fsai_product_free(h);
     csr_free(h->G);
     csr_free(h->Gt);
     if (h->vb) cudaFree(h->vb);
@@ -332,6 +333,8 @@ cudaError_t factor_plans_follow(mps_csr* h, cudaStream_t s) {
     if (h->G.rp && h->G.n_rows) e = spmv_plan_build(h->G, 0, s, h->A.plan.stages, h->A.plan.evict_first);
     if (e == cudaSuccess && h->Gt.rp && h->Gt.n_rows)
         e = spmv_plan_build(h->Gt, 0, s, h->A.plan.stages, h->A.plan.evict_first);
+    if (e == cudaSuccess && h->M.rp && h->M.n_rows)
+        e = spmv_plan_build(h->M, 0, s, h->A.plan.stages, h->A.plan.evict_first);
     return e;
 }
 
@@ -363,8 +366,9 @@ static mps_status csr_solve(SolverKind kind, mps_csr* h, const float* b, float* 
     mps_status st = prepare_precond(h, kind == kCG ? o : nullptr, s);
     if (st != MPS_OK) return st;
     CsrOp op{&h->A, nullptr};
-    CsrOp g{&h->G, nullptr}, gt{&h->Gt, nullptr};
-    PrecondOps<CsrOp> pc{h->has_fsai ? &g : nullptr, h->has_fsai ? &gt : nullptr};
+    CsrOp g{&h->G, nullptr}, gt{&h->Gt, nullptr}, mm{&h->M, nullptr};
+    PrecondOps<CsrOp> pc{h->has_fsai ? &g : nullptr, h->has_fsai ? &gt : nullptr,
+                         h->has_fsai && h->use_m ? &mm : nullptr};
     MPS_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), s));
     st = run_solve(kind, op, pc, h->H, b, x, o, info, s);
     unsigned err = 0;
@@ -393,6 +397,7 @@ mps_status mps_csr_set_fsai(mps_csr* h, const int32_t* d_g_row_ptr, const int32_
                             const float* d_g_vals, uint64_t g_nnz, cudaStream_t s) {
     if (!h || !d_g_row_ptr || !d_g_col_ind || !d_g_vals) return fail(MPS_ERR_ARG, "null argument");
     const uint32_t n = h->A.n_rows;
+    fsai_product_free(h);
     csr_free(h->G);
     csr_free(h->Gt);
     fsai_work_free(h->fw);   // a network factor (if any) is replaced
@@ -414,7 +419,7 @@ mps_status mps_csr_set_fsai(mps_csr* h, const int32_t* d_g_row_ptr, const int32_
     if (st != MPS_OK) return st;
     MPS_CUDA(factor_plans_follow(h, s));
     h->has_fsai = true;
-    return MPS_OK;
+    return fsai_factor_changed(h, s);
 }
 
 }  // extern "C"
@@ -500,13 +505,10 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
     const int g = H.vgrid();
     sumsq64<<<g, kNT, 0, s>>>(d_b, n, scal, H.ws.partials, H.ws.counters + 13);
     MPS_CUDA(cudaMemsetAsync(d_x, 0, (size_t)n * sizeof(double), s));
-    double hs[2] = {0, 0};
-    MPS_CUDA(cudaMemcpyAsync(hs, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
-    MPS_CUDA(cudaStreamSynchronize(s));
-    const double bnorm = std::sqrt(hs[0]);
     CsrOp inner{&h->A, bf16 ? h->vb : nullptr};
-    CsrOp gop{&h->G, nullptr}, gtop{&h->Gt, nullptr};
-    PrecondOps<CsrOp> pc{h->has_fsai ? &gop : nullptr, h->has_fsai ? &gtop : nullptr};
+    CsrOp gop{&h->G, nullptr}, gtop{&h->Gt, nullptr}, mop{&h->M, nullptr};
+    PrecondOps<CsrOp> pc{h->has_fsai ? &gop : nullptr, h->has_fsai ? &gtop : nullptr,
+                         h->has_fsai && h->use_m ? &mop : nullptr};
     const CsrDev view = h->A.view();
     const size_t smem = spmv_smem_bytes<double>(view);
     smem_optin_k(spmv_tiles<double, double, false, EpiResid64>, smem);
@@ -518,31 +520,35 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
         return fail(MPS_ERR_ARG, o.ir_mode == MPS_IR_REPLACE ? "reliable updates run on FP32 values"
                                                               : "unknown ir_mode");
     }
-    if (!bf16 && o.ir_mode != MPS_IR_RESTART && bnorm > 0 && std::isfinite(bnorm)) {
+    if (!bf16 && o.ir_mode != MPS_IR_RESTART) {
         // Reliable updates: one FP32 PCG, x in FP64, r replaced by the FP64
         // b - A x whenever it has dropped by inner_tol; then the FP64 true
-        // residual of the result for the report.
+        // residual of the result for the report.  Everything is enqueued at
+        // once and read back after a single synchronization (b = 0 and a
+        // non-finite b are settled on the device).
         mps_solve_opts ro = io;
         ro.tol = tol;
         const long cap = (long)max_inner * max_outer;
         ro.max_iter = cap > (1L << 30) ? (1 << 30) : (int)cap;
         mps_solve_info ii{};
         int rep = 0;
-        st = run_solve(kCG, inner, pc, H, nullptr, nullptr, &ro, &ii, s, 0, d_b, d_x, inner_tol, &rep);
+        st = run_solve(kCG, inner, pc, H, nullptr, nullptr, &ro, &ii, s, 0, d_b, d_x, inner_tol, &rep, true);
         if (st == MPS_OK) {
             spmv_tiles<double, double, false, EpiResid64><<<h->A.plan.grid, kNT, smem, s>>>(
                 view, d_x, EpiResid64{d_b, r32, scal + 1, H.ws.counters + 14, H.ws.partials});
             st = cudaGetLastError() == cudaSuccess ? MPS_OK : cuda_fail(cudaErrorLaunchFailure, "residual");
         }
         if (st == MPS_OK) {
-            MPS_CUDA(cudaMemcpyAsync(hs + 1, scal + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+            unsigned* h_err = reinterpret_cast<unsigned*>(H.h_aux + 2);
+            MPS_CUDA(cudaMemcpyAsync(H.h_aux, scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+            MPS_CUDA(cudaMemcpyAsync(h_err, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
             MPS_CUDA(cudaStreamSynchronize(s));
-            rel = std::sqrt(hs[1]) / bnorm;
+            st = solve_report(kCG, H, &ii, &rep);
+            const double bnorm = std::sqrt(H.h_aux[0]);
+            rel = bnorm > 0 ? std::sqrt(H.h_aux[1]) / bnorm : std::sqrt(H.h_aux[1]);
+            if (st == MPS_OK && (*h_err & kErrTimeout)) st = fail(MPS_ERR_TIMEOUT, "SpMV: a bulk-copy wait gave up");
         }
         cudaFreeAsync(scal, s);
-        unsigned err = 0;
-        MPS_CUDA(cudaMemcpy(&err, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
-        if (st == MPS_OK && (err & kErrTimeout)) st = fail(MPS_ERR_TIMEOUT, "SpMV: a bulk-copy wait gave up");
         if (info) {
             info->outer_iters = rep;
             info->inner_iters = ii.iters;
@@ -552,6 +558,11 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
         }
         return st;
     }
+    // restarted refinement: ||b|| first (the stop test runs on the host)
+    double hs[2] = {0, 0};
+    MPS_CUDA(cudaMemcpyAsync(hs, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+    MPS_CUDA(cudaStreamSynchronize(s));
+    const double bnorm = std::sqrt(hs[0]);
     for (;; ++outer) {
         // FP64 outer residual r = b - A x (FP32 copy feeds the inner solve)
         spmv_tiles<double, double, false, EpiResid64><<<h->A.plan.grid, kNT, smem, s>>>(

@@ -118,6 +118,61 @@ __device__ __forceinline__ double sum_partials(const double* part, int count, do
     return block_sum_all<NT>(s, sh);
 }
 
+// NS block sums in one pass (one pair of barriers for all of them); the
+// same order of additions per sum as block_sum, so the same bits.  sh holds
+// NS * NT / 32 values; thread 0 receives the totals.
+template <int NT, int NS>
+__device__ __forceinline__ void block_sum_n(double (&v)[NS], double* sh) {
+    constexpr int W = NT / 32;
+    const int w = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < NS; ++i) v[i] = warp_sum(v[i]);
+    if (lane_id() == 0) {
+#pragma unroll
+        for (int i = 0; i < NS; ++i) sh[i * W + w] = v[i];
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int i = 0; i < NS; ++i) {
+            const double r = threadIdx.x < W ? sh[i * W + threadIdx.x] : 0.0;
+            v[i] = warp_sum(r);
+        }
+    }
+    __syncthreads();
+}
+
+// NS sums of `count` FP64 partials each (sum i at part + i * stride), in the
+// fixed order of sum_partials, broadcast to every thread.
+template <int NT, int NS>
+__device__ __forceinline__ void sum_partials_n(const double* part, int stride, int count, double* sh,
+                                               double (&tot)[NS]) {
+    constexpr int W = NT / 32;
+    double s[NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i) s[i] = 0.0;
+    for (int k = threadIdx.x; k < count; k += NT) {
+#pragma unroll
+        for (int i = 0; i < NS; ++i) s[i] += __ldcg(part + i * stride + k);
+    }
+    const int w = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < NS; ++i) s[i] = warp_sum(s[i]);
+    if (lane_id() == 0) {
+#pragma unroll
+        for (int i = 0; i < NS; ++i) sh[i * W + w] = s[i];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+        double r = 0.0;
+#pragma unroll
+        for (int j = 0; j < W; ++j) r += sh[i * W + j];
+        tot[i] = r;
+    }
+    __syncthreads();
+}
+
 __device__ __forceinline__ float bf16_to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
 
 }  // namespace mps

@@ -37,35 +37,36 @@ __host__ __device__ constexpr size_t stream_buf_bytes(int cap, int rcap) {
 
 // Two buffers leave room for 6 CTAs per SM (registers capped to match),
 // three for 4: more warps in flight versus a deeper copy pipeline, chosen
-// per matrix by the autotuner.
+// per matrix by the autotuner.  An epilogue that forms the multiplied vector
+// on the fly (two loads per gathered element) keeps 5 CTAs per SM (48
+// registers), so that its gathers do not spill.
+template <class Epi, int NB>
+constexpr int stream_min_ctas() {
+    return NB == 2 ? (epi_has_gather<Epi>::value ? 5 : 6) : 4;
+}
+
+// Epilogues with `static constexpr bool kPre = true` run only inside solver
+// loops, where the matrix does not change: the kernel requests its first
+// tiles before waiting for the previous kernel of the stream (programmatic
+// dependent launch), so the copies overlap that kernel's tail.
+template <class E, class = void> struct epi_pre : std::false_type {};
+template <class E> struct epi_pre<E, std::enable_if_t<E::kPre>> : std::true_type {};
+
 template <bool BF16, class Epi, int NB, int NT = kNT>
-__global__ void __launch_bounds__(NT, NB == 2 ? 6 : 4)
+__global__ void __launch_bounds__(NT, stream_min_ctas<Epi, NB>())
 spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
     static_assert(NB >= 2 && NB <= 4, "2 to 4 stages");
-    pdl_begin();
+    constexpr bool PRE = epi_pre<Epi>::value;
+    if constexpr (!PRE) pdl_begin();
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ unsigned long long bar[NB];
     __shared__ int4 s_meta[NB];
-    __shared__ double red[NT / 32];
+    __shared__ double red[(Epi::NS > 0 ? Epi::NS : 1) * (NT / 32)];
     __shared__ float redf[NT / 32];
     __shared__ int last_flag;
     __shared__ int timed_out;
-    if (blockIdx.x == 0 && threadIdx.x == 0) epi.tick();
-    if (!epi.active()) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) epi.on_skip();
-        return;
-    }
     constexpr int GA = BF16 ? 8 : 4;   // elements per 16 bytes of the value array
     const size_t bb = stream_buf_bytes<BF16>(A.cap, A.rcap);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int i = 0; i < NB; ++i) mbar_init(&bar[i], 1);
-        timed_out = 0;
-        fence_mbar_init();
-    }
-    double acc[Epi::NS > 0 ? Epi::NS : 1];
-#pragma unroll
-    for (int i = 0; i < (Epi::NS > 0 ? Epi::NS : 1); ++i) acc[i] = 0.0;
 
     auto staged = [&](const int4 m) {
         const int a0 = m.z & ~(GA - 1), a1 = (m.w + GA - 1) & ~(GA - 1);
@@ -101,17 +102,46 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
     const int t0 = blockIdx.x, G = gridDim.x;
     int4 m_ahead = none;           // metadata of tile it + NB - 1 (issued next)
     int4 m_ahead2 = none;          // tile it + NB
-    if (threadIdx.x == 0) {
+    unsigned issued = 0;           // thread 0: buffers the prologue filled
+    auto prologue = [&]() {        // barriers and the first NB - 1 copies
+        if (threadIdx.x != 0) return;
+#pragma unroll
+        for (int i = 0; i < NB; ++i) mbar_init(&bar[i], 1);
+        timed_out = 0;
+        fence_mbar_init();
         if (hint) pol = policy_evict_first();
         for (int i = 0; i < NB - 1; ++i) {
             const int ti = t0 + i * G;
             const int4 mi = ti < A.ntiles ? A.meta[ti] : none;
-            if (ti < A.ntiles && staged(mi)) issue(mi, i);
+            if (ti < A.ntiles && staged(mi)) {
+                issue(mi, i);
+                issued |= 1u << i;
+            }
             s_meta[i] = mi;
         }
         m_ahead = t0 + (NB - 1) * G < A.ntiles ? A.meta[t0 + (NB - 1) * G] : none;
         m_ahead2 = t0 + NB * G < A.ntiles ? A.meta[t0 + NB * G] : none;
+    };
+    if constexpr (PRE) {
+        prologue();
+        pdl_begin();
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) epi.tick();
+    if (!epi.active()) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) epi.on_skip();
+        if constexpr (PRE) {
+            // the requested tiles land before the CTA (and its shared memory) goes
+            if (threadIdx.x == 0)
+                for (int i = 0; i < NB - 1; ++i)
+                    if (((issued >> i) & 1u) && !mbar_wait_bounded(&bar[i], 0u)) atomicOr(A.err, kErrTimeout);
+        }
+        return;
+    }
+    epi_begin(epi);
+    if constexpr (!PRE) prologue();
+    double acc[Epi::NS > 0 ? Epi::NS : 1];
+#pragma unroll
+    for (int i = 0; i < (Epi::NS > 0 ? Epi::NS : 1); ++i) acc[i] = 0.0;
     __syncthreads();
     // Issue the copy of tile it + NB - 1 into the buffer tile it - 1 used.
     auto issue_ahead = [&](int t, int it) {   // one thread
@@ -161,7 +191,7 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
                         v[u] = in ? reinterpret_cast<const float*>(base + (size_t)A.cap * 4)[i] : 0.f;
                 }
 #pragma unroll
-                for (int u = 0; u < U; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : 0.f;
+                for (int u = 0; u < U; ++u) xv[u] = c[u] >= 0 ? epi_x(epi, x, c[u]) : 0.f;
 #pragma unroll
                 for (int u = 0; u < U; ++u)
                     if (kb + u * NT < k1) prod[kb + u * NT - a0] = v[u] * xv[u];
@@ -203,7 +233,7 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
                         float s = 0.f;
                         for (int k = bgn; k < end; ++k) {
                             const float v = BF16 ? bf16_to_f(A.vb[k]) : ld_stream(A.v + k);
-                            s += v * __ldg(x + ld_stream(A.ci + k));
+                            s += v * epi_x(epi, x, ld_stream(A.ci + k));
                         }
                         epi.row(r, s, acc);
                     }
@@ -214,7 +244,7 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
                     float s = 0.f;
                     for (int k = bgn + threadIdx.x; k < end; k += NT) {
                         const float v = BF16 ? bf16_to_f(A.vb[k]) : ld_stream(A.v + k);
-                        s += v * __ldg(x + ld_stream(A.ci + k));
+                        s += v * epi_x(epi, x, ld_stream(A.ci + k));
                     }
                     s = block_sum<NT>(s, redf);
                     if (threadIdx.x == 0) epi.row(r, s, acc);
@@ -227,16 +257,14 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
         mbar_wait_bounded(&bar[(timed_out >> 1) & 3], (unsigned)(timed_out >> 3) & 1u);
     }
     if constexpr (Epi::NS > 0) {
+        block_sum_n<NT, Epi::NS>(acc, red);
+        if (threadIdx.x == 0) {
 #pragma unroll
-        for (int i = 0; i < Epi::NS; ++i) {
-            const double v = block_sum<NT>(acc[i], red);
-            if (threadIdx.x == 0) epi.partials[i * kMaxPartials + blockIdx.x] = v;
+            for (int i = 0; i < Epi::NS; ++i) epi.partials[i * kMaxPartials + blockIdx.x] = acc[i];
         }
         if (arrive_last(epi.counter, &last_flag)) {
             double tot[Epi::NS];
-#pragma unroll
-            for (int i = 0; i < Epi::NS; ++i)
-                tot[i] = sum_partials<NT>(epi.partials + i * kMaxPartials, gridDim.x, red);
+            sum_partials_n<NT, Epi::NS>(epi.partials, kMaxPartials, gridDim.x, red, tot);
             if (threadIdx.x == 0) epi.finalize(tot);
         }
     }

@@ -16,9 +16,9 @@ int default_tile_nnz(uint64_t nnz, uint32_t n_rows);
 // Programmatic dependent launch for the solver kernels (each calls
 // pdl_begin() first): the next kernel's launch overlaps the tail of the
 // current one.  On unless MPS_PDL=0; a graph capture that rejects it is
-// retried without it (pdl_suspend).
+// retried without it (pdl_suspend, which returns the previous setting).
 bool pdl_enabled();
-void pdl_suspend(bool off);
+bool pdl_suspend(bool off);
 
 template <typename... KArgs, typename... Args>
 inline cudaError_t launch_k(void (*k)(KArgs...), dim3 g, dim3 b, size_t smem, cudaStream_t s,
@@ -87,6 +87,11 @@ struct CsrOp {
 
 enum SolverKind { kCG = 0, kBiCG = 1, kRich = 2 };
 enum VecSlot { vB = 0, vX, vR, vP, vQ, vR0, vS, vT, vXAlt, vW, vTmp0, vTmp1 };
+// FSAI-PCG keeps its residual in a pair of buffers (vR, vR1) and, with
+// M = G^T G, its direction too (vP, vP1); vS and vT are BiCGSTAB's and free
+// during a CG solve.  vW holds w = G r (split form) or z = M r (product form).
+constexpr int vR1 = vS;
+constexpr int vP1 = vT;
 
 // State a handle keeps for its solvers.
 struct SolverHost {
@@ -95,7 +100,9 @@ struct SolverHost {
     GraphCache graphs_ir[4];           // reliable-update CG per preconditioner
     double* v64 = nullptr;             // reliable updates: x (FP64) | b (FP64), n_pad each
     cudaStream_t cap = nullptr;
+    cudaStream_t cap_branch = nullptr; // captures the body of an IF node
     SolveParams* h_params = nullptr;   // pinned
+    double* h_aux = nullptr;           // pinned, 4 doubles: read-backs after a deferred solve
     float* dinv = nullptr;             // padded
     int n = 0;
 
@@ -108,8 +115,8 @@ struct SolverHost {
         if (g > cap_g) g = cap_g;
         return g < 1 ? 1 : g;
     }
-    Ctx ctx(cudaGraphConditionalHandle h, int use) const {
-        return Ctx{ws.sc, ws.partials, ws.counters, h, use};
+    Ctx ctx(cudaGraphConditionalHandle h, int use, cudaGraphConditionalHandle hif = {}) const {
+        return Ctx{ws.sc, ws.partials, ws.counters, h, use, hif};
     }
 
     cudaError_t ensure(size_t n_rows) {
@@ -131,7 +138,10 @@ struct SolverHost {
         if ((e = cudaMalloc(&ws.d_params, sizeof(SolveParams))) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&ws.h_sc, sizeof(DevScalars))) != cudaSuccess) return e;
         if ((e = cudaMallocHost(&h_params, sizeof(SolveParams))) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&h_aux, 4 * sizeof(double))) != cudaSuccess) return e;
         if (!cap && (e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        if (!cap_branch && (e = cudaStreamCreateWithFlags(&cap_branch, cudaStreamNonBlocking)) != cudaSuccess)
+            return e;
         ws.n_pad = n_pad ? n_pad : 4;
         return cudaSuccess;
     }
@@ -162,25 +172,31 @@ struct SolverHost {
         if (ws.d_params) cudaFree(ws.d_params);
         if (ws.h_sc) cudaFreeHost(ws.h_sc);
         if (h_params) cudaFreeHost(h_params);
+        if (h_aux) cudaFreeHost(h_aux);
         if (dinv) cudaFree(dinv);
         if (v64) cudaFree(v64);
         v64 = nullptr;
         ws = Workspace{};
         h_params = nullptr;
+        h_aux = nullptr;
         dinv = nullptr;
     }
     void destroy() {
         release();
         if (cap) cudaStreamDestroy(cap);
+        if (cap_branch) cudaStreamDestroy(cap_branch);
         cap = nullptr;
+        cap_branch = nullptr;
     }
 };
 
-// Preconditioner operators for PCG (FSAI: G and G^T as CSR).
+// Preconditioner operators for PCG (FSAI: G and G^T as CSR, and M = G^T G
+// when the product form is in force).
 template <class Op>
 struct PrecondOps {
     const CsrOp* G = nullptr;
     const CsrOp* Gt = nullptr;
+    const CsrOp* M = nullptr;
 };
 
 template <class Op>
@@ -194,6 +210,8 @@ cudaError_t launch_init(SolverKind kind, int precond, const Op& op, const Precon
                 launch_k(cg_init_ir, dim3(g), dim3(kNT), 0, s, static_cast<const double*>(H.b64()), H.x64(),
                          H.v(vR), H.v(vP), static_cast<const float*>(H.dinv), H.n,
                          static_cast<const SolveParams*>(H.ws.d_params), c);
+                if (precond == MPS_PRECOND_FSAI && pc.M)
+                    return pc.M->apply(H.v(vR), EpiMz{H.v(vW), sc, c.ctr + 3, c.part, H.v(vR)}, s);
                 if (precond == MPS_PRECOND_FSAI) {
                     cudaError_t e = pc.G->apply(H.v(vR), EpiFsai1{H.v(vW), sc, c.ctr + 3, c.part}, s);
                     if (e != cudaSuccess) return e;
@@ -205,6 +223,8 @@ cudaError_t launch_init(SolverKind kind, int precond, const Op& op, const Precon
             launch_k(cg_init, dim3(g), dim3(kNT), 0, s, H.v4(vB), H.v4(vX), H.v4(vR), H.v4(vP),
                                       reinterpret_cast<const float4*>(H.dinv), n4, H.n,
                                       H.ws.d_params, c);
+            if (precond == MPS_PRECOND_FSAI && pc.M)
+                return pc.M->apply(H.v(vR), EpiMz{H.v(vW), sc, c.ctr + 3, c.part, H.v(vR)}, s);
             if (precond == MPS_PRECOND_FSAI) {
                 cudaError_t e = pc.G->apply(H.v(vR), EpiFsai1{H.v(vW), sc, c.ctr + 3, c.part}, s);
                 if (e != cudaSuccess) return e;
@@ -223,18 +243,141 @@ cudaError_t launch_init(SolverKind kind, int precond, const Op& op, const Precon
     return cudaGetLastError();
 }
 
+// Replacement branch of reliable-update FSAI-PCG: r = (float)(b - A x) in
+// FP64 (EpiReplace) and its G-apply (EpiFsai1R).  Both return at once unless
+// a replacement is due, so the host loop may launch them every iteration;
+// a graph runs them under an IF node.
+inline cudaError_t launch_replace_fsai(const CsrOp& op, const PrecondOps<CsrOp>& pc, SolverHost& H,
+                                       const Ctx& c, cudaStream_t s) {
+    const CsrDev view = op.A->view();
+    const size_t smem = spmv_smem_bytes<double>(view);
+    smem_optin_k(spmv_tiles<double, double, false, EpiReplace>, smem);
+    spmv_tiles<double, double, false, EpiReplace><<<op.A->plan.grid, kNT, smem, s>>>(
+        view, H.x64(), EpiReplace{H.b64(), H.v(vR), H.dinv, H.ws.sc, c.ctr + 4, c.part, H.v(vR1)});
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return pc.G->apply(nullptr, EpiFsai1R{{H.v(vW), H.ws.sc, c.ctr + 3, c.part}, H.v(vR), H.v(vR1)}, s);
+}
+
+// FSAI-PCG with M = G^T G: one iteration (K1: direction + A p; K2: update +
+// z = M r'), c.h being the loop the iteration runs in.
+inline cudaError_t launch_prod_iter(const CsrOp& op, const PrecondOps<CsrOp>& pc, SolverHost& H, const Ctx& c,
+                                    cudaStream_t s, bool ir) {
+    DevScalars* sc = H.ws.sc;
+    cudaError_t e = op.apply(nullptr, EpiCgPqZ{H.v(vQ), H.v(vW), H.v(vP), H.v(vP1), H.v(vR), H.v(vR1), H.dinv,
+                                               sc, c.ctr + 1, c.part}, s);
+    if (e != cudaSuccess) return e;
+    const float* ra = H.v(vR);
+    const float* rb = H.v(vR1);
+    const float* pa = H.v(vP);
+    const float* pb = H.v(vP1);
+    if (ir)
+        return pc.M->apply(nullptr, EpiFsaiM<true>{ra, rb, H.v(vQ), pa, pb, H.x64(), H.dinv, H.v(vW), sc,
+                                                    c.ctr + 2, c.part, c}, s);
+    return pc.M->apply(nullptr, EpiFsaiM<false>{ra, rb, H.v(vQ), pa, pb, H.v(vX), H.dinv, H.v(vW), sc,
+                                                 c.ctr + 2, c.part, c}, s);
+}
+
+// Its replacement step: r = (float)(b - A x) in FP64, then z = M r.  Both
+// return at once unless a replacement is due.  c_out.h: the loop around the
+// iterations and this step; c_in.h: the iterations' loop (re-armed).
+inline cudaError_t launch_prod_replace(const CsrOp& op, const PrecondOps<CsrOp>& pc, SolverHost& H,
+                                       const Ctx& c_out, const Ctx& c_in, cudaStream_t s) {
+    const CsrDev view = op.A->view();
+    const size_t smem = spmv_smem_bytes<double>(view);
+    smem_optin_k(spmv_tiles<double, double, false, EpiReplace>, smem);
+    spmv_tiles<double, double, false, EpiReplace><<<op.A->plan.grid, kNT, smem, s>>>(
+        view, H.x64(),
+        EpiReplace{H.b64(), H.v(vR), H.dinv, H.ws.sc, c_out.ctr + 4, c_out.part, H.v(vR1), c_out, 1});
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return pc.M->apply(nullptr, EpiMzR{H.v(vW), H.ws.sc, c_in.ctr + 3, c_in.part, H.v(vR), H.v(vR1), c_in, 1}, s);
+}
+
+// During a capture on cs: append an IF node on `hif` after the captured work
+// and capture fn(bs) into its body on the stream bs.
+template <class F>
+cudaError_t capture_if(cudaStream_t cs, cudaStream_t bs, cudaGraphConditionalHandle hif, F&& fn) {
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd);
+    if (e != cudaSuccess) return e;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hif;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    if ((e = cudaGraphAddNode(&node, g, deps, nd, &cp)) != cudaSuccess) return e;
+    if ((e = cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies)) !=
+        cudaSuccess)
+        return e;
+    if ((e = cudaStreamBeginCaptureToGraph(bs, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+        return e;
+    e = fn(bs);
+    cudaGraph_t b2 = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(bs, &b2);
+    return e != cudaSuccess ? e : e2;
+}
+
+// One iteration.  branch_cap: set while capturing a graph whose reliable-update
+// FSAI body holds the replacement branch under an IF node (c.hif).
 template <class Op>
 cudaError_t launch_body(SolverKind kind, int precond, const Op& op, const PrecondOps<Op>& pc,
-                        SolverHost& H, const Ctx& c, cudaStream_t s, bool ir = false) {
+                        SolverHost& H, const Ctx& c, cudaStream_t s, bool ir = false,
+                        cudaStream_t branch_cap = nullptr) {
     const int n4 = H.n4(), g = H.vgrid();
     DevScalars* sc = H.ws.sc;
     cudaError_t e = cudaSuccess;
     const float4* dinv4 = reinterpret_cast<const float4*>(H.dinv);
     switch (kind) {
         case kCG:
+            if constexpr (std::is_same<Op, CsrOp>::value) {
+                if (precond == MPS_PRECOND_FSAI && pc.M) {
+                    // product form (a reliable-update graph nests its loops:
+                    // build_graph_nested; here the host loop or FP32 PCG)
+                    e = launch_prod_iter(op, pc, H, c, s, ir);
+                    if (e != cudaSuccess || !ir) return e;
+                    return launch_prod_replace(op, pc, H, c, c, s);
+                }
+            }
             e = op.apply(H.v(vP), EpiCgPq{H.v(vQ), H.v(vP), sc, c.ctr + 1, c.part}, s);
             if (e != cudaSuccess) return e;
             if constexpr (std::is_same<Op, CsrOp>::value) {
+                if (precond == MPS_PRECOND_FSAI) {
+                    // x/r update fused into the G-apply (EpiFsaiR), then
+                    // [replacement branch], then p = G^T w + beta p
+                    const float* ra = H.v(vR);
+                    const float* rb = H.v(vR1);
+                    if (ir)
+                        e = pc.G->apply(nullptr, EpiFsaiR<true>{ra, rb, H.v(vQ), H.v(vP), H.x64(), H.dinv,
+                                                                 H.v(vW), sc, c.ctr + 2, c.part, c}, s);
+                    else
+                        e = pc.G->apply(nullptr, EpiFsaiR<false>{ra, rb, H.v(vQ), H.v(vP), H.v(vX), H.dinv,
+                                                                  H.v(vW), sc, c.ctr + 2, c.part, c}, s);
+                    if (e != cudaSuccess) return e;
+                    bool pdl_prev = false;
+                    if (ir) {
+                        if (branch_cap) {
+                            e = capture_if(s, branch_cap, c.hif, [&](cudaStream_t bs) {
+                                return launch_replace_fsai(op, pc, H, c, bs);
+                            });
+                            if (e != cudaSuccess) return e;
+                            // the next kernel follows the IF node: plain stream order
+                            pdl_prev = pdl_suspend(true);
+                        } else {
+                            e = launch_replace_fsai(op, pc, H, c, s);
+                            if (e != cudaSuccess) return e;
+                        }
+                    }
+                    e = pc.Gt->apply(H.v(vW), EpiFsai2{H.v(vP), sc, nullptr, nullptr, H.v(vR), H.dinv, c, 1,
+                                                       H.v(vR1)}, s);
+                    if (ir && branch_cap) pdl_suspend(pdl_prev);
+                    return e;
+                }
                 if (ir) {
                     const float* dv = precond ? H.dinv : nullptr;
                     launch_k(cg_update_xr_ir, dim3(g), dim3(kNT), 0, s, H.x64(), H.v(vR),
@@ -300,9 +443,13 @@ cudaError_t build_graph(SolverKind kind, int precond, const Op& op, const Precon
     const cudaGraphNode_t* deps = nullptr;
     size_t nd = 0;
     cudaGraphConditionalHandle h{};
+    cudaGraphConditionalHandle hif{};
     cudaGraphNode_t cn;
     cudaGraphNodeParams cp = {};
     cudaGraph_t body = nullptr;
+    // reliable-update FSAI-PCG: the replacement branch sits under an IF node
+    const bool branch = ir && kind == kCG && precond == MPS_PRECOND_FSAI && !pc.M &&
+                        std::is_same<Op, CsrOp>::value;
     if ((e = cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd)) != cudaSuccess) goto abort;
     if ((e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault)) != cudaSuccess)
         goto abort;
@@ -318,12 +465,17 @@ cudaError_t build_graph(SolverKind kind, int precond, const Op& op, const Precon
         cudaSuccess)
         goto abort;
     if ((e = cudaStreamEndCapture(cs, &g)) != cudaSuccess) return e;
+    if (branch &&
+        (e = cudaGraphConditionalHandleCreate(&hif, body, 0, cudaGraphCondAssignDefault)) != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return e;
+    }
     if ((e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
                                            cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
         cudaGraphDestroy(g);
         return e;
     }
-    e = launch_body(kind, precond, op, pc, H, H.ctx(h, 1), cs, ir);
+    e = launch_body(kind, precond, op, pc, H, H.ctx(h, 1, hif), cs, ir, branch ? H.cap_branch : nullptr);
     {
         cudaGraph_t b2 = nullptr;
         cudaError_t e2 = cudaStreamEndCapture(cs, &b2);
@@ -350,15 +502,129 @@ abort:
     return e;
 }
 
+// Reliable-update FSAI-PCG with M = G^T G:
+//   [init] -> WHILE(h_out) { WHILE(h_in) { kUnroll iterations } -> replacement step }
+// The inner body holds several iterations so that their kernels chain by
+// programmatic dependent launch; once the solve stops or a replacement is
+// due, the rest of the body returns at once.
+constexpr int kUnroll = 4;
+
+inline cudaError_t build_graph_nested(const CsrOp& op, const PrecondOps<CsrOp>& pc, SolverHost& H,
+                                      GraphCache& gc) {
+    cudaStream_t cs = H.cap;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr, body_out = nullptr, body_in = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaGraphConditionalHandle h_out{}, h_in{};
+    cudaGraphNode_t n_out, n_in;
+    cudaGraphNodeParams cp = {};
+    auto end_capture = [&](cudaError_t err) {   // a failed capture of the top graph
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(cs, &junk);
+        if (junk) cudaGraphDestroy(junk);
+        return err;
+    };
+    if ((e = cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd)) != cudaSuccess) return end_capture(e);
+    if ((e = cudaGraphConditionalHandleCreate(&h_out, g, 0, cudaGraphCondAssignDefault)) != cudaSuccess)
+        return end_capture(e);
+    if ((e = launch_init(kCG, MPS_PRECOND_FSAI, op, pc, H, H.ctx(h_out, 1), cs, true)) != cudaSuccess)
+        return end_capture(e);
+    if ((e = cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd)) != cudaSuccess) return end_capture(e);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h_out;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    if ((e = cudaGraphAddNode(&n_out, g, deps, nd, &cp)) != cudaSuccess) return end_capture(e);
+    body_out = cp.conditional.phGraph_out[0];
+    if ((e = cudaStreamUpdateCaptureDependencies(cs, &n_out, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+        return end_capture(e);
+    if ((e = cudaStreamEndCapture(cs, &g)) != cudaSuccess) return e;
+    // outer body: WHILE(h_in) -> replacement step
+    if ((e = cudaGraphConditionalHandleCreate(&h_in, body_out, 1, cudaGraphCondAssignDefault)) != cudaSuccess ||
+        (e = cudaStreamBeginCaptureToGraph(cs, body_out, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+            cudaSuccess) {
+        cudaGraphDestroy(g);
+        return e;
+    }
+    cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h_in;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    if ((e = cudaGraphAddNode(&n_in, body_out, nullptr, 0, &cp)) == cudaSuccess) {
+        body_in = cp.conditional.phGraph_out[0];
+        e = cudaStreamUpdateCaptureDependencies(cs, &n_in, 1, cudaStreamSetCaptureDependencies);
+    }
+    if (e == cudaSuccess) {
+        const bool prev = pdl_suspend(true);   // first kernel after a conditional node
+        e = launch_prod_replace(op, pc, H, H.ctx(h_out, 1), H.ctx(h_in, 1), cs);
+        pdl_suspend(prev);
+    }
+    {
+        cudaGraph_t b2 = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(cs, &b2);
+        if (e == cudaSuccess) e = e2;
+    }
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return e;
+    }
+    // inner body: kUnroll iterations
+    if ((e = cudaStreamBeginCaptureToGraph(cs, body_in, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+        cudaSuccess) {
+        cudaGraphDestroy(g);
+        return e;
+    }
+    for (int u = 0; u < kUnroll && e == cudaSuccess; ++u) e = launch_prod_iter(op, pc, H, H.ctx(h_in, 1), cs, true);
+    {
+        cudaGraph_t b2 = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(cs, &b2);
+        if (e == cudaSuccess) e = e2;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&gc.exec, g, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        gc = GraphCache{};
+        return e;
+    }
+    gc.graph = g;
+    return cudaSuccess;
+}
+
 // Run one solve: b (device, n floats) -> x (device, n floats).
 // Reliable-update mode (CG on a CSR only): d_b64 -> d_x64 in FP64, d_b/d_x
 // unused; *replaced receives the number of residual replacements.
+// The outcome of a solve from the scalars read back into H.ws.h_sc.
+inline mps_status solve_report(SolverKind kind, const SolverHost& H, mps_solve_info* info, int* replaced) {
+    const DevScalars& r = *H.ws.h_sc;
+    if (info) {
+        info->iters = r.iter;
+        info->converged = r.converged;
+        info->breakdown = r.breakdown;
+        info->stalled = r.stalled;
+        info->compat_snapshot = r.snapshot;
+        info->reserved = 0;
+        const double num = kind == kCG ? r.rr : r.rnorm2;
+        info->rel_resid = r.bnorm2 > 0 ? sqrt(num / r.bnorm2) : sqrt(num);
+    }
+    if (replaced) *replaced = r.replaced;
+    if (r.err & kErrNotFinite) return fail(MPS_ERR_NOT_FINITE, "right-hand side holds NaN or Inf");
+    if (r.err & kErrTimeout) return fail(MPS_ERR_TIMEOUT, "solver loop stopped by its watchdog");
+    return MPS_OK;
+}
+
+// defer: enqueue everything (the scalars' read-back into H.ws.h_sc included)
+// and return without synchronizing; the caller synchronizes the stream and
+// calls solve_report.
 template <class Op>
 mps_status run_solve(SolverKind kind, const Op& op, const PrecondOps<Op>& pc, SolverHost& H,
                      const float* d_b, float* d_x, const mps_solve_opts* o_in,
                      mps_solve_info* info, cudaStream_t s, int variant = 0,
                      const double* d_b64 = nullptr, double* d_x64 = nullptr, double delta = 0.0,
-                     int* replaced = nullptr) {
+                     int* replaced = nullptr, bool defer = false) {
     mps_solve_opts o;
     mps_solve_opts_default(&o);
     if (o_in) o = *o_in;
@@ -386,11 +652,18 @@ mps_status run_solve(SolverKind kind, const Op& op, const PrecondOps<Op>& pc, So
         if (!gc.exec) {
             // captured once per (solver, preconditioner) on the handle's
             // private stream; the graph only references handle-owned buffers
-            cudaError_t e = build_graph(kind, precond, op, pc, H, gc, ir);
+            auto build = [&]() -> cudaError_t {
+                if constexpr (std::is_same<Op, CsrOp>::value) {
+                    if (ir && kind == kCG && precond == MPS_PRECOND_FSAI && pc.M)
+                        return build_graph_nested(op, pc, H, gc);
+                }
+                return build_graph(kind, precond, op, pc, H, gc, ir);
+            };
+            cudaError_t e = build();
             if (e != cudaSuccess && pdl_enabled()) {   // retry with plain stream order
                 cudaGetLastError();
                 pdl_suspend(true);
-                e = build_graph(kind, precond, op, pc, H, gc, ir);
+                e = build();
                 pdl_suspend(false);
             }
             if (e != cudaSuccess) return cuda_fail(e, "solver graph capture");
@@ -418,22 +691,9 @@ mps_status run_solve(SolverKind kind, const Op& op, const PrecondOps<Op>& pc, So
         MPS_CUDA(cudaGetLastError());
     }
     MPS_CUDA(cudaMemcpyAsync(H.ws.h_sc, H.ws.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
+    if (defer) return MPS_OK;
     MPS_CUDA(cudaStreamSynchronize(s));
-    const DevScalars& r = *H.ws.h_sc;
-    if (info) {
-        info->iters = r.iter;
-        info->converged = r.converged;
-        info->breakdown = r.breakdown;
-        info->stalled = r.stalled;
-        info->compat_snapshot = r.snapshot;
-        info->reserved = 0;
-        const double num = kind == kCG ? r.rr : r.rnorm2;
-        info->rel_resid = r.bnorm2 > 0 ? sqrt(num / r.bnorm2) : sqrt(num);
-    }
-    if (replaced) *replaced = r.replaced;
-    if (r.err & kErrNotFinite) return fail(MPS_ERR_NOT_FINITE, "right-hand side holds NaN or Inf");
-    if (r.err & kErrTimeout) return fail(MPS_ERR_TIMEOUT, "solver loop stopped by its watchdog");
-    return MPS_OK;
+    return solve_report(kind, H, info, replaced);
 }
 
 }  // namespace mps

@@ -285,6 +285,7 @@ static mps_status fsai_prepare(mps_csr* h, cudaStream_t s) {
     MPS_CUDA(stream_alloc(&cnt, ((size_t)n + 1) * 4, s));
     MPS_CUDA(stream_alloc(&bsum, (((size_t)n + 2048) / 2048 + 1) * 4, s));
     g_count_kernel<<<g1(n), 256, 0, s>>>(A.rp, A.ci, n, cnt);
+    fsai_product_free(h);
     csr_free(h->G);
     csr_free(h->Gt);
     h->has_fsai = false;
@@ -483,7 +484,7 @@ mps_status mps_fsai_attach(mps_csr* h, const mps_fsai_model* m, cudaStream_t s) 
     st = model_error(m, s);
     if (st != MPS_OK) return st;
     h->has_fsai = true;
-    return MPS_OK;
+    return fsai_factor_changed(h, s);
 }
 
 mps_status mps_fsai_features(mps_csr* h, float* d_X, int32_t* d_g_row_ptr, int32_t* d_g_col_ind,
@@ -605,7 +606,9 @@ mps_status mps_fsai_train_step(mps_fsai_model* m, mps_csr* h, int32_t n_probes, 
     pack_kernel<<<16, 256, 0, s>>>(m->params, m->packed);
     MPS_CUDA(cudaGetLastError());
     h->has_fsai = true;   // G now holds the pre-step network's factor
-    return model_error(m, s);
+    st = model_error(m, s);
+    if (st != MPS_OK) return st;
+    return fsai_factor_changed(h, s);
 }
 
 }  // extern "C"

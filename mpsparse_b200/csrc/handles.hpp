@@ -21,6 +21,17 @@ struct FsaiWork {
     float* vec = nullptr;          // probe work vectors (6 x n)
 };
 
+// M = G^T G for the one-SpMV FSAI apply: its pattern and, per nonzero of M,
+// the range of pairs (g_ki, g_kj) whose products sum to it.
+struct FsaiProduct {
+    bool ready = false;        // built for the current pattern of G
+    bool declined = false;     // the cost model chose G and G^T for this pattern
+    uint64_t n_pairs = 0;
+    int32_t* seg = nullptr;    // nnz(M) + 1 offsets into pa / pb
+    int32_t* pa = nullptr;     // index of g_ki in G's values, pairs sorted by (i, j, k)
+    int32_t* pb = nullptr;     // index of g_kj
+};
+
 }  // namespace mps
 
 struct mps_csr {
@@ -31,6 +42,10 @@ struct mps_csr {
     mps::SolverHost H;
     unsigned* d_err = nullptr;
     mps::FsaiWork fw;
+    mps::CsrMat M;             // G^T G (when use_m)
+    mps::FsaiProduct fp;
+    int32_t fsai_apply = 0;    // MPS_FSAI_APPLY_*
+    bool use_m = false;        // PCG applies z = M r (else z = G^T (G r))
 };
 
 namespace mps {
@@ -42,6 +57,12 @@ mps_status prepare_precond(mps_csr* h, const mps_solve_opts* o, cudaStream_t s);
 cudaError_t exclusive_scan_rows(const unsigned* counts, uint64_t n, int32_t* out, unsigned* bsum,
                                 cudaStream_t s);
 void fsai_work_free(FsaiWork& w);
-// Rebuild the SpMV plans of G and G^T with A's pipeline depth and L2 hint.
+// Rebuild the SpMV plans of G, G^T and M with A's pipeline depth and L2 hint.
 cudaError_t factor_plans_follow(mps_csr* h, cudaStream_t s);
+// G^T G: drop it (G's pattern changed) / bring the apply form in line with
+// h->fsai_apply and G's current values (pattern on first use, then values).
+void fsai_product_free(mps_csr* h);
+// Status of a device error word (range / timeout bits) after `what`.
+mps_status device_error(unsigned err, const char* what);
+mps_status fsai_factor_changed(mps_csr* h, cudaStream_t s);
 }  // namespace mps

@@ -57,6 +57,7 @@ struct DevScalars {
     double delta2;      // replace when ||r||^2 < delta2 * rr_ref (or at the target)
     int replace;        // a replacement is due in this iteration
     int replaced;       // replacements so far
+    int refresh;        // FSAI: the replaced residual still needs its G-apply
 };
 
 // Parameters copied host->device before each solve.

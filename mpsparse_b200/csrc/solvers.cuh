@@ -22,8 +22,9 @@ struct Ctx {
     DevScalars* sc;
     double* part;          // 4 * kMaxPartials doubles
     unsigned* ctr;         // 16 counters
-    cudaGraphConditionalHandle h;
+    cudaGraphConditionalHandle h;     // WHILE condition of the solve loop
     int use_cond;
+    cudaGraphConditionalHandle hif;   // IF condition of the replacement branch
 };
 
 __device__ __forceinline__ void set_cond(const Ctx& c, bool run) {
@@ -34,16 +35,21 @@ __device__ __forceinline__ void set_cond(const Ctx& c, bool run) {
 template <int NS>
 __device__ __forceinline__ bool reduce_partials(const Ctx& c, int slot, const double* acc,
                                                 double* tot) {
-    __shared__ double red[kNT / 32];
+    __shared__ double red[NS * (kNT / 32)];
     __shared__ int last_flag;
+    double v[NS];
 #pragma unroll
-    for (int i = 0; i < NS; ++i) {
-        const double v = block_sum<kNT>(acc[i], red);
-        if (threadIdx.x == 0) c.part[i * kMaxPartials + blockIdx.x] = v;
+    for (int i = 0; i < NS; ++i) v[i] = acc[i];
+    block_sum_n<kNT, NS>(v, red);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < NS; ++i) c.part[i * kMaxPartials + blockIdx.x] = v[i];
     }
     if (!arrive_last(c.ctr + slot, &last_flag)) return false;
+    double t[NS];
+    sum_partials_n<kNT, NS>(c.part, kMaxPartials, gridDim.x, red, t);
 #pragma unroll
-    for (int i = 0; i < NS; ++i) tot[i] = sum_partials<kNT>(c.part + i * kMaxPartials, gridDim.x, red);
+    for (int i = 0; i < NS; ++i) tot[i] = t[i];
     return true;
 }
 
@@ -138,6 +144,7 @@ static __device__ void cg_init_scalars(const Ctx& c, const SolveParams* __restri
     s->delta2 = prm->delta * prm->delta;
     s->replace = 0;
     s->replaced = 0;
+    s->refresh = 0;
     if (!isfinite(bb)) {
         s->err = kErrNotFinite;
         s->done = 1;
@@ -152,6 +159,7 @@ static __device__ void cg_init_scalars(const Ctx& c, const SolveParams* __restri
 
 // q = A p ; pq = p.q ; alpha = rz / pq
 struct EpiCgPq {
+    static constexpr bool kPre = true;   // solver loops only
     static constexpr int NS = 1;
     float* q;
     const float* p;
@@ -330,6 +338,9 @@ cg_update_xr_ir(double* __restrict__ x, float* __restrict__ r, const float* __re
 // Replacement (runs only when due): r = (float)(b - A x) with FP64 gathers of
 // x and FP64 sums; ||b - A x||^2 and r.D^-1 r; then the stop test and the
 // next direction.
+// With FSAI the residual is a pair of buffers (r, r1; the current one is
+// picked by iteration parity) and the replaced residual is flagged for its
+// G-apply (EpiFsai1R).
 struct EpiReplace {
     static constexpr int NS = 2;
     const double* b;
@@ -338,13 +349,20 @@ struct EpiReplace {
     DevScalars* sc;
     unsigned* counter;
     double* partials;
+    float* r1 = nullptr;
+    Ctx c = {};                    // loop: c.h is the condition of the loop
+    int loop = 0;                  //   around the iterations and this step
+    float* rw = nullptr;           // per thread: the buffer written
     __device__ bool active() const { return !sc->done && sc->replace; }
-    __device__ void tick() const {}
+    __device__ void tick() const {
+        if (loop) set_cond(c, !sc->done);
+    }
     __device__ void on_skip() const {}
+    __device__ void begin() { rw = (r1 && (sc->iter & 1)) ? r1 : r; }
     __device__ void row(int i, double s, double* acc) const {
         const double rt = b[i] - s;
         const float rf = (float)rt;
-        r[i] = rf;
+        rw[i] = rf;
         acc[0] += rt * rt;
         acc[1] += (double)rf * rf * (dinv ? dinv[i] : 1.f);
     }
@@ -365,7 +383,9 @@ struct EpiReplace {
             s->done = 1;
         } else {
             cg_direction(s, rr, tot[1]);
+            if (r1 && s->mode == 2) s->refresh = 1;
         }
+        if (loop) set_cond(c, !s->done);
     }
 };
 
@@ -390,8 +410,32 @@ cg_update_p(float4* __restrict__ p, const float4* __restrict__ r, const float4* 
     }
 }
 
+// beta = rz / rz_old of an FSAI direction, rz = r.G^T G r = ||G r||^2.
+// Stall watch on rz: when it has not dropped 4x within stall_window
+// iterations, fall back to Jacobi (restart the direction from z = D^-1 r).
+static __device__ void fsai_beta(DevScalars* sc, double rz) {
+    const int it = sc->iter;
+    if (!sc->restart && sc->stall_window > 0) {
+        if (rz < 0.25 * sc->best_rr) {
+            sc->best_rr = rz;
+            sc->best_iter = it;
+        } else if (it - sc->best_iter >= sc->stall_window) {
+            sc->mode = 1;
+            sc->stalled = 1;
+            sc->beta = 0.0;
+            sc->rz = sc->rz_jac;
+            sc->restart = 0;
+            return;
+        }
+    }
+    sc->beta = sc->restart ? 0.0 : rz / sc->rz;
+    sc->rz = rz;
+    sc->restart = 0;
+}
+
 // FSAI step 1: w = G r ; rz = w.w (= r.G^T G r) ; beta = rz / rz_old
 struct EpiFsai1 {
+    static constexpr bool kPre = true;   // solver loops only
     static constexpr int NS = 1;
     float* w;
     DevScalars* sc;
@@ -404,28 +448,85 @@ struct EpiFsai1 {
         w[r] = s;
         acc[0] += (double)s * (double)s;
     }
+    __device__ void finalize(const double* tot) const { fsai_beta(sc, tot[0]); }
+};
+
+// The G-apply of a replaced residual (reliable updates): w = G r with r the
+// current buffer of the pair; runs only after a replacement.
+struct EpiFsai1R : EpiFsai1 {
+    const float* r0 = nullptr;
+    const float* r1 = nullptr;
+    const float* rc = nullptr;     // per thread: the current buffer
+    __device__ bool active() const { return !sc->done && sc->mode == 2 && sc->refresh; }
+    __device__ void begin() { rc = (sc->iter & 1) ? r1 : r0; }
+    __device__ float gather(int c) const { return __ldg(rc + c); }
     __device__ void finalize(const double* tot) const {
-        const double rz = tot[0];
-        // Stall watch on the preconditioned residual r . G^T G r: when it has
-        // not dropped 4x within stall_window iterations, fall back to Jacobi
-        // (restart the direction from z = D^-1 r).
-        const int it = sc->iter;
-        if (!sc->restart && sc->stall_window > 0) {
-            if (rz < 0.25 * sc->best_rr) {
-                sc->best_rr = rz;
-                sc->best_iter = it;
-            } else if (it - sc->best_iter >= sc->stall_window) {
-                sc->mode = 1;
-                sc->stalled = 1;
-                sc->beta = 0.0;
-                sc->rz = sc->rz_jac;
-                sc->restart = 0;
-                return;
-            }
+        sc->refresh = 0;
+        fsai_beta(sc, tot[0]);
+    }
+};
+
+// Fused FSAI-PCG step (one kernel in place of the x/r update and the G-apply):
+//   r' = r - alpha q          (FP32, the same fmaf as the unfused update)
+//   x += alpha p              (FP64 under reliable updates, else FP32)
+//   w = G r'                  with r' gathered as r[c] - alpha q[c]
+//   sums r'.r', r'.D^-1 r', w.w
+// r' goes to the other buffer of the residual pair (the current one is
+// r[iter & 1]), so no CTA overwrites an element another CTA still gathers.
+// The last CTA advances the iteration and, under reliable updates, decides
+// whether a replacement is due (then the IF branch of the graph runs
+// EpiReplace and EpiFsai1R); otherwise it sets the next direction's beta.
+template <bool IR>
+struct EpiFsaiR {
+    static constexpr bool kPre = true;   // solver loops only
+    static constexpr int NS = 3;
+    const float* r0;
+    const float* r1;
+    const float* q;
+    const float* p;
+    std::conditional_t<IR, double, float>* x;
+    const float* dinv;             // null: no diagonal
+    float* w;
+    DevScalars* sc;
+    unsigned* counter;
+    double* partials;
+    Ctx c;
+    const float* rc = nullptr;     // per thread (begin): current residual
+    float* rn = nullptr;           //   the buffer r' goes to
+    double a = 0.0;
+    float af = 0.f;
+    __device__ bool active() const { return !sc->done; }
+    __device__ void tick() const {}
+    __device__ void on_skip() const {}
+    __device__ void begin() {
+        const bool odd = sc->iter & 1;
+        rc = odd ? r1 : r0;
+        rn = const_cast<float*>(odd ? r0 : r1);
+        a = sc->alpha;
+        af = (float)a;
+    }
+    __device__ float gather(int col) const { return fmaf(-af, __ldg(q + col), __ldg(rc + col)); }
+    __device__ void row(int i, float s, double* acc) const {
+        const float rv = fmaf(-af, q[i], rc[i]);
+        rn[i] = rv;
+        if constexpr (IR) x[i] = fma(a, (double)p[i], x[i]);
+        else x[i] = fmaf(af, p[i], x[i]);
+        w[i] = s;
+        acc[0] += (double)rv * rv;
+        if (dinv) acc[1] += (double)rv * rv * dinv[i];
+        acc[2] += (double)s * (double)s;
+    }
+    __device__ void finalize(const double* tot) const {
+        DevScalars* s = sc;
+        if constexpr (IR) {
+            cg_finalize_ir(s, tot[0], tot[1]);
+            if (c.use_cond) cudaGraphSetConditional(c.hif, s->replace ? 1u : 0u);
+            if (s->replace || s->done) return;
+        } else {
+            cg_finalize_xr(s, tot[0], tot[1]);
+            if (s->done) return;
         }
-        sc->beta = sc->restart ? 0.0 : rz / sc->rz;
-        sc->rz = rz;
-        sc->restart = 0;
+        if (s->mode == 2) fsai_beta(s, tot[2]);
     }
 };
 
@@ -436,16 +537,20 @@ struct EpiFsai1 {
 // stall fallback it updates p = D^-1 r + beta p instead (the G^T w row sum is
 // then unused).
 struct EpiFsai2 {
+    static constexpr bool kPre = true;   // solver loops only
     static constexpr int NS = 0;
     float* p;
     DevScalars* sc;
     unsigned* counter = nullptr;
     double* partials = nullptr;
-    const float* r = nullptr;      // body only
+    const float* r = nullptr;      // body only: the residual pair (r, r1)
     const float* dinv = nullptr;
     Ctx c = {};
     int body = 0;
+    const float* r1 = nullptr;
+    const float* rc = nullptr;     // per thread: the current residual
     __device__ bool active() const { return !sc->done && (body ? sc->mode >= 1 : sc->mode == 2); }
+    __device__ void begin() { rc = (r1 && (sc->iter & 1)) ? r1 : r; }
     __device__ void tick() const {
         if (body) {
             loop_watchdog(sc);
@@ -458,11 +563,194 @@ struct EpiFsai2 {
         if (!body || __ldcg(&sc->mode) == 2) {
             p[i] = fmaf(beta, p[i], s);
         } else {
-            const float z = r[i] * dinv[i];
+            const float z = rc[i] * dinv[i];
             p[i] = beta != 0.f ? fmaf(beta, p[i], z) : z;
         }
     }
     __device__ void finalize(const double*) const {}
+};
+
+// ---- FSAI-PCG with M = G^T G (one SpMV per preconditioner apply) ------------
+// Two kernels per iteration:
+//   K1  p_k = z + beta p_(k-1) formed on the fly (gathered, and written to
+//       p[k & 1] for the own rows), q = A p_k, p.q -> alpha      (EpiCgPqZ)
+//   K2  r' = r - alpha q, x += alpha p_k, z = M r' (r' gathered on the fly,
+//       written to the other buffer of the residual pair), r'.r', r'.D^-1 r',
+//       r'.z -> replacement decision or beta, loop condition      (EpiFsaiM)
+// After a Jacobi fallback (stall), K1 forms z = D^-1 r itself.  Under
+// reliable updates the graph nests two loops: the inner one runs iterations
+// (several per body) until a replacement is due or the solve stops; the
+// outer one then runs the replacement (EpiReplace) and z = M r (EpiMzR),
+// which set the outer condition and re-arm the inner one.
+
+// z = M r (init) ; rz = r.z ; beta (restarts the direction)
+struct EpiMz {
+    static constexpr bool kPre = true;   // solver loops only
+    static constexpr int NS = 1;
+    float* z;
+    DevScalars* sc;
+    unsigned* counter;
+    double* partials;
+    const float* r;                // residual M is applied to (own rows, for r.z)
+    __device__ bool active() const { return !sc->done && sc->mode == 2; }
+    __device__ void tick() const {}
+    __device__ void on_skip() const {}
+    __device__ void row(int i, float s, double* acc) const {
+        z[i] = s;
+        acc[0] += (double)r[i] * (double)s;
+    }
+    __device__ void finalize(const double* tot) const { fsai_beta(sc, tot[0]); }
+};
+
+// z = M r for a replaced residual (current buffer of the pair); after a
+// replacement only.
+struct EpiMzR {
+    static constexpr bool kPre = true;   // solver loops only
+    static constexpr int NS = 1;
+    float* z;
+    DevScalars* sc;
+    unsigned* counter;
+    double* partials;
+    const float* r0;
+    const float* r1;
+    Ctx c = {};                    // loop: c.h is the iterations' loop, re-armed
+    int loop = 0;                  //   for the next round
+    const float* rc = nullptr;     // per thread: current residual
+    __device__ bool active() const { return !sc->done && sc->mode == 2 && sc->refresh; }
+    __device__ void tick() const {
+        if (loop) set_cond(c, !sc->done);
+    }
+    __device__ void on_skip() const {}
+    __device__ void begin() { rc = (sc->iter & 1) ? r1 : r0; }
+    __device__ float gather(int c) const { return __ldg(rc + c); }
+    __device__ void row(int i, float s, double* acc) const {
+        z[i] = s;
+        acc[0] += (double)rc[i] * (double)s;
+    }
+    __device__ void finalize(const double* tot) const {
+        sc->refresh = 0;
+        fsai_beta(sc, tot[0]);
+    }
+};
+
+struct EpiCgPqZ {
+    static constexpr bool kPre = true;   // solver loops only
+    static constexpr int NS = 1;
+    float* q;
+    const float* z;
+    float* p0;                     // direction pair: p_k goes to p[k & 1]
+    float* p1;
+    const float* r0;               // residual pair and diagonal (Jacobi fallback)
+    const float* r1;
+    const float* dinv;
+    DevScalars* sc;
+    unsigned* counter;
+    double* partials;
+    const float* po = nullptr;     // per thread (begin)
+    float* pn = nullptr;
+    const float* rc = nullptr;
+    float beta = 0.f;
+    bool jac = false;
+    __device__ bool active() const { return !sc->done && !sc->replace; }
+    __device__ void tick() const {}
+    __device__ void on_skip() const {}
+    __device__ void begin() {
+        const bool odd = sc->iter & 1;
+        pn = odd ? p1 : p0;
+        po = odd ? p0 : p1;
+        rc = odd ? r1 : r0;
+        beta = (float)sc->beta;
+        jac = sc->mode == 1;
+    }
+    __device__ float gather(int c) const {
+        const float zc = jac ? __ldg(rc + c) * __ldg(dinv + c) : __ldg(z + c);
+        return beta != 0.f ? fmaf(beta, __ldg(po + c), zc) : zc;
+    }
+    __device__ void row(int i, float s, double* acc) const {
+        const float zc = jac ? rc[i] * dinv[i] : z[i];
+        const float pv = beta != 0.f ? fmaf(beta, po[i], zc) : zc;
+        pn[i] = pv;
+        q[i] = s;
+        acc[0] += (double)pv * (double)s;
+    }
+    __device__ void finalize(const double* tot) const {
+        const double pq = tot[0];
+        sc->pq = pq;
+        if (!(pq > 0.0) || !isfinite(pq)) {
+            sc->breakdown = 1;
+            sc->done = 1;
+            sc->alpha = 0.0;
+        } else {
+            sc->alpha = sc->rz / pq;
+        }
+    }
+};
+
+template <bool IR>
+struct EpiFsaiM {
+    static constexpr bool kPre = true;   // solver loops only
+    static constexpr int NS = 3;
+    const float* r0;
+    const float* r1;
+    const float* q;
+    const float* p0;
+    const float* p1;
+    std::conditional_t<IR, double, float>* x;
+    const float* dinv;
+    float* z;
+    DevScalars* sc;
+    unsigned* counter;
+    double* partials;
+    Ctx c;
+    const float* rc = nullptr;     // per thread (begin)
+    float* rn = nullptr;
+    const float* pc = nullptr;
+    double a = 0.0;
+    float af = 0.f;
+    __device__ bool active() const { return !sc->done && !sc->replace; }
+    // last kernel of an iteration: watchdog (iterations that run), and the
+    // loop condition in case this launch returns at once (the last CTA sets
+    // it again below)
+    __device__ void tick() const {
+        const bool run = !sc->done && !sc->replace;
+        if (run) loop_watchdog(sc);
+        set_cond(c, run);
+    }
+    __device__ void on_skip() const {}
+    __device__ void begin() {
+        const bool odd = sc->iter & 1;
+        rc = odd ? r1 : r0;
+        rn = const_cast<float*>(odd ? r0 : r1);
+        pc = odd ? p1 : p0;
+        a = sc->alpha;
+        af = (float)a;
+    }
+    __device__ float gather(int col) const { return fmaf(-af, __ldg(q + col), __ldg(rc + col)); }
+    __device__ void row(int i, float s, double* acc) const {
+        const float rv = fmaf(-af, q[i], rc[i]);
+        rn[i] = rv;
+        if constexpr (IR) x[i] = fma(a, (double)pc[i], x[i]);
+        else x[i] = fmaf(af, pc[i], x[i]);
+        z[i] = s;
+        acc[0] += (double)rv * rv;
+        if (dinv) acc[1] += (double)rv * rv * dinv[i];
+        acc[2] += (double)rv * (double)s;
+    }
+    __device__ void finalize(const double* tot) const {
+        DevScalars* s = sc;
+        if constexpr (IR) {
+            // a due replacement ends the loop of iterations; the step after
+            // it (EpiReplace, EpiMzR) re-arms it
+            cg_finalize_ir(s, tot[0], tot[1]);
+            set_cond(c, !s->done && !s->replace);
+            if (s->replace || s->done) return;
+        } else {
+            cg_finalize_xr(s, tot[0], tot[1]);
+            set_cond(c, !s->done);
+            if (s->done) return;
+        }
+        if (s->mode == 2) fsai_beta(s, tot[2]);
+    }
 };
 
 // ============================ BiCGSTAB =====================================
@@ -513,6 +801,7 @@ bicg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restri
     s->delta2 = prm->delta * prm->delta;
     s->replace = 0;
     s->replaced = 0;
+    s->refresh = 0;
     if (!isfinite(bb)) {
         s->err = kErrNotFinite;
         s->done = 1;

@@ -112,7 +112,15 @@ void spmv_plan_free(SpmvPlan& p) {
 }
 
 cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s, int stages, int evict_first) {
-    if (tile_nnz <= 0) tile_nnz = default_tile_nnz(A.nnz, A.n_rows);
+    if (tile_nnz <= 0) {
+        tile_nnz = default_tile_nnz(A.nnz, A.n_rows);
+        // Between one and two waves of the solver kernels (5 CTAs per SM at
+        // least): larger tiles, so that every CTA takes exactly one and none
+        // runs two latency chains back to back.
+        const uint64_t wave = (uint64_t)num_sms() * 5;
+        const uint64_t nt0 = A.nnz ? (A.nnz + tile_nnz - 1) / tile_nnz : 1;
+        if (nt0 > wave && nt0 <= 2 * wave) tile_nnz = (int)((A.nnz + wave - 1) / wave);
+    }
     tile_nnz = (tile_nnz + 3) & ~3;
     const uint64_t nt = A.nnz ? (A.nnz + tile_nnz - 1) / tile_nnz : 1;
     SpmvPlan p;
@@ -191,7 +199,11 @@ bool pdl_enabled() {
     return v == 1;
 }
 
-void pdl_suspend(bool off) { t_pdl_off = off; }
+bool pdl_suspend(bool off) {
+    const bool prev = t_pdl_off;
+    t_pdl_off = off;
+    return prev;
+}
 
 int resident_ctas(const void* kernel, int threads, size_t smem) {
     static std::mutex mu;

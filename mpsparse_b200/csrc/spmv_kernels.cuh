@@ -16,10 +16,37 @@
 // Epilogues fuse the consumer of A*x (store, dot products, Richardson update,
 // FP64 residual) so that no SpMV result makes an extra trip through HBM.
 #pragma once
+#include <type_traits>
+#include <utility>
+
 #include "common.cuh"
 #include "internal.hpp"
 
 namespace mps {
+
+// Optional epilogue hooks, detected at compile time:
+//   __device__ void begin()         run by every thread once the kernel is
+//                                   active (loads the scalars it needs, picks
+//                                   buffers by iteration parity);
+//   __device__ float gather(int c)  element c of the multiplied vector when it
+//                                   is formed from other vectors on the fly
+//                                   (x is then unused).
+template <class E, class = void> struct epi_has_begin : std::false_type {};
+template <class E>
+struct epi_has_begin<E, std::void_t<decltype(std::declval<E&>().begin())>> : std::true_type {};
+template <class E, class = void> struct epi_has_gather : std::false_type {};
+template <class E>
+struct epi_has_gather<E, std::void_t<decltype(std::declval<const E&>().gather(0))>> : std::true_type {};
+
+template <class E>
+__device__ __forceinline__ void epi_begin(E& e) {
+    if constexpr (epi_has_begin<E>::value) e.begin();
+}
+template <class E>
+__device__ __forceinline__ float epi_x(const E& e, const float* __restrict__ x, int c) {
+    if constexpr (epi_has_gather<E>::value) return e.gather(c);
+    else return __ldg(x + c);
+}
 
 template <typename T> struct VT;
 template <> struct VT<float> { using v4 = float4; };
@@ -69,12 +96,14 @@ __device__ __forceinline__ void load_prod4(const CsrDev& A, const XT* __restrict
 //   __device__ void row(int r, ST s, double* acc)  consume row r's A*x
 //   __device__ void finalize(const double* tot)    last CTA, thread 0
 //   unsigned* counter; double* partials;           (when NS > 0)
+// and may provide begin() (no gather(): x is read as given).
 template <typename XT, typename ST, bool BF16, class Epi, int NT = kNT>
 __global__ void __launch_bounds__(NT, 4)
 spmv_tiles(CsrDev A, const XT* __restrict__ x, Epi epi) {
+    static_assert(!epi_has_gather<Epi>::value, "spmv_tiles reads x as given");
     extern __shared__ __align__(16) unsigned char spmv_smem[];
     ST* prod = reinterpret_cast<ST*>(spmv_smem);
-    __shared__ double red[NT / 32];
+    __shared__ double red[(Epi::NS > 0 ? Epi::NS : 1) * (NT / 32)];
     __shared__ ST redf[NT / 32];
     __shared__ int last_flag;
     if (blockIdx.x == 0 && threadIdx.x == 0) epi.tick();
@@ -82,6 +111,7 @@ spmv_tiles(CsrDev A, const XT* __restrict__ x, Epi epi) {
         if (blockIdx.x == 0 && threadIdx.x == 0) epi.on_skip();
         return;
     }
+    epi_begin(epi);
     double acc[Epi::NS > 0 ? Epi::NS : 1];
 #pragma unroll
     for (int i = 0; i < (Epi::NS > 0 ? Epi::NS : 1); ++i) acc[i] = 0.0;
@@ -130,16 +160,14 @@ spmv_tiles(CsrDev A, const XT* __restrict__ x, Epi epi) {
         }
     }
     if constexpr (Epi::NS > 0) {
+        block_sum_n<NT, Epi::NS>(acc, red);
+        if (threadIdx.x == 0) {
 #pragma unroll
-        for (int i = 0; i < Epi::NS; ++i) {
-            const double v = block_sum<NT>(acc[i], red);
-            if (threadIdx.x == 0) epi.partials[i * kMaxPartials + blockIdx.x] = v;
+            for (int i = 0; i < Epi::NS; ++i) epi.partials[i * kMaxPartials + blockIdx.x] = acc[i];
         }
         if (arrive_last(epi.counter, &last_flag)) {
             double tot[Epi::NS];
-#pragma unroll
-            for (int i = 0; i < Epi::NS; ++i)
-                tot[i] = sum_partials<NT>(epi.partials + i * kMaxPartials, gridDim.x, red);
+            sum_partials_n<NT, Epi::NS>(epi.partials, kMaxPartials, gridDim.x, red, tot);
             if (threadIdx.x == 0) epi.finalize(tot);
         }
     }

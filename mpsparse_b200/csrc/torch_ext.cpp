@@ -296,6 +296,43 @@ public:
         check(mps_fsai_attach(h_, m.handle(), cur_stream()), "attach_fsai");
     }
 
+    // "auto" / "split" (w = G r, z = G^T w) / "product" (z = (G^T G) r)
+    void set_fsai_apply(const std::string& mode) {
+        c10::cuda::CUDAGuard g(device_);
+        int32_t m;
+        if (mode == "auto") m = MPS_FSAI_APPLY_AUTO;
+        else if (mode == "split") m = MPS_FSAI_APPLY_SPLIT;
+        else if (mode == "product") m = MPS_FSAI_APPLY_PRODUCT;
+        else throw std::invalid_argument("mode must be 'auto', 'split' or 'product'");
+        check(mps_csr_set_fsai_apply(h_, m, cur_stream()), "set_fsai_apply");
+    }
+
+    std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> fsai_product() const {
+        c10::cuda::CUDAGuard g(device_);
+        int32_t f = -1;
+        uint64_t nnz_m = 0;
+        check(mps_csr_fsai_apply(h_, &f, &nnz_m), "fsai_product");
+        auto o = torch::TensorOptions().device(torch::kCUDA, device_);
+        auto rp = torch::empty({n_rows_ + 1}, o.dtype(torch::kInt32));
+        auto ci = torch::empty({(int64_t)nnz_m}, o.dtype(torch::kInt32));
+        auto v = torch::empty({(int64_t)nnz_m}, o.dtype(torch::kFloat32));
+        check(mps_csr_fsai_product_get(h_, rp.data_ptr<int32_t>(), ci.data_ptr<int32_t>(),
+                                       v.data_ptr<float>(), cur_stream()),
+              "fsai_product");
+        return {rp, ci, v};
+    }
+
+    py::dict fsai_apply() const {
+        int32_t f = -1;
+        uint64_t nnz_m = 0;
+        check(mps_csr_fsai_apply(h_, &f, &nnz_m), "fsai_apply");
+        py::dict d;
+        d["form"] = f < 0 ? py::object(py::none())
+                          : py::object(py::str(f == MPS_FSAI_APPLY_PRODUCT ? "product" : "split"));
+        d["nnz_m"] = nnz_m;
+        return d;
+    }
+
     double fsai_train_step(FsaiModel& m, int64_t n_probes, c10::optional<torch::Tensor> extra,
                            double lr, int64_t seed) {
         c10::cuda::CUDAGuard g(device_);
@@ -633,6 +670,9 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         .def("set_fsai", &CsrTensor::set_fsai, py::arg("row_ptr"), py::arg("col_ind"),
              py::arg("values"))
         .def("attach_fsai", &CsrTensor::attach_fsai, py::arg("model"))
+        .def("set_fsai_apply", &CsrTensor::set_fsai_apply, py::arg("mode"))
+        .def("fsai_apply", &CsrTensor::fsai_apply)
+        .def("fsai_product", &CsrTensor::fsai_product)
         .def("fsai_train_step", &CsrTensor::fsai_train_step, py::arg("model"), py::arg("n_probes") = 4,
              py::arg("extra") = py::none(), py::arg("lr") = 1e-3, py::arg("seed") = 0)
         .def("fsai_features", &CsrTensor::fsai_features)
