@@ -346,7 +346,8 @@ def e2e_drop_in(args, systems, dev, warm, steps, fsai=None):
     path = ("spmv.csr_tensor(pinned host COO) + attach_fsai + cg_mixed(pinned host b, x FP64)"
             if fsai is not None else "spmv.csr_tensor(pinned host COO) + cgd(pinned host b, x)")
     return {"value": statistics.mean(times), "unit": UNIT, "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "path": path}
+            "d2h_bytes_per_step": d2h, "path": path,
+            "step_ms": [round(t, 3) for t in times], "median": statistics.median(times)}
 
 
 def batched_c5(args, dev):

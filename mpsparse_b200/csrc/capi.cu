@@ -52,6 +52,17 @@ int num_sms() {
     return sms;
 }
 
+size_t l2_bytes() {
+    static size_t l2 = 0;
+    if (!l2) {
+        int d = 0, v = 0;
+        cudaGetDevice(&d);
+        cudaDeviceGetAttribute(&v, cudaDevAttrL2CacheSize, d);
+        l2 = v > 0 ? (size_t)v : ((size_t)126 << 20);
+    }
+    return l2;
+}
+
 mps_status device_error(unsigned err, const char* what) {
     if (err & kErrRange) return fail(MPS_ERR_RANGE, std::string(what) + ": a key lies outside [0, num_rows) x [0, num_cols)");
     if (err & kErrTimeout) return fail(MPS_ERR_TIMEOUT, std::string(what) + ": a bounded device wait gave up");

@@ -21,6 +21,7 @@ mps_status cuda_fail(cudaError_t e, const char* what);
     } while (0)
 
 int num_sms();
+size_t l2_bytes();        // L2 cache of the current device
 
 // Stream-ordered scratch allocations of the library come from one memory
 // pool per device that keeps its memory after frees (release threshold at
@@ -95,6 +96,7 @@ struct SpmvPlan {
     int grid_s = 0;           // persistent CTAs of the TMA kernel
     int stages = 2;           // TMA pipeline depth (2 or 3)
     int evict_first = 1;      // L2 evict-first hint on the col_ind/value copies
+    bool evict_auto = true;   // hint chosen by size (no caller set it)
     int max_tile_nnz = 0;     // largest tile (nonzeros) and row count of the plan
     int max_tile_rows = 0;
 };

@@ -131,7 +131,21 @@ cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s, int stages,
     p.grid = p.ntiles < cap_grid ? p.ntiles : cap_grid;
     if (p.grid < 1) p.grid = 1;
     p.stages = stages > 0 ? stages : A.plan.stages;
-    p.evict_first = evict_first >= 0 ? evict_first : A.plan.evict_first;
+    // L2 hint: by size unless a caller (autotuner, set_spmv_plan, the
+    // factors following A) chose it.  A matrix well inside L2 stays there
+    // between the kernels of a solve; a larger one is streamed past L2 so
+    // that the gathered vector keeps its lines.
+    if (evict_first >= 0) {
+        p.evict_first = evict_first ? 1 : 0;
+        p.evict_auto = false;
+    } else if (!A.plan.evict_auto) {
+        p.evict_first = A.plan.evict_first;
+        p.evict_auto = false;
+    } else {
+        const size_t stream_bytes = (size_t)A.nnz * 8 + (size_t)A.n_rows * 4;
+        p.evict_first = stream_bytes > l2_bytes() / 4 ? 1 : 0;
+        p.evict_auto = true;
+    }
     p.grid_s = p.ntiles < num_sms() * 6 ? p.ntiles : num_sms() * 6;
     if (p.grid_s < 1) p.grid_s = 1;
     // tile_row has 2 spare ints at the end for the plan statistics
