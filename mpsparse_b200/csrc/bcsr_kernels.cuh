@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "internal.hpp"
 #include "tma.cuh"
+#include "spmv_kernels.cuh"
 
 namespace mps {
 
@@ -166,9 +167,11 @@ bcsr_tiles(BcsrDev A, const float* __restrict__ x, Epi epi) {
             for (int i = 0; i < Epi::NS; ++i) epi.partials[i * kMaxPartials + blockIdx.x] = acc[i];
         }
         if (arrive_last(epi.counter, &last_flag)) {
+            __shared__ DevScalars s_sc;
+            scalars_stage_in<NT>(epi, &s_sc);
             double tot[Epi::NS];
             sum_partials_n<NT, Epi::NS>(epi.partials, kMaxPartials, gridDim.x, red, tot);
-            if (threadIdx.x == 0) epi.finalize(tot);
+            finalize_staged<NT>(epi, tot, &s_sc);
         }
     }
 }

@@ -114,10 +114,10 @@ void spmv_plan_free(SpmvPlan& p) {
 cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s, int stages, int evict_first) {
     if (tile_nnz <= 0) {
         tile_nnz = default_tile_nnz(A.nnz, A.n_rows);
-        // Between one and two waves of the solver kernels (5 CTAs per SM at
+        // Between one and two waves of the solver kernels (4 CTAs per SM at
         // least): larger tiles, so that every CTA takes exactly one and none
         // runs two latency chains back to back.
-        const uint64_t wave = (uint64_t)num_sms() * 5;
+        const uint64_t wave = (uint64_t)num_sms() * 4;
         const uint64_t nt0 = A.nnz ? (A.nnz + tile_nnz - 1) / tile_nnz : 1;
         if (nt0 > wave && nt0 <= 2 * wave) tile_nnz = (int)((A.nnz + wave - 1) / wave);
     }

@@ -38,6 +38,47 @@ template <class E, class = void> struct epi_has_gather : std::false_type {};
 template <class E>
 struct epi_has_gather<E, std::void_t<decltype(std::declval<const E&>().gather(0))>> : std::true_type {};
 
+// Epilogues of the solvers keep their scalars in `DevScalars* sc`.  The
+// last CTA runs finalize() on a shared-memory copy of them: one cooperative
+// load (issued beside the partial sums' loads) instead of a chain of
+// dependent global loads by one thread, then the copy is written back.  Only
+// block 0's tick() writes the scalars during a launch, before block 0
+// arrives, so the copy the last CTA takes is current.
+template <class E, class = void> struct epi_has_sc : std::false_type {};
+template <class E>
+struct epi_has_sc<E, std::enable_if_t<std::is_same<decltype(std::declval<E&>().sc), DevScalars*>::value>>
+    : std::true_type {};
+
+template <int NT, class E>
+__device__ __forceinline__ void scalars_stage_in(const E& e, DevScalars* sh) {
+    if constexpr (epi_has_sc<E>::value) {
+        static_assert(sizeof(DevScalars) % 8 == 0, "DevScalars is copied in 8-byte words");
+        constexpr int W = (int)(sizeof(DevScalars) / 8);
+        const unsigned long long* g = reinterpret_cast<const unsigned long long*>(e.sc);
+        unsigned long long* l = reinterpret_cast<unsigned long long*>(sh);
+        for (int i = threadIdx.x; i < W; i += NT) l[i] = __ldcg(g + i);
+    }
+}
+
+// After a block barrier that follows scalars_stage_in.
+template <int NT, class E>
+__device__ __forceinline__ void finalize_staged(const E& e, const double* tot, DevScalars* sh) {
+    if constexpr (epi_has_sc<E>::value) {
+        if (threadIdx.x == 0) {
+            E ec = e;
+            ec.sc = sh;
+            ec.finalize(tot);
+        }
+        __syncthreads();
+        constexpr int W = (int)(sizeof(DevScalars) / 8);
+        unsigned long long* g = reinterpret_cast<unsigned long long*>(e.sc);
+        const unsigned long long* l = reinterpret_cast<const unsigned long long*>(sh);
+        for (int i = threadIdx.x; i < W; i += NT) g[i] = l[i];
+    } else {
+        if (threadIdx.x == 0) e.finalize(tot);
+    }
+}
+
 template <class E>
 __device__ __forceinline__ void epi_begin(E& e) {
     if constexpr (epi_has_begin<E>::value) e.begin();
@@ -166,9 +207,11 @@ spmv_tiles(CsrDev A, const XT* __restrict__ x, Epi epi) {
             for (int i = 0; i < Epi::NS; ++i) epi.partials[i * kMaxPartials + blockIdx.x] = acc[i];
         }
         if (arrive_last(epi.counter, &last_flag)) {
+            __shared__ DevScalars s_sc;
+            scalars_stage_in<NT>(epi, &s_sc);
             double tot[Epi::NS];
             sum_partials_n<NT, Epi::NS>(epi.partials, kMaxPartials, gridDim.x, red, tot);
-            if (threadIdx.x == 0) epi.finalize(tot);
+            finalize_staged<NT>(epi, tot, &s_sc);
         }
     }
 }
