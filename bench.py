@@ -270,13 +270,13 @@ def run_ours(args, rank, world, dev):
         # G^T G values in product form) + ||b||^2 + init + per iteration 2
         # kernels (product form: direction + A p, update + M r) or 3 (split:
         # A p, update + G r, G^T w) + 2 per residual replacement + the FP64
-        # true residual at the end; the product form's graph runs 4
+        # true residual at the end; the product form's graph runs 16
         # iterations per loop body, so after each replacement (and at the
-        # stop) about 1.5 iterations' kernels return at once: 3 launches
+        # stop) about 7.5 iterations' kernels return at once: 15 launches
         def per_solve(i):
             if i.get("form") == "product":
                 rounds = max(i["outer"], 1)
-                return 4 + 1 + 2 + 2 * i["iters"] + 2 * rounds + 3 * rounds + 1
+                return 4 + 1 + 2 + 2 * i["iters"] + 2 * rounds + 15 * rounds + 1
             return 3 + 1 + 3 + 3 * i["iters"] + 2 * i["outer"] + 1
         launches = sum(per_solve(i) for i in infos)
     else:
