@@ -273,6 +273,12 @@ static RowInfoDev rinfo_of(const FsaiWork& w, int n) {
     return RowInfoDev{f, f + n, reinterpret_cast<int4*>(f + 2 * (size_t)n)};
 }
 
+// idx[k] = k: the payload that turns the sorted G^T keys into the permutation.
+static __global__ void iota_kernel(uint32_t* __restrict__ idx, long n) {
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
+        idx[k] = (uint32_t)k;
+}
+
 // G's pattern, G^T (pattern + permutation), per-row info and the features.
 static mps_status fsai_prepare(mps_csr* h, cudaStream_t s) {
     FsaiWork& w = h->fw;
@@ -312,19 +318,15 @@ static mps_status fsai_prepare(mps_csr* h, cudaStream_t s) {
     MPS_CUDA(cudaMalloc(&w.d_loss, 8));
     MPS_CUDA(cudaMalloc(&w.vec, 6 * ((size_t)n + 4) * 4));
     g_fill_kernel<<<g1(n), 256, 0, s>>>(A.rp, A.ci, n, h->G.rp, h->G.ci, w.g_row, w.g_aidx);
-    MPS_CUDA(spmv_plan_build(h->G, 0, s));
+    // (G's SpMV plan is built below, with G^T's, by factor_plans_follow)
     // G^T: sort (col << 32 | row) keys with the G index as payload
     unsigned long long* keys = nullptr;
     uint32_t* idx = nullptr;
     MPS_CUDA(stream_alloc(&keys, nz * 8, s));
     MPS_CUDA(stream_alloc(&idx, nz * 4, s));
     MPS_CUDA(transpose_keys_launch(h->G, keys, s));
-    {
-        std::vector<uint32_t> iota((size_t)nnz_g);
-        for (int k = 0; k < nnz_g; ++k) iota[k] = (uint32_t)k;
-        MPS_CUDA(cudaMemcpyAsync(idx, iota.data(), (size_t)nnz_g * 4, cudaMemcpyHostToDevice, s));
-        MPS_CUDA(cudaStreamSynchronize(s));
-    }
+    iota_kernel<<<g1(nnz_g), 256, 0, s>>>(idx, (long)nnz_g);
+    MPS_CUDA(cudaGetLastError());
     st = build_from_keys(h->Gt, reinterpret_cast<const uint64_t*>(keys), idx, (uint64_t)nnz_g, n, n,
                          h->d_err, s);
     cudaFreeAsync(keys, s);
