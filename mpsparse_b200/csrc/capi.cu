@@ -104,15 +104,16 @@ static mps_status check_shape(uint64_t nnz, uint32_t n_rows, uint32_t n_cols) {
     return MPS_OK;
 }
 
-// Sort + CSR + tile plan into a fresh CsrMat.
+// Sort + CSR + tile plan into a fresh CsrMat (plan = false: the caller
+// builds the plan afterwards, as the FSAI factors do with A's pipeline).
 mps_status build_from_keys(CsrMat& m, const uint64_t* keys, const uint32_t* payload,
                                   uint64_t nnz, uint32_t n_rows, uint32_t n_cols, unsigned* d_err,
-                                  cudaStream_t s) {
+                                  cudaStream_t s, bool plan) {
     mps_status st = alloc_csr(m, n_rows, n_cols, nnz, d_err);
     if (st != MPS_OK) return st;
     MPS_CUDA(cudaMemsetAsync(d_err, 0, sizeof(unsigned), s));
     MPS_CUDA(sort_to_csr(keys, payload, nnz, n_rows, n_cols, m.rp, m.ci, (uint32_t*)m.v, d_err, s));
-    MPS_CUDA(spmv_plan_build(m, 0, s));
+    if (plan) MPS_CUDA(spmv_plan_build(m, 0, s));
     unsigned err = 0;
     MPS_CUDA(cudaMemcpyAsync(&err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     MPS_CUDA(cudaStreamSynchronize(s));
@@ -425,7 +426,7 @@ mps_status mps_csr_set_fsai(mps_csr* h, const int32_t* d_g_row_ptr, const int32_
     MPS_CUDA(stream_alloc(&keys, (g_nnz ? g_nnz : 1) * 8, s));
     MPS_CUDA(transpose_keys_launch(h->G, keys, s));
     st = build_from_keys(h->Gt, reinterpret_cast<const uint64_t*>(keys),
-                         reinterpret_cast<const uint32_t*>(h->G.v), g_nnz, n, n, h->d_err, s);
+                         reinterpret_cast<const uint32_t*>(h->G.v), g_nnz, n, n, h->d_err, s, false);
     cudaFreeAsync(keys, s);
     if (st != MPS_OK) return st;
     MPS_CUDA(factor_plans_follow(h, s));

@@ -328,7 +328,7 @@ static mps_status fsai_prepare(mps_csr* h, cudaStream_t s) {
     iota_kernel<<<g1(nnz_g), 256, 0, s>>>(idx, (long)nnz_g);
     MPS_CUDA(cudaGetLastError());
     st = build_from_keys(h->Gt, reinterpret_cast<const uint64_t*>(keys), idx, (uint64_t)nnz_g, n, n,
-                         h->d_err, s);
+                         h->d_err, s, false);   // plans: factor_plans_follow below
     cudaFreeAsync(keys, s);
     cudaFreeAsync(idx, s);
     if (st != MPS_OK) return st;
