@@ -15,8 +15,17 @@ Also measured in the same run (reported, not the headline):
   * cpu_baseline: the CPU oracle's CG on the box's host cores (bounded sample)
     and scipy.sparse.linalg.cg beside it.
 
+  * configs: the other configurations at full size, every answer judged by
+    its FP64 true residual -- C1 CG on the 256^2 Laplacian (iterations
+    against the FP64 oracle, scipy cg on the host), C2 BiCGSTAB on the BCSR
+    4x4 system with 65,536 block rows (BCSR SpMV GB/s, scipy bicgstab), C3
+    mixed-precision CG to 1e-10 with FP32 and BF16 values and plain FP32 CG
+    on the 256^3 operator, with the error against the FP64 oracle on its
+    64^3 member.
+
 `--impl reference` times the reference algorithm's CPU implementation (the
-oracle port of iterative/BiCGSTAB/spmv.cpp cgd_op) on the host cores.
+oracle port of iterative/BiCGSTAB/spmv.cpp cgd_op, FP64, every solve run to
+convergence) on the host cores; it never loads this package's CUDA code.
 """
 from __future__ import annotations
 
@@ -41,6 +50,44 @@ WORKLOAD = "512x512 log-normal diffusion (2D 5-pt, sigma 1.5, corr 16), held-out
 TEST_SEED0 = 100_000        # held-out seeds start here (training uses 0..1999)
 TOL = 1e-6
 MAX_ITER = 40_000
+
+
+def _workloads():
+    """The seeded generators (mpsparse_b200/workloads.py, numpy only) loaded
+    by file path, so the CPU arms never import the package (whose import
+    loads the CUDA extension)."""
+    import importlib.util
+    name = "mpsparse_b200_workloads"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(
+        name, os.path.join(ROOT, "mpsparse_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def host_info():
+    """Host cores and thread settings the CPU numbers ran with."""
+    info = {"affinity_cores": host_threads(), "cpu_count": os.cpu_count()}
+    for k in ("OMP_NUM_THREADS", "MKL_NUM_THREADS", "OPENBLAS_NUM_THREADS"):
+        info[k] = os.environ.get(k)
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    info["cpu_model"] = line.split(":", 1)[1].strip()
+                    break
+    except Exception:
+        pass
+    try:
+        from threadpoolctl import threadpool_info
+        info["blas"] = [{"lib": t.get("internal_api"), "threads": t.get("num_threads")}
+                        for t in threadpool_info()]
+    except Exception:
+        pass
+    return info
 
 
 def peaks():
@@ -135,7 +182,7 @@ class ClockSampler:
 
 # ------------------------------------------------------------- systems -----
 def c4_system(seed):
-    from mpsparse_b200 import workloads as W
+    W = _workloads()
     coo = W.diffusion_512sq(seed).shuffled(seed + 1)
     b = W.rhs(coo.n, seed + 2)
     return coo, b
@@ -282,6 +329,7 @@ def run_ours(args, rank, world, dev):
     else:
         launches = sum(2 + 3 * i["iters"] for i in infos)   # init + 3 kernels/iteration + copy
 
+    ptrue = [i.get("true_resid", -1.0) for i in pinfos]
     out = {
         "solver": solver_name,
         "ms_per_solve": total_ms / steps,
@@ -291,23 +339,36 @@ def run_ours(args, rank, world, dev):
         "step_ms": [round(t, 3) for t in times],
         "plain_cg": {"ms_per_solve": statistics.mean(ptimes), "step_ms": [round(t, 3) for t in ptimes],
                      "iters_mean": statistics.mean(i["iters"] for i in pinfos),
-                     "true_resid_max": max(presid)},
+                     "true_resid_max": max(presid),
+                     "true_resid_max_reported": max(ptrue),
+                     "stop_rule_met": sum(bool(i["stop_rule_met"]) for i in pinfos),
+                     "converged_fp64": sum(bool(i["converged"]) for i in pinfos),
+                     "note": "FP32 CG stops on its recurrence residual; the FP64 true residual of "
+                             "the FP32 x it returns stays above 1e-6 on these systems, so its "
+                             "time is a lower bound on a time to 1e-6"},
         "jacobi_pcg": {"ms_per_solve": statistics.mean(jtimes), "step_ms": [round(t, 3) for t in jtimes],
-                       "iters_mean": statistics.mean(i["iters"] for i in jinfos)},
+                       "iters_mean": statistics.mean(i["iters"] for i in jinfos),
+                       "true_resid_max": max(i.get("true_resid", -1.0) for i in jinfos)},
         "outer_mean": statistics.mean(i.get("outer", 0) for i in infos),
         "setup_ms_first_solve": setup_ms,
         "clocks": clocks, "gpu_launches": launches, "wall_s": t_wall,
     }
     out["e2e"] = e2e_drop_in(args, systems, dev, warm, steps,
                              fsai if args.solver == "learned" else None)
-    out["spmv"] = spmv_c3(args, dev) if not args.skip_spmv else None
-    out["batched"] = batched_c5(args, dev) if not args.skip_batched else None
+    out["e2e_plain_cg"] = (e2e_drop_in(args, systems, dev, warm, steps, None)
+                           if args.solver == "learned" and not args.skip_e2e_plain else None)
+    single = world == 1
+    c3 = C3Context(args, dev) if single and not (args.skip_spmv and args.skip_configs) else None
+    out["spmv"] = spmv_c3(args, dev, c3) if single and not args.skip_spmv else None
+    out["batched"] = batched_c5(args, dev, rank, world) if not args.skip_batched else None
+    out["configs"] = configs_legs(args, dev, c3) if single and not args.skip_configs else None
     return out
 
 
 def e2e_drop_in(args, systems, dev, warm, steps, fsai=None):
     """csr_tensor from pinned host COO + the solve with pinned host b/x, per
-    step (learned: attach the network factor, then cg_mixed in FP64)."""
+    step (learned: attach the network factor, then cg_mixed in FP64; else
+    the plain FP32 cgd drop-in)."""
     import torch
     import mpsparse_b200 as mps
     n = systems[0][0].n
@@ -350,21 +411,30 @@ def e2e_drop_in(args, systems, dev, warm, steps, fsai=None):
             "step_ms": [round(t, 3) for t in times], "median": statistics.median(times)}
 
 
-def batched_c5(args, dev):
+def batched_c5(args, dev, rank=0, world=1):
     """4096 independent SPD systems (row counts log-uniform in [1024, 65536];
     half 2D log-normal diffusion grids, sigma 1, correlation 8; half random
     graph Laplacians, mean degree 8, + 1e-2 I) in one graph-launched
-    persistent kernel; learned FSAI kept per class where it beats Jacobi,
-    warps per system autotuned.  solves/s at 1e-6, FP64-checked residuals."""
+    persistent kernel per GPU; learned FSAI kept per class where it beats
+    Jacobi, warps per system autotuned.  With N ranks each GPU solves an
+    nnz-balanced share of the systems (no collective on the data path); the
+    time is the max over ranks and the per-system records are gathered.
+    solves/s at 1e-6, every system's FP64 true residual checked."""
     import torch
-    from mpsparse_b200 import workloads as W
+    from mpsparse_b200 import shard
     from mpsparse_b200.batched import BatchedSolver
     from mpsparse_b200.fsai import LearnedFsai
-    keys, vals, off, kinds = W.batch_systems(args.batch_systems, seed=7)
+    W = _workloads()
+    n_sys = args.batch_systems
+    _, _, est_nnz = W.batch_plan(n_sys, 7)
+    mine = shard.partition_by_nnz(est_nnz, world)[rank] if world > 1 else np.arange(n_sys)
+    keys, vals, off, kinds = W.batch_systems(n_sys, seed=7, select=mine)
     S = BatchedSolver.from_coo(keys, vals, off)
     del keys, vals
-    g = torch.Generator(device=dev).manual_seed(11)
-    b = torch.randn(S.n, generator=g, device=dev)
+    # b ~ N(0,1) per system from the system's own seed (the same b whatever
+    # the sharding)
+    b = torch.from_numpy(np.concatenate([W.rhs(int(off[k + 1] - off[k]), 11_000_003 + int(s))
+                                         for k, s in enumerate(mine)])).to(dev)
     S.attach_fsai(LearnedFsai.load())
     choice = S.choose_precond(b, kinds, sample=16)
     tune = S.autotune(b)
@@ -372,6 +442,8 @@ def batched_c5(args, dev):
     stream = torch.cuda.current_stream()
     S.solve(b, x)
     torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
     times = []
     for _ in range(3):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -380,6 +452,7 @@ def batched_c5(args, dev):
         e1.record(stream)
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
+    ms_local = statistics.median(times)
     it, cv = it.cpu().numpy(), cv.cpu().numpy()
     # FP64 true residual of every system (verification, untimed)
     rp, ci, v = S.csr
@@ -396,32 +469,57 @@ def batched_c5(args, dev):
     ax = (Mabs @ x.double().abs().unsqueeze(1)).squeeze(1)
     fn = torch.zeros(S.n_systems, dtype=torch.float64, device=dev).index_add_(0, seg, ax * ax)
     floor = (16 * 2.0 ** -24 * fn.sqrt() / bn.sqrt()).cpu().numpy()
-    ms = statistics.median(times)
-    return {"workload": f"{S.n_systems} SPD systems, n log-uniform [1024, 65536], half 2D "
+    ms, rows, nnz = ms_local, S.n, int(S.nnz.sum())
+    if world > 1:
+        ms = shard.max_over_ranks(ms_local, device=dev)
+        rel = shard.gather_records(rel, mine, n_sys, device=dev)
+        floor = shard.gather_records(floor, mine, n_sys, device=dev)
+        it = shard.gather_records(it, mine, n_sys, device=dev)
+        cv = shard.gather_records(cv, mine, n_sys, device=dev)
+        kinds = W.batch_plan(n_sys, 7)[0]
+        rows = int(sum(shard.gather_records([float(S.n)], [rank], world, device=dev)))
+        nnz = int(sum(shard.gather_records([float(S.nnz.sum())], [rank], world, device=dev)))
+    return {"workload": f"{n_sys} SPD systems, n log-uniform [1024, 65536], half 2D "
                         "log-normal diffusion (sigma 1, corr 8), half graph Laplacians + 0.01 I",
-            "rows": S.n, "nnz": int(S.nnz.sum()), "ms": ms,
-            "solves_per_s": S.n_systems / (ms * 1e-3), "converged": int(cv.sum()),
-            "true_resid_max": float(rel.max()),
+            "rows": rows, "nnz": nnz, "ms": ms, "ms_per_rank_local": ms_local, "ranks": world,
+            "sharding": "nnz-balanced LPT shares, one persistent launch per GPU" if world > 1
+                        else "one GPU",
+            "solves_per_s": n_sys / (ms * 1e-3), "converged_recurrence": int(np.sum(cv)),
+            "converged_fp64_1e-6": int((rel <= 1e-6).sum()),
+            "true_resid_max": float(np.max(rel)),
             "systems_within_tol_or_fp32_floor": int((rel <= np.maximum(2e-6, floor)).sum()),
-            "iters_mean": {"grid": float(it[kinds == 0].mean()), "graph": float(it[kinds == 1].mean())},
+            "iters_mean": {"grid": float(np.mean(it[kinds == 0])), "graph": float(np.mean(it[kinds == 1]))},
             "precond_choice": {str(k): v["chosen"] for k, v in choice.items()},
             "warps_per_system": tune["warps_per_system"], "launches_per_solve": 1}
 
 
-def spmv_c3(args, dev):
+class C3Context:
+    """The 256^3 7-point log-normal diffusion operator (C3's matrix, 1.14 GB
+    per SpMV) built once on the GPU from device COO keys; shared by the SpMV
+    roofline leg and the C3 solve legs."""
+
+    def __init__(self, args, dev):
+        import torch
+        import mpsparse_b200 as mps
+        W = _workloads()
+        self.m = args.c3_grid
+        coo = W.lognormal_diffusion_3d(self.m, 1.0, 8.0, 0)
+        e = torch.empty(0)
+        self.keys = torch.from_numpy(coo.keys()).to(dev)
+        self.vals = torch.from_numpy(coo.vals).to(dev)
+        self.A = mps.spmv.csr_tensor(self.keys, self.vals, e, e, e, coo.n, coo.n, fill_outputs=False)
+        self.n, self.nnz = coo.n, coo.nnz
+        del coo
+
+    def drop_coo(self):
+        self.keys = self.vals = None
+
+
+def spmv_c3(args, dev, ctx):
     """CSR SpMV on the 256^3 7-point diffusion operator: GB/s by the byte model
     8*nnz + 4*(n+1) + 4*n_cols + 4*n_rows, CUDA events per launch."""
     import torch
-    import mpsparse_b200 as mps
-    from mpsparse_b200 import workloads as W
-    m = args.c3_grid
-    coo = W.lognormal_diffusion_3d(m, 1.0, 8.0, 0)
-    e = torch.empty(0)
-    keys_d = torch.from_numpy(coo.keys()).to(dev)
-    vals_d = torch.from_numpy(coo.vals).to(dev)
-    A = mps.spmv.csr_tensor(keys_d, vals_d, e, e, e, coo.n, coo.n, fill_outputs=False)
-    n, nnz = coo.n, coo.nnz
-    del coo
+    A, n, nnz = ctx.A, ctx.n, ctx.nnz
     x = torch.randn(n, device=dev)
     y = torch.empty(n, device=dev)
     stream = torch.cuda.current_stream()
@@ -439,18 +537,20 @@ def spmv_c3(args, dev):
     ms = statistics.median(a.elapsed_time(b) for a, b in evs)
     bytes_alg = 8 * nnz + 4 * (n + 1) + 4 * n + 4 * n
     gbs = bytes_alg / (ms * 1e-3) / 1e9
-    out = {"workload": f"{m}^3 7-pt log-normal diffusion", "n": n, "nnz": nnz,
+    out = {"workload": f"{ctx.m}^3 7-pt log-normal diffusion", "n": n, "nnz": nnz,
            "bytes_per_launch": bytes_alg, "ms": ms, "gbs": gbs, "launches": reps,
            "plan": {k: plan[k] for k in ("tile_nnz", "stages", "evict_first")}}
     if not args.only_spmv:
-        out["vendor"] = vendor_baselines(A, keys_d, vals_d, x, n, nnz, bytes_alg, stream)
+        out["vendor"] = vendor_baselines(A, ctx.keys, ctx.vals, x, n, nnz, bytes_alg, stream)
     return out
 
 
-def _event_ms(fn, stream, reps):
+def _event_ms(fn, stream, reps, flush=None):
     import torch
     ts = []
     for _ in range(reps):
+        if flush is not None:
+            flush_l2(flush)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         fn()
@@ -481,43 +581,209 @@ def vendor_baselines(A, keys, vals, x, n, nnz, bytes_alg, stream):
             "ours_coo_to_csr_gbs_onepass_model": (20 * nnz + 4 * (n + 1)) / (ours_ms * 1e-3) / 1e9}
 
 
+# ------------------------------------------------- the other configurations --
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def scipy_solve(method, coo, b, tol, max_iter, budget_s=None):
+    """scipy.sparse.linalg cg / bicgstab on the host cores (FP64, x0 = 0),
+    the CPU path the reference benchmarks against; time, iterations, FP64
+    true residual.  budget_s: a bounded run (stopped by maxiter), flagged."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    rp, ci, v = coo.to_csr()
+    A = sp.csr_matrix((v.astype(np.float64), ci, rp), shape=(coo.n, coo.n))
+    bb = np.asarray(b, np.float64)
+    fn = spla.cg if method == "cg" else spla.bicgstab
+    cap = max_iter
+    if budget_s is not None:
+        t0 = time.perf_counter()
+        fn(A, bb, rtol=1e-300, atol=0.0, maxiter=20)
+        per_it = (time.perf_counter() - t0) / 20
+        cap = max(20, min(max_iter, int(budget_s / per_it)))
+    it = [0]
+    t0 = time.perf_counter()
+    x, flag = fn(A, bb, rtol=tol, atol=0.0, maxiter=cap, callback=lambda xk: it.__setitem__(0, it[0] + 1))
+    dt = time.perf_counter() - t0
+    res = float(np.linalg.norm(bb - A @ x) / np.linalg.norm(bb))
+    return {"ms": dt * 1e3, "iters": it[0], "converged": flag == 0, "true_resid": res,
+            "capped_by_budget": bool(flag != 0 and cap < max_iter)}
+
+
+def c1_leg(dev, flush):
+    """C1: plain FP32 CG (the drop-in cgd) on the 256x256 5-point Laplacian,
+    seed-shuffled COO built on the GPU, tol 1e-6, max 2000 iterations."""
+    import torch
+    import mpsparse_b200 as mps
+    from oracle import oracle as O
+    W = _workloads()
+    coo = W.laplacian_256().shuffled(1)
+    b = W.rhs(coo.n, 0)
+    e = torch.empty(0)
+    A = mps.spmv.csr_tensor(torch.from_numpy(coo.keys()).to(dev), torch.from_numpy(coo.vals).to(dev),
+                            e, e, e, coo.n, coo.n, fill_outputs=False)
+    bt = torch.from_numpy(b).to(dev)
+    x = torch.zeros(coo.n, device=dev)
+    last = {}
+
+    def solve():
+        x.zero_()
+        last["info"] = A.cgd(bt, x, tol=1e-6, max_iter=2000)
+    solve()
+    ms = _event_ms(solve, torch.cuda.current_stream(), 10, flush)
+    info = last["info"]
+    Ao = O.Csr(*coo.to_csr(), coo.n)
+    xo, io = O.cg(Ao, b.astype(np.float64), tol=1e-6, max_iter=2000, threads=host_threads())
+    x20 = torch.zeros(coo.n, device=dev)
+    A.cgd(bt, x20, tol=1e-300, max_iter=20)
+    xo20, _ = O.cg(Ao, b.astype(np.float64), tol=0.0, max_iter=20)
+    xc = torch.zeros(coo.n, device=dev)
+    ic = A.cgd(bt, xc, reference_compat=True)
+    xoc, ioc = O.cg(Ao, b.astype(np.float64), compat=True)
+    sc = scipy_solve("cg", coo, b, 1e-6, 2000)
+    return {"workload": "256x256 5-pt Laplacian (Dirichlet), n 65,536, nnz 326,656, shuffled COO",
+            "solver": "cgd (plain FP32 CG), tol 1e-6, max 2000", "ms": ms, "iters": info["iters"],
+            "oracle_fp64_iters": io["iters"], "true_resid": info["true_resid"],
+            "converged_fp64": bool(info["converged"]),
+            "iterate20_rel_diff_vs_oracle": _rel(x20.cpu().numpy(), xo20),
+            "reference_compat": {"iters": ic["iters"], "oracle_iters": ioc["iters"],
+                                 "true_resid": ic["true_resid"],
+                                 "rel_diff_vs_oracle": _rel(xc.cpu().numpy(), xoc)},
+            "scipy_cg_host": sc}
+
+
+def c2_leg(dev, flush):
+    """C2: plain FP32 BiCGSTAB on the BCSR 4x4 system with 65,536 block rows
+    (8 off-diagonal blocks per row, diagonally dominant, nonsymmetric), BCSR
+    built on the GPU from seed-shuffled COO keys; BCSR SpMV GB/s with L2
+    flushed before each launch."""
+    import torch
+    import mpsparse_b200 as mps
+    from oracle import oracle as O
+    W = _workloads()
+    bm = W.block_dominant_65536(0)
+    coo = bm.to_coo(drop_zeros=True).shuffled(2)
+    n = coo.n
+    b = W.rhs(n, 3)
+    ei = torch.empty(0, dtype=torch.int32)
+    A = mps.bcsr.bcsr_tensor(torch.from_numpy(coo.keys()).to(dev), torch.from_numpy(coo.vals).to(dev),
+                             ei, ei, n, n, 4)
+    bt = torch.from_numpy(b).to(dev)
+    x = torch.zeros(n, device=dev)
+    last = {}
+
+    def solve():
+        x.zero_()
+        last["info"] = A.bicgstab(bt, x, tol=1e-6, max_iter=2000)
+    solve()
+    stream = torch.cuda.current_stream()
+    ms = _event_ms(solve, stream, 10, flush)
+    info = last["info"]
+    nb = int(bm.col_ind.shape[0])
+    nbr = n // 4
+    bytes_alg = 68 * nb + 4 * (nbr + 1) + 8 * n
+    xs, ys = torch.randn(n, device=dev), torch.empty(n, device=dev)
+    for _ in range(3):
+        A.mv(xs, ys)
+    mv_cold = _event_ms(lambda: A.mv(xs, ys), stream, 20, flush)
+    mv_warm = _event_ms(lambda: A.mv(xs, ys), stream, 20)
+    yo = O.spmv(O.Csr(bm.row_ptr, bm.col_ind, bm.vals, n, 4), xs.cpu().numpy().astype(np.float64))
+    Ao = O.Csr(*coo.to_csr(), n)
+    _, io = O.bicgstab(Ao, b.astype(np.float64), tol=1e-6, max_iter=2000, threads=host_threads())
+    sc = scipy_solve("bicgstab", coo, b, 1e-6, 2000)
+    return {"workload": "BCSR 4x4, 65,536 block rows, 589,824 blocks (n 262,144), shuffled COO",
+            "solver": "bicgstab (plain FP32), tol 1e-6", "ms": ms, "iters": info["iters"],
+            "oracle_fp64_iters": io["iters"], "true_resid": info["true_resid"],
+            "converged_fp64": bool(info["converged"]),
+            "bcsr_spmv": {"bytes_per_launch": bytes_alg, "ms_l2_flushed": mv_cold,
+                          "gbs_l2_flushed": bytes_alg / (mv_cold * 1e-3) / 1e9,
+                          "ms_l2_resident": mv_warm,
+                          "effective_gbs_l2_resident": bytes_alg / (mv_warm * 1e-3) / 1e9,
+                          "rel_err_vs_oracle": _rel(ys.cpu().numpy(), yo)},
+            "scipy_bicgstab_host": sc}
+
+
+def c3_leg(args, dev, ctx):
+    """C3: mixed-precision CG with FP64 refinement to 1e-10 (FP32 values,
+    reliable updates; BF16 values, restarted refinement) and plain FP32 CG to
+    1e-6 on the 256^3 operator, each judged by its FP64 true residual; the
+    error against the FP64 oracle's solution on the 64^3 member of the same
+    family (sigma 1, correlation 8), where the oracle runs in seconds."""
+    import torch
+    import mpsparse_b200 as mps
+    from oracle import oracle as O
+    W = _workloads()
+    stream = torch.cuda.current_stream()
+
+    def run(A, n, b32):
+        b64 = b32.double()
+        out = {}
+        for name, kw in (("mp_fp32_values", dict(value_bits=32)),
+                         ("mp_bf16_values", dict(value_bits=16, max_inner=20000, max_outer=200))):
+            x = torch.zeros(n, dtype=torch.float64, device=dev)
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            info = A.cg_mixed(b64, x, tol=1e-10, **kw)
+            e.record(stream)
+            torch.cuda.synchronize()
+            out[name] = ({"ms": a.elapsed_time(e), "inner_iters": info["inner_iters"],
+                          "outer_iters": info["outer_iters"], "true_resid": info["rel_resid"],
+                          "converged_fp64": bool(info["converged"])}, x)
+        x = torch.zeros(n, device=dev)
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        info = A.cgd(b32, x, tol=1e-6, max_iter=40000)
+        e.record(stream)
+        torch.cuda.synchronize()
+        out["plain_fp32_cg_1e-6"] = ({"ms": a.elapsed_time(e), "iters": info["iters"],
+                                      "true_resid": info["true_resid"],
+                                      "converged_fp64": bool(info["converged"])}, x)
+        return out
+
+    big = run(ctx.A, ctx.n, torch.from_numpy(W.rhs(ctx.n, 3)).to(dev))
+    # 64^3 member: errors against the FP64 oracle solution
+    c64 = W.lognormal_diffusion_3d(64, 1.0, 8.0, 0)
+    e0 = torch.empty(0)
+    A64 = mps.spmv.csr_tensor(torch.from_numpy(c64.keys()).to(dev), torch.from_numpy(c64.vals).to(dev),
+                              e0, e0, e0, c64.n, c64.n, fill_outputs=False)
+    b64h = W.rhs(c64.n, 3)
+    small = run(A64, c64.n, torch.from_numpy(b64h).to(dev))
+    Ao = O.Csr(*c64.to_csr(), c64.n)
+    xref, iref = O.cg(Ao, b64h.astype(np.float64), tol=1e-14, max_iter=100000, threads=host_threads())
+    errs = {k: {**v[0], "err_vs_fp64_oracle": _rel(v[1].cpu().numpy(), xref)} for k, v in small.items()}
+    return {"workload": f"{ctx.m}^3 7-pt log-normal diffusion (sigma 1, corr 8), n {ctx.n}, nnz {ctx.nnz}",
+            "solves": {k: v[0] for k, v in big.items()},
+            "member_64cubed": {"oracle": {"solver": "FP64 CG to 1e-14", "iters": iref["iters"],
+                                          "true_resid": O.true_residual(Ao, b64h.astype(np.float64), xref)},
+                               "solves": errs}}
+
+
+def configs_legs(args, dev, c3):
+    import torch
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2
+    out = {"C1": c1_leg(dev, flush), "C2": c2_leg(dev, flush)}
+    del flush
+    if c3 is not None:
+        c3.drop_coo()
+        out["C3"] = c3_leg(args, dev, c3)
+    return out
+
+
 # --------------------------------------------------------- CPU baselines ---
-def cpu_oracle_cg(seed, budget_s, threads, target_iters=None):
-    """The oracle's CG (FP64, OpenMP SpMV/dots) on one system, bounded."""
+def cpu_oracle_cg(seed, threads, max_iter=200_000):
+    """The oracle's CG (FP64, OpenMP SpMV and fused vector passes) on one
+    system, run to its own convergence at relative residual 1e-6."""
     from oracle import oracle as O
     coo, b = c4_system(seed)
     A = O.Csr(*coo.to_csr(), coo.n)
-    probe = 50
+    b = b.astype(np.float64)
     t0 = time.perf_counter()
-    O.cg(A, b, tol=1e-300, max_iter=probe, threads=threads)
-    per_it = (time.perf_counter() - t0) / probe
-    cap = max(probe, int(budget_s / per_it))
-    t0 = time.perf_counter()
-    x, info = O.cg(A, b, tol=TOL, max_iter=cap, threads=threads)
+    x, info = O.cg(A, b, tol=TOL, max_iter=max_iter, threads=threads)
     dt = time.perf_counter() - t0
-    need = info["iters"] if info["converged"] else (target_iters or info["iters"])
-    scale = need / max(info["iters"], 1)
-    return {"ms": dt * 1e3 * scale, "iters_run": info["iters"], "iters_scaled_to": need,
-            "converged_in_sample": info["converged"]}
-
-
-def scipy_cg(seed, budget_s, target_iters=None):
-    import scipy.sparse as sp
-    import scipy.sparse.linalg as spla
-    coo, b = c4_system(seed)
-    rp, ci, v = coo.to_csr()
-    A = sp.csr_matrix((v.astype(np.float64), ci, rp), shape=(coo.n, coo.n))
-    bb = b.astype(np.float64)
-    t0 = time.perf_counter()
-    spla.cg(A, bb, rtol=1e-300, atol=0.0, maxiter=50)
-    per_it = (time.perf_counter() - t0) / 50
-    cap = max(50, int(budget_s / per_it))
-    it = [0]
-    t0 = time.perf_counter()
-    spla.cg(A, bb, rtol=TOL, maxiter=cap, callback=lambda xk: it.__setitem__(0, it[0] + 1))
-    dt = time.perf_counter() - t0
-    need = target_iters if (it[0] >= cap and target_iters) else it[0]
-    return {"ms": dt * 1e3 * need / max(it[0], 1), "iters_run": it[0], "iters_scaled_to": need}
+    return {"ms": dt * 1e3, "iters": info["iters"], "converged": bool(info["converged"]),
+            "true_resid": O.true_residual(A, b, x)}
 
 
 def host_threads():
@@ -525,6 +791,50 @@ def host_threads():
         return len(os.sched_getaffinity(0))
     except Exception:
         return os.cpu_count() or 1
+
+
+# --------------------------------------------------------- reference arm ---
+def run_reference(args):
+    """Rank 0 only: the oracle port of the reference's cgd_op (FP64, all host
+    threads) on the same held-out systems as the timed steps of our arm, each
+    solved to its own convergence at 1e-6 (no iteration budget).  Warm-up
+    steps are short bounded runs (thread pool and caches), untimed."""
+    threads = host_threads()
+    for i in range(args.warmup):
+        from oracle import oracle as O
+        coo, b = c4_system(TEST_SEED0 + i)
+        O.cg(O.Csr(*coo.to_csr(), coo.n), b.astype(np.float64), tol=TOL, max_iter=100, threads=threads)
+    runs = [cpu_oracle_cg(TEST_SEED0 + args.warmup + i, threads) for i in range(args.steps)]
+    v = statistics.mean(r["ms"] for r in runs)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "solver": "plain CG (oracle port of cgd_op), FP64",
+                       "tol": TOL},
+            "step_ms": [round(r["ms"], 1) for r in runs],
+            "iters": [r["iters"] for r in runs],
+            "converged": sum(r["converged"] for r in runs),
+            "true_resid_max": max(r["true_resid"] for r in runs),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} held-out systems (the timed systems of the GPU "
+                                       "arm), each FP64 CG solve run to its own convergence at 1e-6",
+                             "host": host_info()},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def _relaunch_distributed(args):
+    """`bench.py --gpus N` started as one process: start N ranks under
+    torch.distributed.run (127.0.0.1 rendezvous) and return their status."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr=127.0.0.1", f"--master-port={port}",
+           os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
 
 
 # ------------------------------------------------------------------ main ---
@@ -538,6 +848,9 @@ def main():
     ap.add_argument("--skip-spmv", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
+    ap.add_argument("--skip-configs", action="store_true",
+                    help="leave out the C1/C2/C3 legs")
+    ap.add_argument("--skip-e2e-plain", action="store_true")
     ap.add_argument("--batch-systems", type=int, default=4096)
     ap.add_argument("--only-spmv", action="store_true",
                     help="only the 256^3 (or --c3-grid) SpMV measurement; for ncu captures")
@@ -549,43 +862,30 @@ def main():
                     help="drive iterations from the host (kernels visible to ncu launch lists)")
     ap.add_argument("--max-iter", type=int, default=MAX_ITER,
                     help="iteration cap of the solves (shortened runs for ncu launch lists)")
-    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--cpu-budget", type=float, default=20.0,
+                    help="seconds for scipy's CG beside the converged oracle run")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(_relaunch_distributed(args))
 
     if args.impl == "reference":
-        if rank != 0:
-            return
-        threads = host_threads()
-        ms = []
-        for i in range(args.steps):
-            r = cpu_oracle_cg(TEST_SEED0 + i, args.cpu_budget / max(args.steps, 1), threads)
-            ms.append(r["ms"])
-        v = statistics.mean(ms)
-        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "solver": "plain CG (oracle port of cgd_op), FP64"},
-                "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                                 "sample": f"{args.steps} systems; each CG run capped at "
-                                           f"{args.cpu_budget / max(args.steps, 1):.1f}s and scaled "
-                                           "to its iteration count to 1e-6"},
-                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
+        if rank == 0:
+            run_reference(args)
         return
 
     import torch
     if args.only_spmv:
-        print(json.dumps({"spmv": spmv_c3(args, local)}))
+        ctx = C3Context(args, local)
+        print(json.dumps({"spmv": spmv_c3(args, local, ctx)}))
         return
     if world > 1:
         import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                              device_id=torch.device("cuda", local))
     res = run_ours(args, rank, world, local)
     hbm, peak_kind = peaks()
@@ -603,14 +903,19 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         threads = host_threads()
-        target = int(res["plain_cg"]["iters_mean"])
-        o = cpu_oracle_cg(TEST_SEED0, args.cpu_budget, threads, target)
-        s = scipy_cg(TEST_SEED0, args.cpu_budget, target)
+        seed = TEST_SEED0 + args.warmup          # the first timed system
+        o = cpu_oracle_cg(seed, threads)
+        coo, b = c4_system(seed)
+        s = scipy_solve("cg", coo, b, TOL, 200_000, budget_s=args.cpu_budget)
+        if not s["converged"] and s["iters"]:
+            # a bounded run: scaled to the FP64 CG iteration count of the same
+            # system (the oracle's converged run above), flagged
+            s["ms_scaled_to_oracle_iters"] = s["ms"] * o["iters"] / s["iters"]
         cpu = {"value": o["ms"], "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"1 system (seed {TEST_SEED0}), oracle CG ran {o['iters_run']} iterations "
-                         f"scaled to {o['iters_scaled_to']}",
-               "scipy_cg": {"value": s["ms"], "unit": UNIT, "iters_run": s["iters_run"],
-                            "iters_scaled_to": s["iters_scaled_to"]}}
+               "sample": f"1 system (seed {seed}, the first timed system), oracle FP64 CG run to "
+                         f"its own convergence: {o['iters']} iterations, true residual "
+                         f"{o['true_resid']:.2e}",
+               "host": host_info(), "scipy_cg": s}
     if rank == 0:
         line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_solve"],
@@ -626,8 +931,9 @@ def main():
                 "setup_ms_first_solve": res["setup_ms_first_solve"],
                 "plain_cg": res["plain_cg"], "jacobi_pcg": res["jacobi_pcg"],
                 "speedup_vs_plain_cg": res["plain_cg"]["ms_per_solve"] / res["ms_per_solve"],
-                "spmv": spmv, "batched": res["batched"], "roofline": roof, "cpu_baseline": cpu,
-                "e2e": res["e2e"],
+                "spmv": spmv, "batched": res["batched"], "configs": res["configs"],
+                "roofline": roof, "cpu_baseline": cpu,
+                "e2e": res["e2e"], "e2e_plain_cg": res["e2e_plain_cg"],
                 "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]}
         print(json.dumps(line))
     if world > 1:

@@ -65,18 +65,25 @@ typedef struct {
 
 typedef struct {
     int32_t iters;
-    int32_t converged;
+    int32_t converged;        /* the returned x meets the target: true_resid <= tol
+                                 (reference_compat: the reference's stop rule fired) */
     int32_t breakdown;
     int32_t stalled;          /* FSAI-PCG switched to Jacobi */
     int32_t compat_snapshot;  /* reference_compat BiCGSTAB returned its last checkpoint */
-    int32_t reserved;
+    int32_t stop_rule_met;    /* the solver's own stop test on its recurrence residual
+                                 fired (the FP32 recurrence can reach tol while the
+                                 FP32 x it returns cannot: see true_resid) */
     double rel_resid;         /* recurrence residual ||r||/||b|| at exit */
+    double true_resid;        /* ||b - A x|| / ||b|| of the returned x, recomputed on the
+                                 GPU after the solve in FP64 (FP64 products and sums
+                                 over the stored FP32 matrix and x) */
 } mps_solve_info;
 
 /* Fill opts with the defaults (tol 1e-6, max_iter 2000, graphs on). */
 void mps_solve_opts_default(mps_solve_opts* opts);
 const char* mps_last_error_string(void);
 const char* mps_status_string(mps_status s);
+/* 2: mps_solve_info carries stop_rule_met and true_resid. */
 int32_t mps_abi_version(void);
 
 /* ---- COO -> CSR ------------------------------------------------------- */

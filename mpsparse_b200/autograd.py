@@ -37,7 +37,9 @@ def _solve(H, b, method, tol, max_iter, precond):
         info = H.cgd(b.float().contiguous(), x, tol=tol, max_iter=max_iter, precond=precond)
     else:
         info = H.bicgstab(b.float().contiguous(), x, tol=tol, max_iter=max_iter)
-    if not info["converged"]:
+    # the FP32 solver's own stop test; the FP64 true residual of an FP32 x can
+    # sit above tol on ill-conditioned systems (info["true_resid"])
+    if not info["stop_rule_met"]:
         raise RuntimeError(f"sparse solve did not converge ({method}, {info['iters']} iterations)")
     return x
 

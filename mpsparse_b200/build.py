@@ -53,13 +53,16 @@ def build_lib(verbose: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     os.makedirs(OBJDIR, exist_ok=True)
     hdrs = _headers()
-    objs = []
+    objs, todo = [], []
     for cu in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
         obj = os.path.join(OBJDIR, os.path.basename(cu) + ".o")
         objs.append(obj)
         if _newer(obj, [cu] + hdrs):
-            cmd = [NVCC] + NVCC_FLAGS + ["-I", os.path.join(ROOT, "include"), "-c", cu, "-o", obj]
-            r = _run(cmd)
+            todo.append([NVCC] + NVCC_FLAGS + ["-I", os.path.join(ROOT, "include"), "-c", cu, "-o", obj])
+    # translation units compile independently: one nvcc per host core
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 1))) as ex:
+        for r in ex.map(_run, todo):
             if verbose:
                 sys.stderr.write(r.stderr)
     if _newer(LIB, objs):

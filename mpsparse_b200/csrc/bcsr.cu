@@ -104,6 +104,37 @@ int grid1(uint64_t n) {
     return (int)(g < 1 ? 1 : (g > c ? c : g));
 }
 
+// *out = ||b - A x||^2 in FP64 (the true residual of a returned x): one
+// thread per scalar row, exact FP64 products of the FP32 block values and x,
+// FP64 sums, per-CTA partials summed in a fixed order by the last CTA.
+template <int B>
+__global__ void __launch_bounds__(kNT)
+bcsr_true_resid(const int* __restrict__ rp, const int* __restrict__ ci, const float* __restrict__ v,
+                int nbr, const float* __restrict__ x, const float* __restrict__ b, double* out,
+                unsigned* ctr, double* part) {
+    __shared__ double red[kNT / 32];
+    __shared__ int last;
+    double acc = 0.0;
+    const int n = nbr * B;
+    for (int row = blockIdx.x * kNT + threadIdx.x; row < n; row += gridDim.x * kNT) {
+        const int br = row / B, k = row % B;
+        double s = 0.0;
+        for (int j = rp[br]; j < rp[br + 1]; ++j) {
+            const float* a = v + (size_t)j * B * B + k * B;
+            const float* xs = x + (size_t)ci[j] * B;
+#pragma unroll
+            for (int c = 0; c < B; ++c) s += (double)a[c] * (double)xs[c];
+        }
+        const double r = (double)b[row] - s;
+        acc += r * r;
+    }
+    const double t = block_sum<kNT>(acc, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+    if (!arrive_last(ctr, &last)) return;
+    const double tot = sum_partials<kNT>(part, gridDim.x, red);
+    if (threadIdx.x == 0) *out = tot;
+}
+
 }  // namespace
 
 // BCSR operator for the shared solver driver.
@@ -112,6 +143,15 @@ struct BcsrOp {
     template <class Epi>
     cudaError_t apply(const float* x, const Epi& e, cudaStream_t s) const {
         return A->B == 8 ? bcsr_apply<8>(*A, x, e, s) : bcsr_apply<4>(*A, x, e, s);
+    }
+    cudaError_t true_resid(const float* x, const float* b, double* out, unsigned* ctr, double* part,
+                           cudaStream_t s) const {
+        const int g = grid1((uint64_t)A->nbr * A->B);
+        if (A->B == 8)
+            bcsr_true_resid<8><<<g, kNT, 0, s>>>(A->rp, A->ci, A->v, (int)A->nbr, x, b, out, ctr, part);
+        else
+            bcsr_true_resid<4><<<g, kNT, 0, s>>>(A->rp, A->ci, A->v, (int)A->nbr, x, b, out, ctr, part);
+        return cudaGetLastError();
     }
 };
 

@@ -1,4 +1,5 @@
 // capi.cu -- extern "C" entry points (include/mpsparse.h) for CSR handles.
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <cmath>
@@ -41,26 +42,29 @@ cudaMemPool_t lib_pool() {
     return pool;
 }
 
-int num_sms() {
-    static int sms = 0;
-    if (!sms) {
-        int d = 0, v = 0;
-        cudaGetDevice(&d);
-        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
-        sms = v > 0 ? v : 148;
+// Device attributes, cached per device (a process may drive several GPUs).
+static int device_attr(cudaDeviceAttr attr, std::atomic<int>* cache, int fallback) {
+    int d = 0;
+    cudaGetDevice(&d);
+    if (d >= 0 && d < kMaxDevices) {
+        const int c = cache[d].load(std::memory_order_relaxed);
+        if (c) return c;
     }
-    return sms;
+    int v = 0;
+    cudaDeviceGetAttribute(&v, attr, d);
+    if (v <= 0) v = fallback;
+    if (d >= 0 && d < kMaxDevices) cache[d].store(v, std::memory_order_relaxed);
+    return v;
+}
+
+int num_sms() {
+    static std::atomic<int> cache[kMaxDevices];
+    return device_attr(cudaDevAttrMultiProcessorCount, cache, 148);
 }
 
 size_t l2_bytes() {
-    static size_t l2 = 0;
-    if (!l2) {
-        int d = 0, v = 0;
-        cudaGetDevice(&d);
-        cudaDeviceGetAttribute(&v, cudaDevAttrL2CacheSize, d);
-        l2 = v > 0 ? (size_t)v : ((size_t)126 << 20);
-    }
-    return l2;
+    static std::atomic<int> cache[kMaxDevices];
+    return (size_t)device_attr(cudaDevAttrL2CacheSize, cache, 126 << 20);
 }
 
 mps_status device_error(unsigned err, const char* what) {
@@ -124,7 +128,7 @@ mps_status build_from_keys(CsrMat& m, const uint64_t* keys, const uint32_t* payl
 
 extern "C" {
 
-int32_t mps_abi_version(void) { return 1; }
+int32_t mps_abi_version(void) { return 2; }
 
 void mps_solve_opts_default(mps_solve_opts* o) {
     if (!o) return;

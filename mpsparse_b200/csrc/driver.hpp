@@ -76,6 +76,17 @@ struct CsrOp {
         }
         return cudaGetLastError();
     }
+    // *out = ||b - A x||^2 in FP64 (the true residual of a returned x; the
+    // FP32 values, never the BF16 copy).
+    cudaError_t true_resid(const float* x, const float* b, double* out, unsigned* ctr, double* part,
+                           cudaStream_t s) const {
+        const CsrDev view = A->view();
+        const size_t smem = spmv_smem_bytes<double>(view);
+        smem_optin_k(spmv_tiles<float, double, false, EpiTrueResid>, smem);
+        spmv_tiles<float, double, false, EpiTrueResid><<<A->plan.grid, kNT, smem, s>>>(
+            view, x, EpiTrueResid{b, out, ctr, part});
+        return cudaGetLastError();
+    }
     template <bool BF16, int NB, class Epi>
     static void launch(const CsrStreamDev& v, const float* x, const Epi& e, cudaStream_t s) {
         const size_t smem = NB * stream_buf_bytes<BF16>(v.cap, v.rcap);
@@ -609,17 +620,27 @@ inline cudaError_t build_graph_nested(const CsrOp& op, const PrecondOps<CsrOp>& 
 // Reliable-update mode (CG on a CSR only): d_b64 -> d_x64 in FP64, d_b/d_x
 // unused; *replaced receives the number of residual replacements.
 // The outcome of a solve from the scalars read back into H.ws.h_sc.
-inline mps_status solve_report(SolverKind kind, const SolverHost& H, mps_solve_info* info, int* replaced) {
+// have_true: the solve ended with the FP64 true residual of its x (r.true_rr),
+// which then decides `converged` (outside reference_compat); otherwise (the
+// inner solve of a refinement) `converged` is the stop rule and true_resid -1.
+inline mps_status solve_report(SolverKind kind, const SolverHost& H, mps_solve_info* info, int* replaced,
+                               bool have_true = false) {
     const DevScalars& r = *H.ws.h_sc;
     if (info) {
         info->iters = r.iter;
-        info->converged = r.converged;
+        info->stop_rule_met = r.converged;
         info->breakdown = r.breakdown;
         info->stalled = r.stalled;
         info->compat_snapshot = r.snapshot;
-        info->reserved = 0;
         const double num = kind == kCG ? r.rr : r.rnorm2;
         info->rel_resid = r.bnorm2 > 0 ? sqrt(num / r.bnorm2) : sqrt(num);
+        if (have_true) {
+            info->true_resid = r.bnorm2 > 0 ? sqrt(r.true_rr / r.bnorm2) : sqrt(r.true_rr);
+            info->converged = r.compat ? r.converged : (r.err == 0 && r.true_rr <= r.tol2);
+        } else {
+            info->true_resid = -1.0;
+            info->converged = r.converged;
+        }
     }
     if (replaced) *replaced = r.replaced;
     if (r.err & kErrNotFinite) return fail(MPS_ERR_NOT_FINITE, "right-hand side holds NaN or Inf");
@@ -700,11 +721,13 @@ mps_status run_solve(SolverKind kind, const Op& op, const PrecondOps<Op>& pc, So
                  static_cast<const float*>(H.v(vXAlt)), H.v(vXAlt), d_x, H.n,
                  kind == kRich ? kResRich : kResX, static_cast<const DevScalars*>(H.ws.sc));
         MPS_CUDA(cudaGetLastError());
+        // the FP64 true residual of the x just returned (one SpMV pass)
+        MPS_CUDA(op.true_resid(d_x, H.v(vB), &H.ws.sc->true_rr, H.ws.counters + 11, H.ws.partials, s));
     }
     MPS_CUDA(cudaMemcpyAsync(H.ws.h_sc, H.ws.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
     if (defer) return MPS_OK;
     MPS_CUDA(cudaStreamSynchronize(s));
-    return solve_report(kind, H, info, replaced);
+    return solve_report(kind, H, info, replaced, !ir);
 }
 
 }  // namespace mps

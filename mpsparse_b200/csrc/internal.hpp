@@ -45,6 +45,7 @@ struct DevScalars {
     double bnorm2, tol2, staged, best_rr;
     double omega_rich;
     double rz_jac;      // r . D^-1 r of the last update (Jacobi fallback)
+    double true_rr;     // ||b - A x||^2 of the returned x in FP64 (after the solve)
     // control
     int iter, max_iter, done, converged, breakdown, stalled, snapshot, compat;
     int mode;           // preconditioner in force: 0 none, 1 Jacobi, 2 FSAI
@@ -123,6 +124,7 @@ struct VecGeom {
 
 constexpr int kNT = 256;           // threads per CTA of the solver kernels
 constexpr int kMaxPartials = 4096; // FP64 partial slots per reduction
+constexpr int kMaxDevices = 64;    // per-device host caches (device ordinals below this)
 
 // Solver workspace owned by a handle (lazily allocated, padded to x4 floats).
 struct Workspace {

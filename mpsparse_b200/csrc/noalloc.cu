@@ -37,8 +37,7 @@ struct NoAllocScratch {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
 
 std::mutex g_mu;
-constexpr int kMaxDevices = 64;
-NoAllocScratch* g_addr[kMaxDevices] = {};
+NoAllocScratch* g_addr[mps::kMaxDevices] = {};
 
 // Device address of the scratch on the current device, looked up once per
 // device (with that device current).
@@ -46,7 +45,7 @@ cudaError_t scratch_address(NoAllocScratch** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    if (dev < 0 || dev >= mps::kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_addr[dev]) {
         void* p = nullptr;

@@ -16,6 +16,7 @@
 //     col_ind (low bits) instead of keys, so no separate compress kernel;
 //   * row_ptr is an exclusive scan of the row counts, so empty rows need no
 //     fixer pass.
+#include <atomic>
 #include "common.cuh"
 #include "internal.hpp"
 
@@ -359,13 +360,17 @@ cudaError_t sort_to_csr(const uint64_t* keys, const uint32_t* payload, uint64_t 
                                                 hist, rows, d_err);
         sort_digit_bases<<<1, 256, 0, s>>>(hist, base, passes);
         const size_t smem = sizeof(SortSmem);
-        static bool attr_done = false;
-        if (!attr_done) {
+        // the shared-memory opt-in is a per-device function attribute
+        static std::atomic<unsigned long long> attr_done{0};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        const unsigned long long bit = dev >= 0 && dev < 64 ? 1ull << dev : 0ull;
+        if (!bit || !(attr_done.load() & bit)) {
             cudaFuncSetAttribute(sort_onesweep<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             cudaFuncSetAttribute(sort_onesweep<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             cudaFuncSetAttribute(sort_onesweep<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             cudaFuncSetAttribute(sort_onesweep<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            attr_done = true;
+            attr_done.fetch_or(bit);
         }
         const unsigned long long* kin = (const unsigned long long*)keys;
         const unsigned* vin = payload;

@@ -2,6 +2,7 @@
 #include <atomic>
 #include <cstdlib>
 #include <map>
+#include <tuple>
 #include <mutex>
 
 #include "driver.hpp"
@@ -221,9 +222,11 @@ bool pdl_suspend(bool off) {
 
 int resident_ctas(const void* kernel, int threads, size_t smem) {
     static std::mutex mu;
-    static std::map<std::pair<const void*, size_t>, int> cache;
+    static std::map<std::tuple<int, const void*, size_t>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lock(mu);
-    auto key = std::make_pair(kernel, smem);
+    auto key = std::make_tuple(dev, kernel, smem);
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
     int n = 0;

@@ -246,6 +246,25 @@ struct EpiStoreDot {   // y = A x ; *out = w . y
     __device__ void finalize(const double* tot) const { *out = tot[0]; }
 };
 
+// ||b - A x||^2 in FP64 for an FP32 x: the products of the FP32 values and
+// x are exact in FP64 and summed in FP64 (used with ST = double), so this is
+// the true residual of the x a solve returns, not its FP32 recurrence.
+struct EpiTrueResid {
+    static constexpr int NS = 1;
+    const float* b;
+    double* out;
+    unsigned* counter;
+    double* partials;
+    __device__ bool active() const { return true; }
+    __device__ void tick() const {}
+    __device__ void on_skip() const {}
+    __device__ void row(int r, double s, double* acc) const {
+        const double rv = (double)b[r] - s;
+        acc[0] += rv * rv;
+    }
+    __device__ void finalize(const double* tot) const { *out = tot[0]; }
+};
+
 // Shared-memory bytes for a tile loop.
 template <typename ST>
 inline size_t spmv_smem_bytes(const CsrDev& A) { return (size_t)A.cap * sizeof(ST); }

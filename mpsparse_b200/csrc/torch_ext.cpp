@@ -49,6 +49,8 @@ py::dict info_dict(const mps_solve_info& i) {
     d["stalled"] = (bool)i.stalled;
     d["compat_snapshot"] = (bool)i.compat_snapshot;
     d["rel_resid"] = i.rel_resid;
+    d["stop_rule_met"] = (bool)i.stop_rule_met;
+    d["true_resid"] = i.true_resid;
     return d;
 }
 

@@ -38,29 +38,33 @@ def local_rows(row_off, systems):
     return loc
 
 
-def gather_records(values, systems, n_systems: int, group=None):
+def gather_records(values, systems, n_systems: int, group=None, device=None):
     """All ranks' per-system values (one per local system) merged into one
-    array indexed by global system id, on every rank."""
+    array indexed by global system id, on every rank.  device: where the
+    exchanged tensors live (a CUDA device for the NCCL backend, None = CPU
+    for gloo)."""
     import torch
     import torch.distributed as dist
 
     values = np.asarray(values, np.float64)
     systems = np.asarray(systems, np.int64)
     world = dist.get_world_size(group)
-    cnt = torch.tensor([systems.shape[0]], dtype=torch.int64)
-    counts = [torch.zeros(1, dtype=torch.int64) for _ in range(world)]
+    cnt = torch.tensor([systems.shape[0]], dtype=torch.int64, device=device)
+    counts = [torch.zeros(1, dtype=torch.int64, device=device) for _ in range(world)]
     dist.all_gather(counts, cnt, group=group)
     m = max(1, int(max(c.item() for c in counts)))
     pad_i = torch.full((m,), -1, dtype=torch.int64)
     pad_v = torch.zeros(m, dtype=torch.float64)
     pad_i[: systems.shape[0]] = torch.from_numpy(systems)
     pad_v[: systems.shape[0]] = torch.from_numpy(values)
-    all_i = [torch.empty(m, dtype=torch.int64) for _ in range(world)]
-    all_v = [torch.empty(m, dtype=torch.float64) for _ in range(world)]
+    pad_i, pad_v = pad_i.to(device), pad_v.to(device)
+    all_i = [torch.empty(m, dtype=torch.int64, device=device) for _ in range(world)]
+    all_v = [torch.empty(m, dtype=torch.float64, device=device) for _ in range(world)]
     dist.all_gather(all_i, pad_i, group=group)
     dist.all_gather(all_v, pad_v, group=group)
     out = np.full(n_systems, np.nan)
     for i, v in zip(all_i, all_v):
+        i, v = i.cpu(), v.cpu()
         keep = i >= 0
         out[i[keep].numpy()] = v[keep].numpy()
     return out

@@ -294,30 +294,52 @@ def graph_laplacian_torch(n: int, mean_degree: float, seed: int, shift: float = 
     return (rows << 32) | cols, vals, n
 
 
+def batch_plan(n_systems: int, seed: int, n_min: int = 1024, n_max: int = 65536,
+               mean_degree: float = 8.0):
+    """Shapes of the systems batch_systems makes, without making them:
+    (kind per system: 0 grid / 1 graph, grid (nx, ny) or graph row count,
+    estimated nonzeros per system) -- what a rank needs to pick its share."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(n_min), np.log(n_max), n_systems))
+    kinds = np.arange(n_systems) % 2
+    shapes, nnz = [], np.empty(n_systems, np.int64)
+    for s, target in enumerate(sizes):
+        if kinds[s] == 0:
+            nx = max(2, int(round(np.sqrt(target))))
+            ny = max(2, int(round(target / nx)))
+            shapes.append((nx, ny))
+            nnz[s] = 5 * nx * ny - 2 * nx - 2 * ny
+        else:
+            n = int(round(target))
+            shapes.append(n)
+            nnz[s] = int(n * (1 + mean_degree))
+    return kinds.astype(np.int8), shapes, nnz
+
+
 def batch_systems(n_systems: int, seed: int, n_min: int = 1024, n_max: int = 65536,
                   grid_sigma: float = 1.0, grid_corr: float = 8.0, mean_degree: float = 8.0,
-                  device="cuda"):
+                  device="cuda", select=None):
     """Independent SPD systems with row counts log-uniform in [n_min, n_max]:
     even indices are 2D 5-point log-normal diffusion grids (near-square),
     odd indices random graph Laplacians + 1e-2 I.  Returns the stacked
     (keys, values) on ``device`` with global indices, row offsets (numpy) and
-    the kind of every system (0 grid, 1 graph)."""
+    the kind of every system (0 grid, 1 graph).  ``select``: only these
+    system indices, stacked in the order given (each system comes from its
+    own seed, so a subset is the same systems as in the whole batch)."""
     import torch
 
-    rng = np.random.default_rng(seed)
-    sizes = np.exp(rng.uniform(np.log(n_min), np.log(n_max), n_systems))
+    kinds_all, shapes, _ = batch_plan(n_systems, seed, n_min, n_max, mean_degree)
+    idx = range(n_systems) if select is None else [int(i) for i in select]
     keys, vals, off, kinds = [], [], [0], []
-    for s, target in enumerate(sizes):
-        if s % 2 == 0:
-            nx = max(2, int(round(np.sqrt(target))))
-            ny = max(2, int(round(target / nx)))
+    for s in idx:
+        if kinds_all[s] == 0:
+            nx, ny = shapes[s]
             k, v, n = lognormal_diffusion_2d_torch(nx, ny, grid_sigma, grid_corr,
                                                    seed * 1_000_003 + s, device)
-            kinds.append(0)
         else:
-            k, v, n = graph_laplacian_torch(int(round(target)), mean_degree,
-                                            seed * 1_000_003 + s, device=device)
-            kinds.append(1)
+            k, v, n = graph_laplacian_torch(shapes[s], mean_degree, seed * 1_000_003 + s,
+                                            device=device)
+        kinds.append(int(kinds_all[s]))
         base = off[-1]
         keys.append(k + ((base << 32) | base))
         vals.append(v)

@@ -159,6 +159,86 @@ static double dot(const double* a, const double* b, int64_t n, int threads) {
     return s;
 }
 
+/* Row chunk c of t (the chunks dot() sums in order). */
+static void chunk_of(int64_t n, int t, int c, int64_t* lo, int64_t* hi) {
+    int64_t chunk = (n + t - 1) / t;
+    *lo = (int64_t)c * chunk;
+    *hi = *lo + chunk < n ? *lo + chunk : n;
+    if (*lo > n) *lo = n;
+}
+
+/* q = A p (CSR) and p.q with the chunking and order of dot(): the same
+ * numbers as orc_csr_spmv followed by dot(p, q), in one parallel pass. */
+static double spmv_dot(const orc_op* A, const double* p, double* q, int threads) {
+    int t = threads > 0 ? threads : 1;
+    if (t > 256) t = 256;
+    double part[256] = {0};
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static, 1) num_threads(t)
+#endif
+    for (int c = 0; c < t; ++c) {
+        int64_t lo, hi;
+        chunk_of(A->n, t, c, &lo, &hi);
+        double s = 0.0;
+        for (int64_t i = lo; i < hi; ++i) {
+            double y = 0.0;
+            for (int32_t k = A->row_ptr[i]; k < A->row_ptr[i + 1]; ++k)
+                y += (double)A->val[k] * p[A->col_ind[k]];
+            q[i] = y;
+            s += p[i] * y;
+        }
+        part[c] = s;
+    }
+    double s = 0.0;
+    for (int c = 0; c < t; ++c) s += part[c];
+    return s;
+}
+
+/* x += alpha p, r -= alpha q, then r.r and (Jacobi) z = D^-1 r, r.z, in one
+ * parallel pass with dot()'s chunking and order. */
+static void update_xr(double* x, double* r, double* z, const double* p, const double* q,
+                      const double* dinv, double alpha, int64_t n, int threads, double* rr,
+                      double* rz) {
+    int t = threads > 0 ? threads : 1;
+    if (t > 256) t = 256;
+    double prr[256] = {0}, prz[256] = {0};
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static, 1) num_threads(t)
+#endif
+    for (int c = 0; c < t; ++c) {
+        int64_t lo, hi;
+        chunk_of(n, t, c, &lo, &hi);
+        double s = 0.0, sz = 0.0;
+        for (int64_t k = lo; k < hi; ++k) {
+            x[k] += alpha * p[k];
+            r[k] -= alpha * q[k];
+            s += r[k] * r[k];
+            if (dinv) {
+                z[k] = dinv[k] * r[k];
+                sz += r[k] * z[k];
+            }
+        }
+        prr[c] = s;
+        prz[c] = sz;
+    }
+    double s = 0.0, sz = 0.0;
+    for (int c = 0; c < t; ++c) {
+        s += prr[c];
+        sz += prz[c];
+    }
+    *rr = s;
+    *rz = dinv ? sz : s;
+}
+
+/* p = zz + beta p */
+static void axpby_p(double* p, const double* zz, double beta, int64_t n, int threads) {
+    int t = threads > 0 ? threads : 1;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(t)
+#endif
+    for (int64_t k = 0; k < n; ++k) p[k] = zz[k] + beta * p[k];
+}
+
 static void diag_of(const orc_op* A, double* d) {
     for (int64_t i = 0; i < A->n; ++i) d[i] = 0.0;
     if (A->block == 0) {
@@ -232,8 +312,13 @@ int orc_cg(const orc_op* A, const double* b, double* x, const orc_opts* o, orc_i
         goto done;
     }
     for (int i = 0; i < cap; ++i) {
-        apply(A, p, q, th);
-        double pq = dot(p, q, n, th);
+        double pq;
+        if (A->block == 0) {
+            pq = spmv_dot(A, p, q, th);               /* q = A p and p.q, one pass */
+        } else {
+            apply(A, p, q, th);
+            pq = dot(p, q, n, th);
+        }
         double alpha;
         if (o->compat) {
             alpha = fabs(pq) > 1e-9 ? rz / pq : 0.0;
@@ -241,19 +326,11 @@ int orc_cg(const orc_op* A, const double* b, double* x, const orc_opts* o, orc_i
             if (!(pq > 0.0)) { info->breakdown = 1; break; }
             alpha = rz / pq;
         }
-        for (int64_t k = 0; k < n; ++k) {
-            x[k] += alpha * p[k];
-            r[k] -= alpha * q[k];
-        }
-        double rr_new = dot(r, r, n, th);
-        double rz_new = rr_new;
-        if (dinv) {
-            for (int64_t k = 0; k < n; ++k) z[k] = dinv[k] * r[k];
-            rz_new = dot(r, z, n, th);
-        }
+        double rr_new, rz_new;
+        update_xr(x, r, z, p, q, dinv, alpha, n, th, &rr_new, &rz_new);
         double beta = rz_new / rz;
         const double* zz = dinv ? z : r;
-        for (int64_t k = 0; k < n; ++k) p[k] = zz[k] + beta * p[k];
+        axpby_p(p, zz, beta, n, th);
         info->iters = i + 1;
         if (o->compat) {
             if (i % 50 == 0 && rr < 1e-5) { rr = rr_new; info->converged = 1; break; }

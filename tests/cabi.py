@@ -18,8 +18,8 @@ class SolveOpts(C.Structure):
 
 class SolveInfo(C.Structure):
     _fields_ = [("iters", C.c_int32), ("converged", C.c_int32), ("breakdown", C.c_int32),
-                ("stalled", C.c_int32), ("compat_snapshot", C.c_int32), ("reserved", C.c_int32),
-                ("rel_resid", C.c_double)]
+                ("stalled", C.c_int32), ("compat_snapshot", C.c_int32), ("stop_rule_met", C.c_int32),
+                ("rel_resid", C.c_double), ("true_resid", C.c_double)]
 
 
 def declared_symbols():

@@ -54,8 +54,8 @@ def test_cg_converges_true_residual(mps, oracle, c1):
     x = torch.zeros(c1.n)
     info = A.cgd(torch.from_numpy(b), x, tol=1e-6, max_iter=2000)   # CPU tensors: drop-in path
     _, io = oracle.cg(Ao, b, tol=1e-6, max_iter=2000)
-    assert info["converged"] and abs(info["iters"] - io["iters"]) <= 5
-    assert_solved_fp32(oracle, Ao, b, x.numpy(), 1e-6)
+    assert info["stop_rule_met"] and abs(info["iters"] - io["iters"]) <= 5
+    assert_solved_fp32(oracle, Ao, b, x.numpy(), 1e-6, info)
 
 
 def test_cg_graph_host_loop_and_reruns_bitwise(mps, c1):
@@ -95,8 +95,8 @@ def test_jacobi_pcg_iterates(mps, oracle):
     x = torch.zeros(c.n, device="cuda")
     info = A.cgd(bt, x, tol=1e-6, max_iter=5000, precond="jacobi")
     info0 = A.cgd(bt, torch.zeros(c.n, device="cuda"), tol=1e-6, max_iter=5000)
-    assert info["converged"] and info["iters"] < info0["iters"]
-    assert_solved_fp32(oracle, Ao, b, x.cpu().numpy(), 1e-6)
+    assert info["stop_rule_met"] and info["iters"] < info0["iters"]
+    assert_solved_fp32(oracle, Ao, b, x.cpu().numpy(), 1e-6, info)
 
 
 def test_bicgstab_iterates(mps, oracle):
@@ -113,8 +113,8 @@ def test_bicgstab_iterates(mps, oracle):
         assert _rel(x.cpu().numpy().astype(np.float64), xo) <= ITERATE_RTOL, k
     x = torch.zeros(c.n, device="cuda")
     info = A.bicgstab(bt, x, tol=1e-6)
-    assert info["converged"]
-    assert_solved_fp32(oracle, Ao, b, x.cpu().numpy(), 1e-6)
+    assert info["stop_rule_met"]
+    assert_solved_fp32(oracle, Ao, b, x.cpu().numpy(), 1e-6, info)
 
 
 def test_bicgstab_golden_scipy(mps, golden):
@@ -178,6 +178,7 @@ def test_edge_cases(mps, c1):
     x = torch.ones(c1.n, device="cuda")
     info = A.cgd(torch.zeros(c1.n, device="cuda"), x)
     assert info["converged"] and info["iters"] == 0 and float(x.abs().max()) == 0.0
+    assert info["true_resid"] == 0.0
     b = torch.ones(c1.n, device="cuda")
     b[17] = float("nan")
     with pytest.raises(RuntimeError, match="non-finite"):

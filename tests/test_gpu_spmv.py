@@ -145,5 +145,5 @@ def test_autotune_then_solve(mps, oracle):
     assert 256 <= choice["tile_nnz"] <= 8192 and choice["spmv_us"] > 0
     x.zero_()
     info = A.cgd(torch.from_numpy(b).float().cuda(), x, tol=1e-6, max_iter=5000)
-    assert info["converged"]
-    assert_solved_fp32(oracle, oracle.Csr(rp, ci, cv, c.n), b, x.cpu().numpy(), 1e-6)
+    assert info["stop_rule_met"]
+    assert_solved_fp32(oracle, oracle.Csr(rp, ci, cv, c.n), b, x.cpu().numpy(), 1e-6, info)

@@ -63,3 +63,54 @@ def test_gather_over_two_gloo_ranks():
     for rank, merged, t in out:
         assert np.allclose(merged, np.arange(37) * 10.0 + 0.5)
         assert t == 2.0
+
+
+def _batch_worker(rank, world, port, q):
+    """The batched leg's sharding path on CPU: each rank builds only its
+    nnz-balanced share of a generated batch and the per-system records are
+    gathered back into global system order."""
+    import torch.distributed as dist
+    from mpsparse_b200 import workloads as W
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        n_sys, seed = 12, 5
+        _, _, est = W.batch_plan(n_sys, seed, n_min=64, n_max=400)
+        mine = shard.partition_by_nnz(est, world)[rank]
+        keys, vals, off, kinds = W.batch_systems(n_sys, seed, n_min=64, n_max=400, device="cpu",
+                                                 select=mine)
+        rows = np.diff(off).astype(np.float64)
+        nnz = np.array([((keys >> 32) >= off[k]).logical_and((keys >> 32) < off[k + 1]).sum().item()
+                        for k in range(len(mine))], np.float64)
+        merged_rows = shard.gather_records(rows, mine, n_sys)
+        merged_nnz = shard.gather_records(nnz, mine, n_sys)
+        q.put((rank, merged_rows.tolist(), merged_nnz.tolist(), kinds.tolist(), mine.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_batched_shards_over_two_gloo_ranks():
+    from mpsparse_b200 import workloads as W
+    n_sys, seed = 12, 5
+    keys, vals, off, kinds = W.batch_systems(n_sys, seed, n_min=64, n_max=400, device="cpu")
+    rows = np.diff(off)
+    rk = (keys >> 32).numpy()
+    nnz = np.array([((rk >= off[k]) & (rk < off[k + 1])).sum() for k in range(n_sys)])
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_batch_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=180) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    shares = []
+    for rank, mrows, mnnz, k_local, mine in out:
+        assert np.array_equal(np.array(mrows), rows)          # same systems as the whole batch
+        assert np.array_equal(np.array(mnnz), nnz)
+        assert np.array_equal(np.array(k_local), kinds[mine])
+        shares.append(mine)
+    assert sorted(shares[0] + shares[1]) == list(range(n_sys))
