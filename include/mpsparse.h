@@ -149,7 +149,9 @@ mps_status mps_csr_spmv_dot(const mps_csr* A, const float* d_x, const float* d_w
  * Takes the CSR arrays and vectors as device pointers and allocates nothing:
  * its scratch (tile plan, FP64 partial sums, counter) is one file-scope device
  * array of about 280 KB that every GPU loading this library holds until exit.
- * Limit: nnz <= 33,554,432; larger matrices return MPS_ERR_ARG.  The first call
+ * Limit: nnz <= 33,554,432; larger matrices return MPS_ERR_ARG.  d_col_ind and
+ * d_vals must be 16-byte aligned (they are read 16 bytes at a time; a
+ * cudaMalloc'd buffer is), else MPS_ERR_ARG.  The first call
  * on a device looks up the scratch's device address (cudaGetSymbolAddress), so
  * make that first call before any stream capture.  All calls share the one
  * scratch array: calls that overlap on the GPU (other streams, other threads)

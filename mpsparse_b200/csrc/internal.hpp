@@ -125,6 +125,7 @@ struct VecGeom {
 constexpr int kNT = 256;           // threads per CTA of the solver kernels
 constexpr int kMaxPartials = 4096; // FP64 partial slots per reduction
 constexpr int kMaxDevices = 64;    // per-device host caches (device ordinals below this)
+constexpr int kMinTileNnz = 512;   // smallest default SpMV tile (nonzeros); sizes static tile plans
 
 // Solver workspace owned by a handle (lazily allocated, padded to x4 floats).
 struct Workspace {

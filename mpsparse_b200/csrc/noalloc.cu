@@ -23,8 +23,10 @@ namespace {
 
 constexpr int kNoAllocMaxTiles = 65536;
 constexpr int kNoAllocMaxGrid = 2048;
-// Tiles hold at least 512 nonzeros, so this many nonzeros fit the tile plan.
-constexpr unsigned long long kNoAllocMaxNnz = (unsigned long long)kNoAllocMaxTiles * 512;
+// Default tiles hold at least kMinTileNnz nonzeros (default_tile_nnz), so
+// this many nonzeros fit the static tile plan.
+constexpr unsigned long long kNoAllocMaxNnz = (unsigned long long)kNoAllocMaxTiles * mps::kMinTileNnz;
+static_assert(kNoAllocMaxNnz == 33554432ull, "the documented limit of mps_csr_spmv_dot_noalloc");
 
 struct NoAllocScratch {
     double partials[kNoAllocMaxGrid];
@@ -70,6 +72,9 @@ extern "C" mps_status mps_csr_spmv_dot_noalloc(const int32_t* d_row_ptr, const i
         return fail(MPS_ERR_ARG, "spmv_dot_noalloc: null pointer");
     if (n_rows == 0 || n_cols == 0 || n_rows >= 0x7fffffffu)
         return fail(MPS_ERR_ARG, "spmv_dot_noalloc: num_rows / num_cols must be in [1, 2^31 - 1)");
+    // the tile loads read col_ind and values 16 bytes at a time
+    if (nnz && ((reinterpret_cast<uintptr_t>(d_col_ind) | reinterpret_cast<uintptr_t>(d_vals)) & 15))
+        return fail(MPS_ERR_ARG, "spmv_dot_noalloc: d_col_ind and d_vals must be 16-byte aligned");
     if (nnz > kNoAllocMaxNnz)
         return fail(MPS_ERR_ARG, "spmv_dot_noalloc: nnz " + std::to_string(nnz) +
                                      " exceeds the allocation-free limit of " +

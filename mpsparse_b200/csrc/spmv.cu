@@ -101,7 +101,7 @@ int default_tile_nnz(uint64_t nnz, uint32_t n_rows) {
     const double avg = n_rows ? (double)nnz / n_rows : 1.0;
     int t = (int)(kNT * (avg < 1.0 ? 1.0 : avg + 0.999));
     t = (t + 3) & ~3;
-    if (t < 512) t = 512;
+    if (t < kMinTileNnz) t = kMinTileNnz;
     if (t > 4096) t = 4096;
     return t;
 }

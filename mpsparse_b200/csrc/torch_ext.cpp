@@ -166,6 +166,17 @@ public:
               "set_plan");
     }
 
+    // The matrix as a torch sparse CSR tensor (int32 indices, FP32 values)
+    // on the handle's device: torch's own sparse ops (matmul, to_dense,
+    // autograd through torch) work on it directly.
+    torch::Tensor sparse_csr() {
+        auto t = export_csr();
+        c10::cuda::CUDAGuard g(device_);
+        return torch::sparse_csr_tensor(std::get<0>(t), std::get<1>(t), std::get<2>(t),
+                                        {n_rows_, n_cols_},
+                                        torch::TensorOptions().dtype(torch::kFloat32)
+                                            .device(torch::kCUDA, device_));
+    }
     std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> export_csr() {
         c10::cuda::CUDAGuard g(device_);
         auto opt = torch::TensorOptions().device(torch::kCUDA, device_);
@@ -491,6 +502,16 @@ public:
         return info_dict(info);
     }
 
+    // The matrix as a torch sparse BSR tensor (blocks B x B, row-major) of the
+    // padded size on the handle's device.
+    torch::Tensor sparse_bsr() {
+        auto t = export_bcsr();
+        c10::cuda::CUDAGuard g(device_);
+        auto vals = std::get<2>(t).view({-1, block_, block_});
+        return torch::sparse_bsr_tensor(std::get<0>(t), std::get<1>(t), vals, {padded_, padded_},
+                                        torch::TensorOptions().dtype(torch::kFloat32)
+                                            .device(torch::kCUDA, device_));
+    }
     std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> export_bcsr() {
         c10::cuda::CUDAGuard g(device_);
         uint32_t nbr, blk, pn;
@@ -681,6 +702,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         .def("fsai_g_values", &CsrTensor::fsai_g_values)
         .def("fsai_probe_grad", &CsrTensor::fsai_probe_grad, py::arg("V"))
         .def("csr", &CsrTensor::export_csr)
+        .def("sparse_csr", &CsrTensor::sparse_csr, "the matrix as a torch.sparse_csr_tensor")
         .def("set_plan", &CsrTensor::set_plan, py::arg("tile_nnz") = 0, py::arg("stages") = 0,
              py::arg("evict_first") = -1)
         .def("autotune", &CsrTensor::autotune,
@@ -728,6 +750,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
              py::arg("b"), py::arg("x"), py::arg("tol") = 1e-6, py::arg("max_iter") = 2000,
              py::arg("reference_compat") = false, py::arg("host_loop") = false)
         .def("bcsr", &BcsrTensor::export_bcsr)
+        .def("sparse_bsr", &BcsrTensor::sparse_bsr, "the padded matrix as a torch.sparse_bsr_tensor")
         .def_property_readonly("padded_rows", &BcsrTensor::padded_rows)
         .def_property_readonly("num_rows", &BcsrTensor::num_rows)
         .def_property_readonly("num_cols", &BcsrTensor::num_cols)

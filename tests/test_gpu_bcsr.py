@@ -81,3 +81,21 @@ def test_unpadded_and_solvers(mps, oracle):
     A2o = oracle.Csr(*spd.to_csr(), spd.n)
     assert info["stop_rule_met"]
     assert_solved_fp32(oracle, A2o, b2, x2.numpy(), 1e-6, info)
+
+
+def test_sparse_bsr_export(mps):
+    """bcsr_tensor.sparse_bsr(): the padded BCSR as a torch.sparse_bsr_tensor
+    (row-major B x B blocks) equal to the handle's arrays."""
+    bm = W.block_dominant(300, 5, seed=4)
+    c = bm.to_coo(drop_zeros=True).shuffled(5)
+    ei = torch.empty(0, dtype=torch.int32)
+    A = mps.bcsr.bcsr_tensor(torch.from_numpy(c.keys()), torch.from_numpy(c.vals), ei, ei, c.n, c.n, 4)
+    S = A.sparse_bsr()
+    assert S.layout == torch.sparse_bsr and tuple(S.shape) == (A.padded_rows, A.padded_rows)
+    rp, ci, v = A.bcsr()
+    assert torch.equal(S.crow_indices(), rp) and torch.equal(S.col_indices(), ci)
+    assert torch.equal(S.values().reshape(-1), v)
+    dense = torch.zeros(c.n, c.n, dtype=torch.float64)
+    dense.index_put_((torch.from_numpy(c.rows), torch.from_numpy(c.cols)),
+                     torch.from_numpy(c.vals).double(), accumulate=True)
+    assert torch.equal(S.to_dense().cpu().double(), dense)

@@ -147,3 +147,23 @@ def test_autotune_then_solve(mps, oracle):
     info = A.cgd(torch.from_numpy(b).float().cuda(), x, tol=1e-6, max_iter=5000)
     assert info["stop_rule_met"]
     assert_solved_fp32(oracle, oracle.Csr(rp, ci, cv, c.n), b, x.cpu().numpy(), 1e-6, info)
+
+
+def test_sparse_csr_export(mps, oracle):
+    """csr_tensor.sparse_csr(): the sorted matrix as a torch.sparse_csr_tensor
+    whose arrays equal the handle's CSR and whose product matches A.mv."""
+    from mpsparse_b200 import workloads as W
+    c = W.lognormal_diffusion_2d(96, 80, 1.0, 6.0, 2).shuffled(3)
+    e = torch.empty(0)
+    A = mps.spmv.csr_tensor(torch.from_numpy(c.keys()), torch.from_numpy(c.vals), e, e, e, c.n, c.n)
+    S = A.sparse_csr()
+    assert S.layout == torch.sparse_csr and S.is_cuda and tuple(S.shape) == (c.n, c.n)
+    rp, ci, cv = A.csr()
+    assert torch.equal(S.crow_indices(), rp) and torch.equal(S.col_indices(), ci)
+    assert torch.equal(S.values(), cv)
+    orp, oci, ocv = oracle.coo_to_csr(c.keys(), c.vals, c.n, c.n)
+    assert np.array_equal(rp.cpu().numpy(), orp) and np.array_equal(ci.cpu().numpy(), oci)
+    x = torch.randn(c.n, device="cuda")
+    y = torch.empty(c.n, device="cuda")
+    A.mv(x, y)
+    assert torch.allclose(S @ x, y, rtol=1e-5, atol=1e-5)

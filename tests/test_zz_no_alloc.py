@@ -28,9 +28,35 @@ def _noalloc():
     return L, f
 
 
-def test_noalloc_matches_regular_entry_point(mps):
+def _dense_rows_coo():
+    """Short rows plus a few long ones: a row of 1,500 nonzeros inside a
+    staged tile (its tile averages more than 16 nonzeros per row: one warp
+    per row) and rows of 10k and 25k nonzeros, longer than a tile's staging
+    capacity (the whole CTA strides each)."""
+    rng = np.random.default_rng(3)
+    n = 30000
+    lens = rng.integers(1, 9, n)
+    lens[11] = 1500
+    lens[15000] = 10000
+    lens[20000] = 25000
+    rows = np.repeat(np.arange(n, dtype=np.int64), lens)
+    cols = np.concatenate([np.sort(rng.choice(n, l, replace=False)) for l in lens]).astype(np.int64)
+    vals = rng.standard_normal(rows.shape[0]).astype(np.float32)
+    return W.Coo(rows, cols, vals, n).shuffled(4)
+
+
+CASES = {
+    "diffusion_400x300": lambda: W.lognormal_diffusion_2d(400, 300, 1.0, 8.0, 5).shuffled(2),
+    "dense_rows": _dense_rows_coo,
+    # about 5M nonzeros: more tiles than one wave of CTAs holds
+    "laplacian_1000x1000": lambda: W.laplacian_2d(1000).shuffled(6),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_noalloc_matches_regular_entry_point(mps, oracle, case):
     L, noalloc = _noalloc()
-    coo = W.lognormal_diffusion_2d(400, 300, 1.0, 8.0, 5).shuffled(2)
+    coo = CASES[case]()
     n, nnz = coo.n, coo.nnz
     keys = torch.from_numpy(coo.keys()).cuda()
     vals = torch.from_numpy(coo.vals).cuda()
@@ -56,8 +82,28 @@ def test_noalloc_matches_regular_entry_point(mps):
             torch.cuda.synchronize()
             assert torch.allclose(y, y_ref, rtol=1e-6, atol=1e-6), call
             assert abs(d.item() - d_ref.item()) <= 1e-9 * abs(d_ref.item()) + 1e-9, call
+            # and against the CPU oracle in FP64 (FP32 accumulation bound)
+            Ao = oracle.Csr(rp.cpu().numpy(), ci.cpu().numpy(), cv.cpu().numpy(), n)
+            xh = x.cpu().numpy().astype(np.float64)
+            yo = oracle.spmv(Ao, xh)
+            bound = oracle.spmv(oracle.Csr(Ao.row_ptr, Ao.col_ind, np.abs(Ao.val), n), np.abs(xh))
+            assert np.all(np.abs(y.cpu().numpy() - yo) <= 1e-6 * bound + 1e-30), call
+            wh = w.cpu().numpy().astype(np.float64)
+            dot_bound = np.abs(wh) @ bound
+            assert abs(d.item() - wh @ yo) <= 1e-6 * dot_bound + 1e-30, call
     finally:
         L.mps_csr_destroy(h)
+
+
+def test_noalloc_rejects_unaligned_arrays(mps):
+    L, noalloc = _noalloc()
+    buf = torch.zeros(64, device="cuda")
+    ibuf = torch.zeros(64, dtype=torch.int32, device="cuda")
+    rp = torch.tensor([0, 4, 8], dtype=torch.int32, device="cuda")
+    off = C.c_void_p(buf.data_ptr() + 4)               # 4-byte offset: not 16-byte aligned
+    st = noalloc(cabi.ptr(rp), cabi.ptr(ibuf), off, 2, 2, 8, cabi.ptr(buf), cabi.ptr(buf),
+                 cabi.ptr(buf), cabi.ptr(buf), None)
+    assert st == 1 and b"aligned" in L.mps_last_error_string()
 
 
 def test_noalloc_rejects_matrices_above_limit(mps):
