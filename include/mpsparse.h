@@ -101,6 +101,16 @@ mps_status mps_csr_create_from_csr(const int32_t* d_row_ptr, const int32_t* d_co
                                    const float* d_vals, uint32_t n_rows, uint32_t n_cols,
                                    uint64_t nnz, mps_csr** out, cudaStream_t stream);
 
+/* Test hook for the bounded device waits (no reference counterpart; the
+ * reference's waits are host-side and unbounded): runs the COO -> CSR sort
+ * into scratch it frees again, with tile `silent_tile` (tiles of 4096 keys)
+ * publishing no look-back status and every look-back wait bounded by
+ * `spin_limit` polls, so the tiles after it give up.  Returns MPS_ERR_TIMEOUT
+ * (the sort's output is discarded); the device and every handle stay usable. */
+mps_status mps_test_sort_lookback_timeout(const uint64_t* d_keys, const float* d_vals, uint64_t nnz,
+                                          uint32_t n_rows, uint32_t n_cols, uint32_t spin_limit,
+                                          uint32_t silent_tile, cudaStream_t stream);
+
 /* Release a handle (csr_tensor::~csr_tensor, iterative/BiCGSTAB/spmv.cpp:354-366). */
 mps_status mps_csr_destroy(mps_csr* A);
 

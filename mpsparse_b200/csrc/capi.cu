@@ -205,6 +205,32 @@ mps_status mps_csr_create_from_csr(const int32_t* d_row_ptr, const int32_t* d_co
     return MPS_OK;
 }
 
+mps_status mps_test_sort_lookback_timeout(const uint64_t* d_keys, const float* d_vals, uint64_t nnz,
+                                          uint32_t n_rows, uint32_t n_cols, uint32_t spin_limit,
+                                          uint32_t silent_tile, cudaStream_t s) {
+    if (!d_keys || !d_vals || spin_limit == 0) return fail(MPS_ERR_ARG, "null argument or zero spin limit");
+    mps_status st = check_shape(nnz, n_rows, n_cols);
+    if (st != MPS_OK) return st;
+    CsrMat m;
+    unsigned* d_err = nullptr;
+    MPS_CUDA(cudaMalloc(&d_err, sizeof(unsigned)));
+    st = alloc_csr(m, n_rows, n_cols, nnz, d_err);
+    cudaError_t e = cudaSuccess;
+    if (st == MPS_OK) {
+        e = cudaMemsetAsync(d_err, 0, sizeof(unsigned), s);
+        if (e == cudaSuccess)
+            e = sort_to_csr(d_keys, reinterpret_cast<const uint32_t*>(d_vals), nnz, n_rows, n_cols, m.rp,
+                            m.ci, reinterpret_cast<uint32_t*>(m.v), d_err, s, spin_limit, silent_tile);
+        unsigned err = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        st = e != cudaSuccess ? cuda_fail(e, "sort (timeout test)") : device_error(err, "COO->CSR");
+    }
+    csr_free(m);
+    cudaFree(d_err);
+    return st;
+}
+
 mps_status mps_csr_destroy(mps_csr* h) {
     if (!h) return MPS_OK;
     csr_free(h->A);

@@ -167,10 +167,13 @@ constexpr int kCsrPad = 16;
 // ---- internal entry points ---------------------------------------------------
 // Sort packed keys into CSR arrays (caller-allocated outputs).  `payload` is
 // moved as 32-bit words.  Returns a CUDA error; device-side range / timeout
-// errors are OR-ed into *d_err.
+// errors are OR-ed into *d_err.  spin_limit (0: the standard bound) and
+// silent_tile (a tile that publishes no look-back status; none by default)
+// exist for the bounded-wait test hook only.
 cudaError_t sort_to_csr(const uint64_t* keys, const uint32_t* payload, uint64_t nnz,
                         uint32_t n_rows, uint32_t n_cols, int32_t* row_ptr, int32_t* col_out,
-                        uint32_t* payload_out, unsigned* d_err, cudaStream_t s);
+                        uint32_t* payload_out, unsigned* d_err, cudaStream_t s,
+                        unsigned spin_limit = 0, unsigned silent_tile = 0xffffffffu);
 
 // Tile plan of A (tile_nnz <= 0: the default size; stages <= 0 /
 // evict_first < 0: keep the current plan's choice).  Synchronises `s` once to

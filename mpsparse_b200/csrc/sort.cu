@@ -126,7 +126,7 @@ sort_onesweep(const unsigned long long* __restrict__ kin, const unsigned* __rest
               unsigned long long* __restrict__ kout, int32_t* __restrict__ col_out,
               unsigned* __restrict__ vout, uint64_t nnz, KeyShape ks, int shift,
               const unsigned* __restrict__ digit_base, unsigned long long* status,
-              unsigned* tile_counter, unsigned* err) {
+              unsigned* tile_counter, unsigned* err, unsigned spin_limit, unsigned silent_tile) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SortSmem& S = *reinterpret_cast<SortSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -189,20 +189,25 @@ sort_onesweep(const unsigned long long* __restrict__ kin, const unsigned* __rest
         S.whist[ww][tid] = total;
         total += c;
     }
-    // Decoupled look-back for digit `tid` across earlier tiles.
+    // Decoupled look-back for digit `tid` across earlier tiles.  Each wait is
+    // bounded (spin_limit polls): on a timeout the error word is set and the
+    // tile publishes what it has, so no later tile waits on it in turn.
+    // silent_tile (only ever set by the timeout test hook) names a tile that
+    // publishes nothing, so that the waits of the tiles after it run out.
     unsigned long long* st = status + (size_t)tile * 256 + tid;
+    const bool publish = tile != silent_tile;
     unsigned excl = 0;
     if (tile == 0) {
-        st_relaxed_u64(st, kFlagPrefix | total);
+        if (publish) st_relaxed_u64(st, kFlagPrefix | total);
     } else {
-        st_relaxed_u64(st, kFlagAgg | total);
+        if (publish) st_relaxed_u64(st, kFlagAgg | total);
         long look = (long)tile - 1;
         unsigned spins = 0;
         while (look >= 0) {
             unsigned long long s = ld_relaxed_u64(status + (size_t)look * 256 + tid);
             const unsigned flag = (unsigned)(s >> 32);
             if (flag == 0) {
-                if (++spins > kSpinLimit) {
+                if (++spins > spin_limit) {
                     atomicOr(err, kErrTimeout);
                     break;
                 }
@@ -213,7 +218,7 @@ sort_onesweep(const unsigned long long* __restrict__ kin, const unsigned* __rest
             if (flag == 2) break;
             --look;
         }
-        st_relaxed_u64(st, kFlagPrefix | (unsigned long long)(excl + total));
+        if (publish) st_relaxed_u64(st, kFlagPrefix | (unsigned long long)(excl + total));
     }
     const unsigned dstart = block_excl_scan_256(total, S.wsum);
     S.dstart[tid] = dstart;
@@ -316,7 +321,9 @@ cudaError_t exclusive_scan_rows(const unsigned* counts, uint64_t n, int32_t* out
 
 cudaError_t sort_to_csr(const uint64_t* keys, const uint32_t* payload, uint64_t nnz,
                         uint32_t n_rows, uint32_t n_cols, int32_t* row_ptr, int32_t* col_out,
-                        uint32_t* payload_out, unsigned* d_err, cudaStream_t s) {
+                        uint32_t* payload_out, unsigned* d_err, cudaStream_t s,
+                        unsigned spin_limit, unsigned silent_tile) {
+    if (spin_limit == 0) spin_limit = kSpinLimit;
     const int rb = bit_width(n_rows ? n_rows - 1 : 0), cb = bit_width(n_cols ? n_cols - 1 : 0);
     const int bits = rb + cb;
     const int passes = bits > 0 ? (bits + 7) / 8 : 1;
@@ -384,16 +391,16 @@ cudaError_t sort_to_csr(const uint64_t* keys, const uint32_t* payload, uint64_t 
             const int sh = 8 * p;
             if (first && last)
                 sort_onesweep<true, true><<<(unsigned)ntiles, kSortNT, smem, s>>>(
-                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err);
+                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err, spin_limit, silent_tile);
             else if (first)
                 sort_onesweep<true, false><<<(unsigned)ntiles, kSortNT, smem, s>>>(
-                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err);
+                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err, spin_limit, silent_tile);
             else if (last)
                 sort_onesweep<false, true><<<(unsigned)ntiles, kSortNT, smem, s>>>(
-                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err);
+                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err, spin_limit, silent_tile);
             else
                 sort_onesweep<false, false><<<(unsigned)ntiles, kSortNT, smem, s>>>(
-                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err);
+                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err, spin_limit, silent_tile);
             kin = ko;
             vin = vo;
         }

@@ -31,6 +31,10 @@ def test_argument_checks_without_gpu():
     assert L.mps_csr_create_from_keys(None, None, 10, 4, 4, C.byref(h), None) == 1
     assert L.mps_csr_create_from_keys(None, None, 1 << 31, 4, 4, C.byref(h), None) == 1
     assert L.mps_csr_cg(None, None, None, None, None, None) == 1
+    f = L.mps_test_sort_lookback_timeout
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
+                  C.c_uint32, C.c_void_p]
+    assert f(None, None, 10, 4, 4, 100, 0, None) == 1
     assert L.mps_csr_destroy(None) == 0
 
 

@@ -101,3 +101,30 @@ def test_csr_tensor_fills_outputs_and_cabi(mps, golden):
     L.mps_csr_destroy(h)
     assert np.array_equal(r2.cpu().numpy(), g["row_ptr"])
     assert np.array_equal(v2.cpu().numpy(), g["csr_vals"])
+
+
+def test_lookback_timeout_returns_error_and_device_stays_usable(mps, oracle):
+    """A bounded device wait that runs out: the timeout hook makes tile 0
+    publish no look-back status, so the later tiles' waits (bounded at 20,000
+    polls, well under a second) give up.  The call returns MPS_ERR_TIMEOUT,
+    and afterwards the device and the library still convert bit-exactly."""
+    import ctypes as C
+    from mpsparse_b200 import workloads as W
+    from tests import cabi
+    L = cabi.lib()
+    f = L.mps_test_sort_lookback_timeout
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
+                  C.c_uint32, C.c_void_p]
+    f.restype = C.c_int
+    c = W.laplacian_2d(128).shuffled(3)               # 81,408 keys: 20 tiles
+    keys = torch.from_numpy(c.keys()).cuda()
+    vals = torch.from_numpy(c.vals).cuda()
+    for _ in range(2):
+        st = f(cabi.ptr(keys), cabi.ptr(vals), c.nnz, c.n, c.n, 20000, 0, None)
+        assert st == 4, st                             # MPS_ERR_TIMEOUT
+        assert b"bounded device wait" in L.mps_last_error_string()
+    torch.cuda.synchronize()
+    # the same hook with no silent tile is an ordinary conversion
+    assert f(cabi.ptr(keys), cabi.ptr(vals), c.nnz, c.n, c.n, 20000, 0xFFFFFFFF, None) == 0
+    out = _csr_gpu(mps, c.keys(), c.vals, c.n, c.n)
+    _assert_same(out, oracle.coo_to_csr(c.keys(), c.vals, c.n, c.n))
