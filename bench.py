@@ -358,11 +358,50 @@ def run_ours(args, rank, world, dev):
     out["e2e_plain_cg"] = (e2e_drop_in(args, systems, dev, warm, steps, None)
                            if args.solver == "learned" and not args.skip_e2e_plain else None)
     single = world == 1
+    out["mlp"] = mlp_leg(systems[0][1], dev) if args.solver == "learned" and single else None
     c3 = C3Context(args, dev) if single and not (args.skip_spmv and args.skip_configs) else None
     out["spmv"] = spmv_c3(args, dev, c3) if single and not args.skip_spmv else None
     out["batched"] = batched_c5(args, dev, rank, world) if not args.skip_batched else None
     out["configs"] = configs_legs(args, dev, c3) if single and not args.skip_configs else None
     return out
+
+
+def mlp_leg(A, dev):
+    """The learned factor's network on the tensor cores: forward and backward
+    passes over the features of a 512^2 system's G (785,408 nonzeros = rows
+    of the network), BF16 features resident on the GPU, CUDA events per
+    launch.  FLOPs: 2 (16*64 + 64*64 + 64) = 10,368 per row forward; the
+    backward pass (forward recomputed) counted as 3x that."""
+    import torch
+    from mpsparse_b200.fsai import LearnedFsai
+    m = LearnedFsai.load().model
+    X = A.fsai_features()[0]
+    Xb = X.to(torch.bfloat16).contiguous()
+    N = Xb.shape[0]
+    out = torch.empty(N, device=dev)
+    dout = torch.randn(N, device=dev, generator=torch.Generator(device=dev).manual_seed(5))
+    grad = torch.empty(5313, device=dev)
+    stream = torch.cuda.current_stream()
+    for _ in range(3):
+        m.forward_bf16(Xb, out)
+        m.backward_bf16(Xb, dout, grad)
+    m.status()
+    fwd = _event_ms(lambda: m.forward_bf16(Xb, out), stream, 20)
+    bwd = _event_ms(lambda: m.backward_bf16(Xb, dout, grad), stream, 20)
+    m.status()
+    f_fwd, f_bwd = 10368.0 * N, 3 * 10368.0 * N
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["bf16_tflops"])
+    except Exception:
+        pass
+    tf = lambda fl, ms: fl / (ms * 1e-3) / 1e12
+    return {"rows": N, "forward_us": fwd * 1e3, "forward_tflops": tf(f_fwd, fwd),
+            "backward_us": bwd * 1e3, "backward_tflops": tf(f_bwd, bwd),
+            "bf16_peak_tflops": peak,
+            "forward_frac_of_bf16_peak": tf(f_fwd, fwd) / peak if peak else None,
+            "note": "128 GELU activations per row run on the SFU/FP32 pipes beside the MMAs"}
 
 
 def e2e_drop_in(args, systems, dev, warm, steps, fsai=None):
@@ -931,7 +970,7 @@ def main():
                 "setup_ms_first_solve": res["setup_ms_first_solve"],
                 "plain_cg": res["plain_cg"], "jacobi_pcg": res["jacobi_pcg"],
                 "speedup_vs_plain_cg": res["plain_cg"]["ms_per_solve"] / res["ms_per_solve"],
-                "spmv": spmv, "batched": res["batched"], "configs": res["configs"],
+                "spmv": spmv, "batched": res["batched"], "configs": res["configs"], "mlp": res["mlp"],
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": res["e2e"], "e2e_plain_cg": res["e2e_plain_cg"],
                 "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]}

@@ -278,6 +278,17 @@ mps_status mps_fsai_mlp_backward(const mps_fsai_model* m, const float* d_X, cons
                                  uint64_t N, float* d_grad, cudaStream_t stream);
 mps_status mps_fsai_probe_grad(mps_csr* A, const float* d_V, int32_t k, float* d_grad_g,
                                double* loss, cudaStream_t stream);
+/* The same network passes on BF16 features (N x 16, 16-byte aligned), the
+ * form attach uses internally: stream-ordered, no allocation and no
+ * synchronisation, so they can be chained or timed with events.  A bounded
+ * tensor-core wait that gave up is reported by mps_fsai_model_status (which
+ * synchronises the stream).  backward_bf16 overwrites d_grad. */
+mps_status mps_fsai_mlp_forward_bf16(const mps_fsai_model* m, const void* d_Xbf16, uint64_t N,
+                                     float* d_out, cudaStream_t stream);
+mps_status mps_fsai_mlp_backward_bf16(const mps_fsai_model* m, const void* d_Xbf16,
+                                      const float* d_dout, uint64_t N, float* d_grad,
+                                      cudaStream_t stream);
+mps_status mps_fsai_model_status(const mps_fsai_model* m, cudaStream_t stream);
 
 /* ---- Batched solve ------------------------------------------------------ */
 

@@ -349,10 +349,12 @@ static mps_status fsai_prepare(mps_csr* h, cudaStream_t s) {
 
 static cudaError_t mlp_forward_launch(const MlpPacked* wp, const __nv_bfloat16* X, long N, float* out,
                                       unsigned* err, cudaStream_t s) {
-    const size_t smem = sizeof(MlpFwdSmem);
+    const size_t smem = sizeof(MlpFwdSmem) > kMlpFwdSmemFloor ? sizeof(MlpFwdSmem) : kMlpFwdSmemFloor;
+    static_assert(sizeof(MlpFwdSmem) + 1024 <= (228 * 1024) / kMlpFwdCtasPerSm, "forward CTAs per SM");
+    static_assert((kMlpFwdSmemFloor + 1024) * (kMlpFwdCtasPerSm + 1) > 228 * 1024, "at most 4 per SM");
     cudaFuncSetAttribute(mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     long tiles = (N + kMlpRows - 1) / kMlpRows;
-    int grid = num_sms() * 2;
+    int grid = num_sms() * kMlpFwdCtasPerSm;
     if (tiles < grid) grid = (int)(tiles > 0 ? tiles : 1);
     mlp_forward_tc<<<grid, kMlpThreads, smem, s>>>(wp, X, N, out, err);
     return cudaGetLastError();
@@ -361,9 +363,11 @@ static cudaError_t mlp_forward_launch(const MlpPacked* wp, const __nv_bfloat16* 
 static cudaError_t mlp_backward_launch(const MlpPacked* wp, const __nv_bfloat16* X, const float* dout,
                                        long N, float* grad, unsigned* err, cudaStream_t s) {
     const size_t smem = sizeof(MlpBwdSmem);
+    static_assert(sizeof(MlpBwdSmem) + 1024 <= (228 * 1024) / kMlpBwdCtasPerSm, "backward CTAs per SM");
+    static_assert((sizeof(MlpBwdSmem) + 1024) * (kMlpBwdCtasPerSm + 1) > 228 * 1024, "at most 2 per SM");
     cudaFuncSetAttribute(mlp_backward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     long tiles = (N + kMlpRows - 1) / kMlpRows;
-    int grid = num_sms();
+    int grid = num_sms() * kMlpBwdCtasPerSm;
     if (tiles < grid) grid = (int)(tiles > 0 ? tiles : 1);
     mlp_backward_tc<<<grid, kMlpThreads, smem, s>>>(wp, X, dout, N, grad, err);
     return cudaGetLastError();
@@ -522,6 +526,32 @@ mps_status mps_fsai_mlp_forward(const mps_fsai_model* m, const float* d_X, uint6
     MPS_CUDA(to_bf16_launch(d_X, xb, N * kNF, s));
     MPS_CUDA(mlp_forward_launch(m->packed, xb, (long)N, d_out, m->err, s));
     cudaFreeAsync(xb, s);
+    return model_error(m, s);
+}
+
+mps_status mps_fsai_mlp_forward_bf16(const mps_fsai_model* m, const void* d_Xbf16, uint64_t N,
+                                     float* d_out, cudaStream_t s) {
+    if (!m || !d_Xbf16 || !d_out) return fail(MPS_ERR_ARG, "null argument");
+    if (reinterpret_cast<uintptr_t>(d_Xbf16) & 15) return fail(MPS_ERR_ARG, "X must be 16-byte aligned");
+    if (N == 0) return MPS_OK;
+    MPS_CUDA(mlp_forward_launch(m->packed, static_cast<const __nv_bfloat16*>(d_Xbf16), (long)N, d_out,
+                                m->err, s));
+    return MPS_OK;
+}
+
+mps_status mps_fsai_mlp_backward_bf16(const mps_fsai_model* m, const void* d_Xbf16, const float* d_dout,
+                                      uint64_t N, float* d_grad, cudaStream_t s) {
+    if (!m || !d_Xbf16 || !d_dout || !d_grad) return fail(MPS_ERR_ARG, "null argument");
+    if (reinterpret_cast<uintptr_t>(d_Xbf16) & 15) return fail(MPS_ERR_ARG, "X must be 16-byte aligned");
+    MPS_CUDA(cudaMemsetAsync(d_grad, 0, kNParam * 4, s));
+    if (N == 0) return MPS_OK;
+    MPS_CUDA(mlp_backward_launch(m->packed, static_cast<const __nv_bfloat16*>(d_Xbf16), d_dout, (long)N,
+                                 d_grad, m->err, s));
+    return MPS_OK;
+}
+
+mps_status mps_fsai_model_status(const mps_fsai_model* m, cudaStream_t s) {
+    if (!m) return fail(MPS_ERR_ARG, "null argument");
     return model_error(m, s);
 }
 

@@ -126,10 +126,27 @@ __device__ __forceinline__ void tmem_ld64(unsigned taddr, float* v) {
     for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ float gelu_f(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// The network's activation: GELU in its tanh form (Hendrycks & Gimpel 2016),
+//   gelu(x) = 0.5 x (1 + tanh(c (x + 0.044715 x^3))),  c = sqrt(2 / pi),
+// with the SFU's tanh (tanh.approx.f32: about 11 correct bits, finer than the
+// BF16 rounding of the activations that follows).  One SFU operation and a
+// few FMAs per activation; the activations, not the MMAs, are the bulk of
+// the network's instruction work (128 per row against 5 MMAs per 128 rows).
+__device__ __forceinline__ float tanh_sfu(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float kGeluC = 0.7978845608028654f;   // sqrt(2 / pi)
+constexpr float kGeluA = 0.044715f;
+__device__ __forceinline__ float gelu_f(float x) {
+    const float t = tanh_sfu(kGeluC * fmaf(kGeluA * x, x * x, x));
+    return 0.5f * x * (1.0f + t);
+}
 __device__ __forceinline__ float gelu_d(float x) {
-    return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) +
-           x * expf(-0.5f * x * x) * 0.39894228040143268f;
+    const float x2 = x * x;
+    const float t = tanh_sfu(kGeluC * fmaf(kGeluA * x, x2, x));
+    return fmaf(0.5f * x * kGeluC * fmaf(3.0f * kGeluA, x2, 1.0f), fmaf(-t, t, 1.0f), 0.5f * (1.0f + t));
 }
 
 // Eight FP32 values -> one 16-byte chunk of BF16 in SMEM.
@@ -154,13 +171,15 @@ struct MlpFwdSmem {
     unsigned long long bar;
     unsigned taddr;
     int abort;
-    // Operand reads of the MMAs stay inside the tiles above; this margin keeps
-    // them inside the CTA's allocation even for a misdescribed stride.
-    unsigned char margin[32 * 1024];
 };
+// Four forward CTAs per SM: 4 x 128 TMEM columns fill the SM's 512, and the
+// launch asks for at least this much shared memory so that a fifth CTA never
+// becomes resident (its TMEM allocation would wait for a column range).
+constexpr int kMlpFwdCtasPerSm = 4;
+constexpr size_t kMlpFwdSmemFloor = 50 * 1024;
 
 // out[r] = net(X[r]) for r < N.  X is BF16 [N][16] (32 bytes per row).
-__global__ void __launch_bounds__(kMlpThreads, 1)
+__global__ void __launch_bounds__(kMlpThreads, kMlpFwdCtasPerSm)
 mlp_forward_tc(const MlpPacked* __restrict__ wg, const __nv_bfloat16* __restrict__ X, long N,
                float* __restrict__ out, unsigned* err) {
     extern __shared__ __align__(1024) unsigned char mlp_smem[];
@@ -262,8 +281,10 @@ struct MlpBwdSmem {
     unsigned long long bar;
     unsigned taddr;
     int abort;
-    unsigned char margin[64 * 1024];   // see MlpFwdSmem::margin
 };
+// Two backward CTAs per SM: 2 x 256 TMEM columns; the shared memory of a CTA
+// (about 85 KB) admits no third.
+constexpr int kMlpBwdCtasPerSm = 2;
 
 // Warp-reduce 64 per-row values and add them to a shared accumulator.
 __device__ __forceinline__ void warp_accum64(const float* v, float* acc) {
@@ -276,7 +297,7 @@ __device__ __forceinline__ void warp_accum64(const float* v, float* acc) {
 
 // grad (FP32, parameter layout W1, b1, W2, b2, w3, b3) += d loss / d params
 // for d loss / d out = dout.
-__global__ void __launch_bounds__(kMlpThreads, 1)
+__global__ void __launch_bounds__(kMlpThreads, kMlpBwdCtasPerSm)
 mlp_backward_tc(const MlpPacked* __restrict__ wg, const __nv_bfloat16* __restrict__ X,
                 const float* __restrict__ dout, long N, float* __restrict__ grad, unsigned* err) {
     extern __shared__ __align__(1024) unsigned char mlp_smem[];

@@ -105,6 +105,31 @@ public:
               "mlp_backward");
         return g;
     }
+    // Raw passes on BF16 features, stream-ordered without a synchronisation
+    // (timing, chaining); status() synchronises and reports a timed-out wait.
+    void forward_bf16(torch::Tensor Xb, torch::Tensor out) const {
+        TORCH_CHECK(Xb.is_cuda() && Xb.scalar_type() == torch::kBFloat16 && Xb.is_contiguous() &&
+                        Xb.dim() == 2 && Xb.size(1) == 16, "Xb must be a contiguous CUDA bf16 N x 16 tensor");
+        TORCH_CHECK(out.is_cuda() && out.scalar_type() == torch::kFloat32 && out.is_contiguous() &&
+                        out.numel() == Xb.size(0), "out must be a contiguous CUDA float32 N tensor");
+        c10::cuda::CUDAGuard g(Xb.get_device());
+        check(mps_fsai_mlp_forward_bf16(m_, Xb.data_ptr(), (uint64_t)Xb.size(0), out.data_ptr<float>(),
+                                        cur_stream()),
+              "mlp_forward_bf16");
+    }
+    void backward_bf16(torch::Tensor Xb, torch::Tensor dout, torch::Tensor grad) const {
+        TORCH_CHECK(Xb.is_cuda() && Xb.scalar_type() == torch::kBFloat16 && Xb.is_contiguous() &&
+                        Xb.dim() == 2 && Xb.size(1) == 16, "Xb must be a contiguous CUDA bf16 N x 16 tensor");
+        TORCH_CHECK(dout.is_cuda() && dout.scalar_type() == torch::kFloat32 && dout.is_contiguous() &&
+                        dout.numel() == Xb.size(0), "dout must be a contiguous CUDA float32 N tensor");
+        TORCH_CHECK(grad.is_cuda() && grad.scalar_type() == torch::kFloat32 && grad.is_contiguous() &&
+                        grad.numel() == mps_fsai_param_count(), "grad must hold the parameter count");
+        c10::cuda::CUDAGuard g(Xb.get_device());
+        check(mps_fsai_mlp_backward_bf16(m_, Xb.data_ptr(), dout.data_ptr<float>(), (uint64_t)Xb.size(0),
+                                         grad.data_ptr<float>(), cur_stream()),
+              "mlp_backward_bf16");
+    }
+    void status() const { check(mps_fsai_model_status(m_, cur_stream()), "fsai model"); }
     mps_fsai_model* handle() const { return m_; }
 
 private:
@@ -716,7 +741,10 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         .def("params", &FsaiModel::params)
         .def("set_params", &FsaiModel::set_params, py::arg("params"))
         .def("forward", &FsaiModel::forward, py::arg("X"))
-        .def("backward", &FsaiModel::backward, py::arg("X"), py::arg("dout"));
+        .def("backward", &FsaiModel::backward, py::arg("X"), py::arg("dout"))
+        .def("forward_bf16", &FsaiModel::forward_bf16, py::arg("Xb"), py::arg("out"))
+        .def("backward_bf16", &FsaiModel::backward_bf16, py::arg("Xb"), py::arg("dout"), py::arg("grad"))
+        .def("status", &FsaiModel::status);
 
     py::class_<BatchSolver>(m, "batch_solver")
         .def(py::init<torch::Tensor, torch::Tensor, torch::Tensor, torch::Tensor>(), py::arg("row_ptr"),

@@ -573,9 +573,16 @@ static float bf16r(float f) {
     return r;
 }
 
-static double gelu(double x) { return 0.5 * x * (1.0 + erf(x / sqrt(2.0))); }
+/* The network's activation: GELU in its tanh form (Hendrycks & Gimpel 2016),
+ * 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))), and its derivative. */
+static double gelu(double x) {
+    const double c = sqrt(2.0 / M_PI);
+    return 0.5 * x * (1.0 + tanh(c * (x + 0.044715 * x * x * x)));
+}
 static double gelu_d(double x) {
-    return 0.5 * (1.0 + erf(x / sqrt(2.0))) + x * exp(-0.5 * x * x) / sqrt(2.0 * M_PI);
+    const double c = sqrt(2.0 / M_PI);
+    const double t = tanh(c * (x + 0.044715 * x * x * x));
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * c * (1.0 + 3.0 * 0.044715 * x * x);
 }
 
 typedef struct {

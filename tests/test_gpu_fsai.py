@@ -135,3 +135,24 @@ def test_stall_falls_back_to_jacobi(mps):
     x = torch.zeros(n, device="cuda")
     info = A.cgd(b, x, tol=1e-6, max_iter=20000, precond="fsai", stall_window=20)
     assert info["stalled"] and info["stop_rule_met"]
+
+
+def test_bf16_entry_points_match(mps, oracle, small):
+    """forward_bf16 / backward_bf16 (no allocation, no synchronisation) give
+    what the FP32-input passes give (the same kernels after the same
+    round-to-nearest BF16 conversion): the same bits forward; backward up to
+    the order of the per-CTA float atomics that sum the weight gradients."""
+    A = _csr_tensor(mps, small)
+    X = A.fsai_features()[0]
+    p = _random_params(oracle, 5)
+    m = mps._C.fsai_model(torch.from_numpy(p))
+    Xb = X.to(torch.bfloat16).contiguous()
+    out = torch.empty(X.shape[0], device="cuda")
+    m.forward_bf16(Xb, out)
+    dout = torch.from_numpy(np.random.default_rng(6).standard_normal(X.shape[0]).astype(np.float32)).cuda()
+    grad = torch.full((oracle.NPARAM,), float("nan"), device="cuda")
+    m.backward_bf16(Xb, dout, grad)
+    m.status()
+    assert torch.equal(out, m.forward(X))
+    g2 = m.backward(X, dout)
+    assert torch.allclose(grad, g2, rtol=1e-5, atol=1e-6 * float(g2.abs().max()))
