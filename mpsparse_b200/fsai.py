@@ -85,8 +85,23 @@ class LearnedFsai:
         return losses
 
 
-def evaluate(fsai: LearnedFsai | None, seeds, spec=SPEC_512, tol=1e-6, max_iter=40000):
-    """PCG iterations to ``tol`` with the learned factor, Jacobi and none."""
+def _timed(fn):
+    """fn() on the current stream, timed with CUDA events (device time)."""
+    st = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    out = fn()
+    b.record(st)
+    torch.cuda.synchronize()
+    return out, a.elapsed_time(b)
+
+
+def evaluate(fsai: LearnedFsai | None, seeds, spec=SPEC_512, tol=1e-6, max_iter=40000,
+             inner_tol=1e-4, timed=False):
+    """Per held-out seed: iterations (and, with ``timed``, device time of a
+    second solve on the same handle, after graph capture) to ``tol`` for the
+    learned factor in mixed-precision PCG (FP64 true residual), Jacobi-PCG
+    and plain CG in FP32 (their FP64 true residual reported beside)."""
     e = torch.empty(0)
     rows = []
     for s in seeds:
@@ -95,31 +110,104 @@ def evaluate(fsai: LearnedFsai | None, seeds, spec=SPEC_512, tol=1e-6, max_iter=
         A = csr_tensor(keys, vals, e, e, e, n, n, fill_outputs=False)
         b = torch.from_numpy(W.rhs(n, s + 7)).cuda()
         row = {"seed": s}
-        for name in (["fsai"] if fsai is not None else []) + ["jacobi", "none"]:
-            if name == "fsai":
+        if fsai is not None:
+            b64 = b.double()
+
+            def learned():
                 fsai.attach(A)
-            x = torch.zeros(n, device="cuda")
-            info = A.cgd(b, x, tol=tol, max_iter=max_iter, precond=name)
-            row[name] = info["iters"]
+                x = torch.zeros(n, dtype=torch.float64, device="cuda")
+                return A.cg_mixed(b64, x, tol=tol, inner_tol=inner_tol, max_inner=max_iter,
+                                  precond="fsai")
+            info, ms = _timed(learned)
+            if timed:
+                info, ms = _timed(learned)
+            row["fsai"] = {"iters": info["inner_iters"], "true_resid": info["rel_resid"],
+                           "converged": bool(info["converged"])}
+            if timed:
+                row["fsai"]["ms"] = ms
+        for name in ("jacobi", "none"):
+            def solve():
+                x = torch.zeros(n, device="cuda")
+                return A.cgd(b, x, tol=tol, max_iter=max_iter, precond=name)
+            info, ms = _timed(solve)
+            if timed:
+                info, ms = _timed(solve)
+            row[name] = {"iters": info["iters"], "true_resid": info["true_resid"],
+                         "converged": bool(info["converged"])}
+            if timed:
+                row[name]["ms"] = ms
         rows.append(row)
     return rows
 
 
+def summarize(rows):
+    """Mean / median / 95th percentile of iterations and times per method."""
+    out = {"systems": len(rows)}
+    for name in ("fsai", "jacobi", "none"):
+        if name not in rows[0]:
+            continue
+        it = np.array([r[name]["iters"] for r in rows], np.float64)
+        d = {"iters_mean": float(it.mean()), "iters_median": float(np.median(it)),
+             "iters_p95": float(np.percentile(it, 95)),
+             "true_resid_max": float(max(r[name]["true_resid"] for r in rows)),
+             "converged_fp64": int(sum(r[name]["converged"] for r in rows))}
+        if "ms" in rows[0][name]:
+            ms = np.array([r[name]["ms"] for r in rows], np.float64)
+            d.update(ms_mean=float(ms.mean()), ms_median=float(np.median(ms)),
+                     ms_p95=float(np.percentile(ms, 95)))
+        out[name] = d
+    if "fsai" in out:
+        out["fsai_fewer_iters_than_jacobi"] = int(sum(r["fsai"]["iters"] < r["jacobi"]["iters"]
+                                                     for r in rows))
+    return out
+
+
 def main():
     import argparse
-    ap = argparse.ArgumentParser(description="train the learned FSAI network on the GPU")
-    ap.add_argument("--systems", type=int, default=2000)
+    import json
+    ap = argparse.ArgumentParser(description="train the learned FSAI network on the GPU and "
+                                             "evaluate it on held-out systems")
+    ap.add_argument("--systems", type=int, default=2000, help="training seeds 0..systems-1")
     ap.add_argument("--epochs", type=int, default=1)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
-    ap.add_argument("--eval", type=int, default=5)
+    ap.add_argument("--no-train", action="store_true", help="evaluate the weights in --out")
+    ap.add_argument("--log", default=None, help="training record (JSON lines) written here")
+    ap.add_argument("--eval", type=int, default=5, help="held-out systems evaluated")
+    ap.add_argument("--eval-seed0", type=int, default=100_000)
+    ap.add_argument("--timed", action="store_true", help="also time the evaluation solves")
+    ap.add_argument("--report", default=None, help="evaluation rows + summary (JSON) written here")
     args = ap.parse_args()
-    f = LearnedFsai()
-    seeds = [s for _ in range(args.epochs) for s in range(args.systems)]
-    f.train(seeds, lr=args.lr)
-    f.save(args.out)
-    for r in evaluate(f, range(100_000, 100_000 + args.eval)):
-        print(r)
+    if args.no_train:
+        f = LearnedFsai.load(args.out)
+    else:
+        f = LearnedFsai()
+        seeds = [s for _ in range(args.epochs) for s in range(args.systems)]
+        logf = open(args.log, "w") if args.log else None
+        t0 = time.time()
+
+        def log(msg):
+            print(msg, flush=True)
+        losses = f.train(seeds, lr=args.lr, log=log)
+        f.save(args.out)
+        if logf:
+            logf.write(json.dumps({"command": "python -m mpsparse_b200.fsai " +
+                                   f"--systems {args.systems} --epochs {args.epochs} --lr {args.lr}",
+                                   "training_seeds": [0, args.systems - 1], "steps": len(seeds),
+                                   "lr": [args.lr, 2e-4], "probes": 4, "residual_iters": 30,
+                                   "seconds": time.time() - t0,
+                                   "loss_first_100": float(np.mean(losses[:100])),
+                                   "loss_last_100": float(np.mean(losses[-100:]))}) + "\n")
+            for k in range(0, len(losses), 100):
+                logf.write(json.dumps({"steps": [k + 1, min(k + 100, len(losses))],
+                                       "loss_mean": float(np.mean(losses[k:k + 100]))}) + "\n")
+            logf.close()
+    rows = evaluate(f, range(args.eval_seed0, args.eval_seed0 + args.eval), timed=args.timed)
+    summ = summarize(rows)
+    print(json.dumps(summ))
+    if args.report:
+        with open(args.report, "w") as fh:
+            json.dump({"summary": summ, "rows": rows}, fh)
 
 
 if __name__ == "__main__":
