@@ -568,11 +568,13 @@ def spmv_c3(args, dev, ctx):
     reps = 20
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(reps)]
+    torch.cuda.nvtx.range_push("spmv_timed")      # profilers can filter on this range
     for a, b in evs:
         a.record(stream)
         A.mv(x, y)
         b.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     ms = statistics.median(a.elapsed_time(b) for a, b in evs)
     bytes_alg = 8 * nnz + 4 * (n + 1) + 4 * n + 4 * n
     gbs = bytes_alg / (ms * 1e-3) / 1e9
@@ -893,6 +895,8 @@ def main():
     ap.add_argument("--batch-systems", type=int, default=4096)
     ap.add_argument("--only-spmv", action="store_true",
                     help="only the 256^3 (or --c3-grid) SpMV measurement; for ncu captures")
+    ap.add_argument("--only-mlp", action="store_true",
+                    help="only the network forward/backward timing on one 512^2 system's factor")
     ap.add_argument("--solver", default="learned", choices=["learned", "plain"],
                     help="headline solver (plain: the FP32 CG drop-in)")
     ap.add_argument("--inner-tol", type=float, default=1e-4,
@@ -921,6 +925,14 @@ def main():
     if args.only_spmv:
         ctx = C3Context(args, local)
         print(json.dumps({"spmv": spmv_c3(args, local, ctx)}))
+        return
+    if args.only_mlp:
+        import mpsparse_b200 as mps
+        coo, _ = c4_system(TEST_SEED0)
+        e = torch.empty(0)
+        A = mps.spmv.csr_tensor(torch.from_numpy(coo.keys()), torch.from_numpy(coo.vals), e, e, e,
+                                coo.n, coo.n, fill_outputs=False)
+        print(json.dumps({"mlp": mlp_leg(A, local)}))
         return
     if world > 1:
         import datetime

@@ -105,8 +105,13 @@ __device__ __forceinline__ unsigned block_excl_scan_256(unsigned v, unsigned* ws
     return off + inc - v;
 }
 
+// Look-back status word: epoch (bits 34+, the pass number + 1) | flag (bits
+// 32-33: 1 aggregate, 2 inclusive prefix) | count.  A word counts only in the
+// pass whose epoch it carries, so the array is zeroed once per sort, not once
+// per pass.
 constexpr unsigned long long kFlagAgg = 1ull << 32;
 constexpr unsigned long long kFlagPrefix = 2ull << 32;
+constexpr int kEpochShift = 34;
 
 struct SortSmem {
     unsigned long long keys[kTile];
@@ -126,7 +131,8 @@ sort_onesweep(const unsigned long long* __restrict__ kin, const unsigned* __rest
               unsigned long long* __restrict__ kout, int32_t* __restrict__ col_out,
               unsigned* __restrict__ vout, uint64_t nnz, KeyShape ks, int shift,
               const unsigned* __restrict__ digit_base, unsigned long long* status,
-              unsigned* tile_counter, unsigned* err, unsigned spin_limit, unsigned silent_tile) {
+              unsigned* tile_counter, unsigned* err, unsigned spin_limit, unsigned silent_tile,
+              unsigned epoch) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SortSmem& S = *reinterpret_cast<SortSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -196,16 +202,17 @@ sort_onesweep(const unsigned long long* __restrict__ kin, const unsigned* __rest
     // publishes nothing, so that the waits of the tiles after it run out.
     unsigned long long* st = status + (size_t)tile * 256 + tid;
     const bool publish = tile != silent_tile;
+    const unsigned long long ep = (unsigned long long)epoch << kEpochShift;
     unsigned excl = 0;
     if (tile == 0) {
-        if (publish) st_relaxed_u64(st, kFlagPrefix | total);
+        if (publish) st_relaxed_u64(st, ep | kFlagPrefix | total);
     } else {
-        if (publish) st_relaxed_u64(st, kFlagAgg | total);
+        if (publish) st_relaxed_u64(st, ep | kFlagAgg | total);
         long look = (long)tile - 1;
         unsigned spins = 0;
         while (look >= 0) {
             unsigned long long s = ld_relaxed_u64(status + (size_t)look * 256 + tid);
-            const unsigned flag = (unsigned)(s >> 32);
+            const unsigned flag = (s >> kEpochShift) == epoch ? (unsigned)(s >> 32) & 3u : 0u;
             if (flag == 0) {
                 if (++spins > spin_limit) {
                     atomicOr(err, kErrTimeout);
@@ -218,7 +225,7 @@ sort_onesweep(const unsigned long long* __restrict__ kin, const unsigned* __rest
             if (flag == 2) break;
             --look;
         }
-        if (publish) st_relaxed_u64(st, kFlagPrefix | (unsigned long long)(excl + total));
+        if (publish) st_relaxed_u64(st, ep | kFlagPrefix | (unsigned long long)(excl + total));
     }
     const unsigned dstart = block_excl_scan_256(total, S.wsum);
     S.dstart[tid] = dstart;
@@ -381,26 +388,30 @@ cudaError_t sort_to_csr(const uint64_t* keys, const uint32_t* payload, uint64_t 
         }
         const unsigned long long* kin = (const unsigned long long*)keys;
         const unsigned* vin = payload;
+        e = cudaMemsetAsync(status, 0, ntiles * 256 * 8, s);   // epoch 0: no pass's
+        if (e != cudaSuccess) goto out;
         for (int p = 0; p < passes; ++p) {
             const bool first = p == 0, last = p == passes - 1;
-            e = cudaMemsetAsync(status, 0, ntiles * 256 * 8, s);
-            if (e != cudaSuccess) goto out;
             unsigned long long* ko = kb[p & 1];
             unsigned* vo = last ? payload_out : vb[p & 1];
             const unsigned* db = base + p * 256;
             const int sh = 8 * p;
             if (first && last)
                 sort_onesweep<true, true><<<(unsigned)ntiles, kSortNT, smem, s>>>(
-                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err, spin_limit, silent_tile);
+                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err, spin_limit, silent_tile,
+                    (unsigned)(p + 1));
             else if (first)
                 sort_onesweep<true, false><<<(unsigned)ntiles, kSortNT, smem, s>>>(
-                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err, spin_limit, silent_tile);
+                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err, spin_limit, silent_tile,
+                    (unsigned)(p + 1));
             else if (last)
                 sort_onesweep<false, true><<<(unsigned)ntiles, kSortNT, smem, s>>>(
-                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err, spin_limit, silent_tile);
+                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err, spin_limit, silent_tile,
+                    (unsigned)(p + 1));
             else
                 sort_onesweep<false, false><<<(unsigned)ntiles, kSortNT, smem, s>>>(
-                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err, spin_limit, silent_tile);
+                    kin, vin, ko, col_out, vo, nnz, ks, sh, db, status, ctr + p, d_err, spin_limit, silent_tile,
+                    (unsigned)(p + 1));
             kin = ko;
             vin = vo;
         }
