@@ -330,6 +330,17 @@ mps_status mps_batch_cg(mps_batch* B, const float* d_b, float* d_x, double tol, 
                         int32_t* d_iters, int32_t* d_converged, float* d_relres,
                         cudaStream_t stream);
 
+/* Mixed-precision batched solve: every system's solution accumulated in FP64
+ * (d_x64), its Krylov recurrences in FP32, and its residual replaced by the
+ * FP64 b - A x (FP64 products over the FP32 matrix) whenever it has dropped
+ * by inner_tol since the last replacement (0: 1e-3) or meets tol.  A system
+ * stops only when that true residual meets tol; d_relres receives it and
+ * d_converged says whether it met tol.  Same launch structure, queue and
+ * autotuned warps per system as mps_batch_cg.  No reference counterpart. */
+mps_status mps_batch_cg_mixed(mps_batch* B, const float* d_b, double* d_x64, double tol,
+                              double inner_tol, int32_t max_iter, int32_t* d_iters,
+                              int32_t* d_converged, float* d_relres, cudaStream_t stream);
+
 /* ---- BCSR --------------------------------------------------------------- */
 
 /* BCSR from pre-built block arrays: row-major B x B blocks (B = 4 or 8),

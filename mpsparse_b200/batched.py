@@ -101,6 +101,14 @@ class BatchedSolver:
         converged, relres) per system, on the device; no host sync."""
         return self.impl.cg(b, x, tol=tol, max_iter=max_iter)
 
+    def solve_mixed(self, b, x64, tol=1e-6, inner_tol=1e-3, max_iter=20000):
+        """Mixed precision: x64 (CUDA float64, total_rows) receives every
+        system's solution accumulated in FP64; each system's residual is
+        replaced by its FP64 b - A x as it drops, and a system stops only when
+        that true residual meets tol.  Returns (iters, converged, FP64 true
+        relative residual) per system, on the device; no host sync."""
+        return self.impl.cg_mixed(b, x64, tol=tol, inner_tol=inner_tol, max_iter=max_iter)
+
     @property
     def warps_per_system(self):
         return self.impl.warps_per_system

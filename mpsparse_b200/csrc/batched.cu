@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <chrono>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 #include "handles.hpp"
@@ -117,6 +118,7 @@ struct WarpGroup {
         return q;
     }
     __device__ float gather(const float* x, int c) const { return x[c]; }
+    __device__ double gather64(const double* x, int c) const { return x[c]; }
 };
 
 template <int CS>
@@ -173,6 +175,7 @@ struct ClusterGroup {
     }
     // vectors written by other CTAs of the cluster: read through L2
     __device__ float gather(const float* x, int c) const { return __ldcg(x + c); }
+    __device__ double gather64(const double* x, int c) const { return __ldcg(x + c); }
 };
 
 // Rows i and j of a CSR times x through the group's gather (see row_dot2).
@@ -206,12 +209,30 @@ __device__ __forceinline__ void grp_dot2(const Grp& G, const int* __restrict__ r
     }
 }
 
-// PCG on the systems the queue hands out, one system per group at a time.
+// b_i - (A x)_i in FP64 for an FP64 x (exact products of the FP32 values).
 template <class Grp>
+__device__ __forceinline__ double grp_resid64(const Grp& G, const int* __restrict__ rp,
+                                              const int* __restrict__ ci, const float* __restrict__ v,
+                                              const double* x, float bi, int i) {
+    const int e = __ldg(rp + i + 1);
+    double s = 0.0;
+    for (int k = __ldg(rp + i); k < e; ++k) s = fma((double)__ldg(v + k), G.gather64(x, __ldg(ci + k)), s);
+    return (double)bi - s;
+}
+
+// PCG on the systems the queue hands out, one system per group at a time.
+// XT = float: x in FP32, a system stops when its recurrence residual meets
+// tol.  XT = double (mixed precision): x accumulated in FP64, and whenever a
+// system's recurrence residual has dropped by sqrt(delta2) since the last
+// replacement, or meets tol, it is replaced by the FP64 b - A x (reliable
+// updates, as in the single-system solver); the system stops only when that
+// true residual meets tol, and relres reports it.
+template <class Grp, typename XT>
 __device__ __forceinline__ void batch_pcg_body(const BatchDev& B, const float* __restrict__ b,
-                                               float* __restrict__ x, const BatchOut& out, double tol,
+                                               XT* __restrict__ x, const BatchOut& out, double tol,
                                                int max_iter, int stall_window, unsigned* queue,
-                                               GroupShared& sh) {
+                                               GroupShared& sh, double delta2) {
+    constexpr bool kIR = std::is_same<XT, double>::value;
     const Grp G;
     constexpr int GS = Grp::GS;
     const int lt = G.lt;
@@ -233,7 +254,7 @@ __device__ __forceinline__ void batch_pcg_body(const BatchDev& B, const float* _
         double acc[2] = {0.0, 0.0};
         for (int i = lo + lt; i < hi; i += GS) {
             const float bi = b[i];
-            x[i] = 0.f;
+            x[i] = XT(0);
             B.r[i] = bi;
             const float z = mode == 1 ? bi * B.dinv[i] : bi;
             if (mode != 2) B.p[i] = z;
@@ -245,7 +266,7 @@ __device__ __forceinline__ void batch_pcg_body(const BatchDev& B, const float* _
         double rz = acc[1], rr = bb;
         const double thresh = tol * tol * bb;
         int it = 0, conv = bb == 0.0, best_it = 0;
-        double best = 1e300;
+        double best = 1e300, rr_ref = bb;
         if (!conv && mode == 2) {                 // p = G^T G b
             double a2[1] = {0.0};
             for (int i = lo + lt; i < hi; i += 2 * GS) {
@@ -285,10 +306,12 @@ __device__ __forceinline__ void batch_pcg_body(const BatchDev& B, const float* _
             }
             G.template reduce<1>(a, sh);
             if (!(a[0] > 0.0)) break;             // breakdown (not SPD)
-            const float alpha = (float)(rz / a[0]);
+            const double alpha64 = rz / a[0];
+            const float alpha = (float)alpha64;
             double c[2] = {0.0, 0.0};
             for (int i = lo + lt; i < hi; i += GS) {
-                x[i] = fmaf(alpha, B.p[i], x[i]);
+                if constexpr (kIR) x[i] = fma(alpha64, (double)B.p[i], x[i]);
+                else x[i] = fmaf(alpha, B.p[i], x[i]);
                 const float ri = fmaf(-alpha, B.q[i], B.r[i]);
                 B.r[i] = ri;
                 c[0] += (double)ri * ri;
@@ -297,6 +320,24 @@ __device__ __forceinline__ void batch_pcg_body(const BatchDev& B, const float* _
             G.template reduce<2>(c, sh);
             ++it;
             rr = c[0];
+            if constexpr (kIR) {
+                if (rr <= thresh || rr < delta2 * rr_ref) {
+                    // residual replacement: r = (float)(b - A x) from the FP64 x
+                    double t[2] = {0.0, 0.0};
+                    for (int i = lo + lt; i < hi; i += GS) {
+                        const double rt = grp_resid64(G, B.rp, B.ci, B.v, x, b[i], i);
+                        const float rf = (float)rt;
+                        B.r[i] = rf;
+                        t[0] += rt * rt;
+                        t[1] += (double)rf * rf * B.dinv[i];
+                    }
+                    G.template reduce<2>(t, sh);
+                    c[0] = t[0];
+                    c[1] = t[1];
+                    rr = t[0];
+                    rr_ref = t[0];
+                }
+            }
             if (rr <= thresh) {
                 conv = 1;
                 break;
@@ -358,20 +399,21 @@ __device__ __forceinline__ void batch_pcg_body(const BatchDev& B, const float* _
     }
 }
 
-template <int WPS>
+template <int WPS, typename XT>
 __global__ void __launch_bounds__(kBatchNT, 2)
-batch_pcg(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchOut out, double tol,
-          int max_iter, int stall_window, unsigned* queue) {
+batch_pcg(BatchDev B, const float* __restrict__ b, XT* __restrict__ x, BatchOut out, double tol,
+          int max_iter, int stall_window, unsigned* queue, double delta2) {
     __shared__ GroupShared sh;
-    batch_pcg_body<WarpGroup<WPS>>(B, b, x, out, tol, max_iter, stall_window, queue, sh);
+    batch_pcg_body<WarpGroup<WPS>, XT>(B, b, x, out, tol, max_iter, stall_window, queue, sh, delta2);
 }
 
 // 32 warps per system: one 1024-thread CTA per system.
+template <typename XT>
 __global__ void __launch_bounds__(1024, 1)
-batch_pcg_cta(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchOut out,
-              double tol, int max_iter, int stall_window, unsigned* queue) {
+batch_pcg_cta(BatchDev B, const float* __restrict__ b, XT* __restrict__ x, BatchOut out,
+              double tol, int max_iter, int stall_window, unsigned* queue, double delta2) {
     __shared__ GroupShared sh;
-    batch_pcg_body<WarpGroup<32>>(B, b, x, out, tol, max_iter, stall_window, queue, sh);
+    batch_pcg_body<WarpGroup<32>, XT>(B, b, x, out, tol, max_iter, stall_window, queue, sh, delta2);
 }
 
 // One cluster of kClusterCTAs CTAs per system (launched with the cluster
@@ -379,26 +421,30 @@ batch_pcg_cta(BatchDev B, const float* __restrict__ b, float* __restrict__ x, Ba
 // so every cluster barrier is reached by all of them.
 constexpr int kClusterCTAs = 8;
 
+template <typename XT>
 __global__ void __launch_bounds__(kBatchNT, 2)
-batch_pcg_cluster(BatchDev B, const float* __restrict__ b, float* __restrict__ x, BatchOut out,
-                  double tol, int max_iter, int stall_window, unsigned* queue) {
+batch_pcg_cluster(BatchDev B, const float* __restrict__ b, XT* __restrict__ x, BatchOut out,
+                  double tol, int max_iter, int stall_window, unsigned* queue, double delta2) {
     __shared__ GroupShared sh;
     if (threadIdx.x == 0) sh.flip = 0;
     cooperative_groups::this_cluster().sync();
-    batch_pcg_body<ClusterGroup<kClusterCTAs>>(B, b, x, out, tol, max_iter, stall_window, queue, sh);
+    batch_pcg_body<ClusterGroup<kClusterCTAs>, XT>(B, b, x, out, tol, max_iter, stall_window, queue, sh,
+                                                   delta2);
     cooperative_groups::this_cluster().sync();   // no CTA leaves while another reads its memory
 }
 
-using BatchKernel = void (*)(BatchDev, const float*, float*, BatchOut, double, int, int, unsigned*);
+template <typename XT>
+using BatchKernel = void (*)(BatchDev, const float*, XT*, BatchOut, double, int, int, unsigned*, double);
 
-BatchKernel batch_kernel(int wps) {
+template <typename XT>
+BatchKernel<XT> batch_kernel(int wps) {
     switch (wps) {
-        case 1: return batch_pcg<1>;
-        case 2: return batch_pcg<2>;
-        case 4: return batch_pcg<4>;
-        case 8: return batch_pcg<8>;
-        case 16: return batch_pcg<16>;
-        default: return batch_pcg_cta;
+        case 1: return batch_pcg<1, XT>;
+        case 2: return batch_pcg<2, XT>;
+        case 4: return batch_pcg<4, XT>;
+        case 8: return batch_pcg<8, XT>;
+        case 16: return batch_pcg<16, XT>;
+        default: return batch_pcg_cta<XT>;
     }
 }
 
@@ -427,6 +473,8 @@ struct mps_batch {
     // one-launch graph of the last call: [queue reset, persistent kernel]
     cudaGraphExec_t exec = nullptr;
     const void* exec_key[5] = {};
+    int exec_mode = 0;             // 0: FP32 x, 1: mixed precision (FP64 x)
+    double exec_delta2 = -1.0;
     int exec_wps = 0;
     int exec_clusters = -1;
     double exec_tol = -1.0;
@@ -467,9 +515,10 @@ static BatchDev batch_view(mps_batch* B) {
 
 // One batch: the largest systems (queue order front) on clusters in a side
 // branch, the rest on warp groups, both persistent and fed by their queues.
-static mps_status batch_launch(mps_batch* B, int wps, const float* b, float* x,
+template <typename XT>
+static mps_status batch_launch(mps_batch* B, int wps, const float* b, XT* x,
                                double tol, int max_iter, int stall_window, BatchOut out,
-                               cudaStream_t s, int use_clusters) {
+                               cudaStream_t s, int use_clusters, double delta2 = 0.0) {
     BatchDev all = batch_view(B);
     const int nb = std::min(std::max(use_clusters, 0), B->n_big);
     MPS_CUDA(cudaMemsetAsync(B->d_queue, 0, 2 * sizeof(unsigned), s));
@@ -487,7 +536,7 @@ static mps_status batch_launch(mps_batch* B, int wps, const float* b, float* x,
         cfg.numAttrs = 1;
         cfg.gridDim = dim3(kClusterCTAs);
         int max_clusters = 0;
-        if (cudaOccupancyMaxActiveClusters(&max_clusters, batch_pcg_cluster, &cfg) != cudaSuccess ||
+        if (cudaOccupancyMaxActiveClusters(&max_clusters, batch_pcg_cluster<XT>, &cfg) != cudaSuccess ||
             max_clusters < 1)
             return cuda_fail(cudaGetLastError(), "cluster occupancy");
         // half of the GPU's clusters at most: the warp groups run beside them
@@ -496,19 +545,19 @@ static mps_status batch_launch(mps_batch* B, int wps, const float* b, float* x,
         cfg.stream = B->side;
         MPS_CUDA(cudaEventRecord(B->fork, s));
         MPS_CUDA(cudaStreamWaitEvent(B->side, B->fork, 0));
-        MPS_CUDA(cudaLaunchKernelEx(&cfg, batch_pcg_cluster, big, b, x, out, tol, max_iter, stall_window,
-                                    B->d_queue + 1));
+        MPS_CUDA(cudaLaunchKernelEx(&cfg, batch_pcg_cluster<XT>, big, b, x, out, tol, max_iter, stall_window,
+                                    B->d_queue + 1, delta2));
         MPS_CUDA(cudaEventRecord(B->join, B->side));
     }
     BatchDev small = all;
     small.order = all.order + nb;
     small.n_sys = all.n_sys - nb;
     if (small.n_sys > 0) {
-        BatchKernel k = batch_kernel(wps);
+        BatchKernel<XT> k = batch_kernel<XT>(wps);
         const int nt = batch_threads(wps);
         int per_sm = resident_ctas(reinterpret_cast<const void*>(k), nt, 0);
         const int grid = num_sms() * (per_sm > 0 ? per_sm : 1);
-        k<<<grid, nt, 0, s>>>(small, b, x, out, tol, max_iter, stall_window, B->d_queue);
+        k<<<grid, nt, 0, s>>>(small, b, x, out, tol, max_iter, stall_window, B->d_queue, delta2);
         MPS_CUDA(cudaGetLastError());
     }
     if (nb > 0) MPS_CUDA(cudaStreamWaitEvent(s, B->join, 0));
@@ -674,7 +723,7 @@ mps_status mps_batch_autotune(mps_batch* B, const float* d_b, double tol, int32_
         cfg.gridDim = dim3(kClusterCTAs);
         cfg.attrs = at;
         cfg.numAttrs = 1;
-        if (cudaOccupancyMaxActiveClusters(&max_clusters, batch_pcg_cluster, &cfg) != cudaSuccess) {
+        if (cudaOccupancyMaxActiveClusters(&max_clusters, batch_pcg_cluster<float>, &cfg) != cudaSuccess) {
             cudaGetLastError();
             max_clusters = 0;
         }
@@ -713,25 +762,31 @@ mps_status mps_batch_set_clusters(mps_batch* B, int32_t n_systems) {
     return MPS_OK;
 }
 
-mps_status mps_batch_cg(mps_batch* B, const float* d_b, float* d_x, double tol, int32_t max_iter,
-                        int32_t* d_iters, int32_t* d_converged, float* d_relres, cudaStream_t s) {
+}  // extern "C"
+
+// The whole batch is one CUDA-graph launch (queue reset + persistent
+// kernel), captured once per set of buffers and settings and reused.
+template <typename XT>
+static mps_status batch_solve(mps_batch* B, const float* d_b, XT* d_x, double tol, int32_t max_iter,
+                              double delta2, int32_t* d_iters, int32_t* d_converged, float* d_relres,
+                              cudaStream_t s) {
     if (!B || !d_b || !d_x || !d_iters || !d_converged || !d_relres)
         return fail(MPS_ERR_ARG, "null argument");
     BatchOut o{d_iters, d_converged, d_relres};
     tol = tol > 0 ? tol : 1e-6;
     max_iter = max_iter > 0 ? max_iter : 20000;
-    // The whole batch is one CUDA-graph launch (queue reset + persistent
-    // kernel), captured once per set of buffers and reused.
+    const int mode = std::is_same<XT, double>::value ? 1 : 0;
     const void* key[5] = {d_b, d_x, d_iters, d_converged, d_relres};
     bool same = B->exec && B->exec_wps == B->wps && B->exec_clusters == B->clusters;
     for (int i = 0; i < 5 && same; ++i) same = key[i] == B->exec_key[i];
-    same = same && B->exec_tol == tol && B->exec_max_iter == max_iter;
+    same = same && B->exec_tol == tol && B->exec_max_iter == max_iter && B->exec_mode == mode &&
+           B->exec_delta2 == delta2;
     if (!same) {
         if (B->exec) cudaGraphExecDestroy(B->exec);
         B->exec = nullptr;
         if (!B->cap) MPS_CUDA(cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking));
         MPS_CUDA(cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal));
-        mps_status st = batch_launch(B, B->wps, d_b, d_x, tol, max_iter, 400, o, B->cap, B->clusters);
+        mps_status st = batch_launch(B, B->wps, d_b, d_x, tol, max_iter, 400, o, B->cap, B->clusters, delta2);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(B->cap, &g);
         if (st != MPS_OK) {
@@ -747,9 +802,26 @@ mps_status mps_batch_cg(mps_batch* B, const float* d_b, float* d_x, double tol, 
         B->exec_clusters = B->clusters;
         B->exec_tol = tol;
         B->exec_max_iter = max_iter;
+        B->exec_mode = mode;
+        B->exec_delta2 = delta2;
     }
     MPS_CUDA(cudaGraphLaunch(B->exec, s));
     return MPS_OK;
+}
+
+extern "C" {
+
+mps_status mps_batch_cg(mps_batch* B, const float* d_b, float* d_x, double tol, int32_t max_iter,
+                        int32_t* d_iters, int32_t* d_converged, float* d_relres, cudaStream_t s) {
+    return batch_solve<float>(B, d_b, d_x, tol, max_iter, 0.0, d_iters, d_converged, d_relres, s);
+}
+
+mps_status mps_batch_cg_mixed(mps_batch* B, const float* d_b, double* d_x64, double tol, double inner_tol,
+                              int32_t max_iter, int32_t* d_iters, int32_t* d_converged, float* d_relres,
+                              cudaStream_t s) {
+    if (!(inner_tol > 0.0) || !(inner_tol < 1.0)) inner_tol = 1e-3;
+    return batch_solve<double>(B, d_b, d_x64, tol, max_iter, inner_tol * inner_tol, d_iters, d_converged,
+                               d_relres, s);
 }
 
 }  // extern "C"

@@ -622,6 +622,24 @@ public:
               "batch cg");
         return {it, cv, rr};
     }
+    std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> cg_mixed(torch::Tensor b, torch::Tensor x,
+                                                                     double tol, double inner_tol,
+                                                                     int64_t max_iter) {
+        c10::cuda::CUDAGuard g(device_);
+        auto bd = on_device(b, torch::kFloat32, "b");
+        TORCH_CHECK(bd.numel() == n_ && x.numel() == n_, "b and x need total_rows entries");
+        TORCH_CHECK(x.is_cuda() && x.is_contiguous() && x.scalar_type() == torch::kFloat64,
+                    "x must be a contiguous CUDA float64 tensor");
+        auto opt = bd.options();
+        auto it = torch::empty({n_sys_}, opt.dtype(torch::kInt32));
+        auto cv = torch::empty({n_sys_}, opt.dtype(torch::kInt32));
+        auto rr = torch::empty({n_sys_}, opt.dtype(torch::kFloat32));
+        check(mps_batch_cg_mixed(h_, bd.data_ptr<float>(), x.data_ptr<double>(), tol, inner_tol,
+                                 (int32_t)max_iter, it.data_ptr<int32_t>(), cv.data_ptr<int32_t>(),
+                                 rr.data_ptr<float>(), cur_stream()),
+              "batch cg_mixed");
+        return {it, cv, rr};
+    }
     int64_t warps_per_system() const { return mps_batch_warps_per_system(h_); }
     int64_t uses_clusters() const { return mps_batch_uses_clusters(h_); }
     void set_clusters(int64_t n) { check(mps_batch_set_clusters(h_, (int32_t)n), "set_clusters"); }
@@ -755,6 +773,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
              py::arg("max_iter") = 20000)
         .def("cg", &BatchSolver::cg, py::arg("b"), py::arg("x"), py::arg("tol") = 1e-6,
              py::arg("max_iter") = 20000)
+        .def("cg_mixed", &BatchSolver::cg_mixed, py::arg("b"), py::arg("x"), py::arg("tol") = 1e-6,
+             py::arg("inner_tol") = 1e-3, py::arg("max_iter") = 20000)
         .def_property_readonly("warps_per_system", &BatchSolver::warps_per_system)
         .def_property_readonly("uses_clusters", &BatchSolver::uses_clusters)
         .def("set_clusters", &BatchSolver::set_clusters, py::arg("n_systems"))
