@@ -76,7 +76,7 @@ def test_fsai_graph_matches_host_loop(mps, oracle):
     for host_loop in (False, True):
         x = torch.zeros(c.n, device="cuda")
         i = A.cgd(b.float(), x, tol=1e-6, max_iter=20000, precond="fsai", host_loop=host_loop)
-        assert i["converged"]
+        assert i["stop_rule_met"]
         x32.append((x, i))
     assert x32[0][1] == x32[1][1] and torch.equal(x32[0][0], x32[1][0])
 
@@ -103,7 +103,7 @@ def test_fsai_stall_fallback_graph_matches_host_loop(mps):
         x = torch.zeros(n, device="cuda")
         info = A.cgd(b, x, tol=1e-6, max_iter=20000, precond="fsai", stall_window=20,
                      host_loop=host_loop)
-        assert info["stalled"] and info["converged"]
+        assert info["stalled"] and info["stop_rule_met"]
         out.append((x, info))
     assert out[0][1] == out[1][1] and torch.equal(out[0][0], out[1][0])
 
