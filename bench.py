@@ -700,6 +700,18 @@ def c1_leg(dev, flush):
     x20 = torch.zeros(coo.n, device=dev)
     A.cgd(bt, x20, tol=1e-300, max_iter=20)
     xo20, _ = O.cg(Ao, b.astype(np.float64), tol=0.0, max_iter=20)
+    # the FP32 x of cgd cannot reach an FP64 true residual of 1e-6 here (its
+    # rounding floor is above it): mixed-precision CG (FP64 x) to 1e-6 beside
+    b64t = bt.double()
+    x64 = torch.zeros(coo.n, dtype=torch.float64, device=dev)
+    last_mp = {}
+
+    def solve_mp():
+        x64.zero_()
+        last_mp["info"] = A.cg_mixed(b64t, x64, tol=1e-6, inner_tol=1e-3, max_inner=2000)
+    solve_mp()
+    ms_mp = _event_ms(solve_mp, torch.cuda.current_stream(), 10, flush)
+    imp = last_mp["info"]
     xc = torch.zeros(coo.n, device=dev)
     ic = A.cgd(bt, xc, reference_compat=True)
     xoc, ioc = O.cg(Ao, b.astype(np.float64), compat=True)
@@ -709,6 +721,10 @@ def c1_leg(dev, flush):
             "oracle_fp64_iters": io["iters"], "true_resid": info["true_resid"],
             "converged_fp64": bool(info["converged"]),
             "iterate20_rel_diff_vs_oracle": _rel(x20.cpu().numpy(), xo20),
+            "mixed_precision_cg": {"ms": ms_mp, "iters": imp["inner_iters"],
+                                   "replacements": imp["outer_iters"],
+                                   "true_resid": imp["rel_resid"],
+                                   "converged_fp64": bool(imp["converged"])},
             "reference_compat": {"iters": ic["iters"], "oracle_iters": ioc["iters"],
                                  "true_resid": ic["true_resid"],
                                  "rel_diff_vs_oracle": _rel(xc.cpu().numpy(), xoc)},

@@ -362,7 +362,7 @@ static mps_status bcsr_solve(SolverKind kind, mps_bcsr* h, const float* b, float
     mps_solve_opts_default(&oo);
     if (o) oo = *o;
     oo.precond = MPS_PRECOND_NONE;
-    MPS_CUDA(h->H.ensure(h->A.padded));
+    MPS_CUDA(h->H.ensure(h->A.padded, s));
     MPS_CUDA(cudaMemsetAsync(h->A.d_err, 0, 4, s));
     BcsrOp op{&h->A};
     PrecondOps<BcsrOp> pc{};

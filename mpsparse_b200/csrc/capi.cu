@@ -42,6 +42,57 @@ cudaMemPool_t lib_pool() {
     return pool;
 }
 
+namespace {
+constexpr size_t kPinnedBlock = 4096;
+std::mutex g_pin_mu;
+std::vector<void*> g_pin_free;
+std::mutex g_stream_mu;
+std::map<int, std::vector<cudaStream_t>> g_stream_free;
+}  // namespace
+
+void* pinned_block_get(size_t bytes) {
+    if (bytes > kPinnedBlock) return nullptr;
+    void* p = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_pin_mu);
+        if (!g_pin_free.empty()) {
+            p = g_pin_free.back();
+            g_pin_free.pop_back();
+        }
+    }
+    if (!p && cudaMallocHost(&p, kPinnedBlock) != cudaSuccess) return nullptr;
+    std::memset(p, 0, kPinnedBlock);
+    return p;
+}
+void pinned_block_put(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_pin_mu);
+    g_pin_free.push_back(p);
+}
+cudaStream_t capture_stream_get() {
+    int d = 0;
+    cudaGetDevice(&d);
+    {
+        std::lock_guard<std::mutex> lock(g_stream_mu);
+        auto& v = g_stream_free[d];
+        if (!v.empty()) {
+            cudaStream_t s = v.back();
+            v.pop_back();
+            return s;
+        }
+    }
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    return s;
+}
+void capture_stream_put(cudaStream_t s) {
+    if (!s) return;
+    int d = 0;
+    cudaGetDevice(&d);
+    std::lock_guard<std::mutex> lock(g_stream_mu);
+    g_stream_free[d].push_back(s);
+}
+
 // Device attributes, cached per device (a process may drive several GPUs).
 static int device_attr(cudaDeviceAttr attr, std::atomic<int>* cache, int fallback) {
     int d = 0;
@@ -81,23 +132,23 @@ using namespace mps;
 namespace mps {
 
 void csr_free(CsrMat& m) {
-    if (m.rp) cudaFree(m.rp);
-    if (m.ci) cudaFree(m.ci);
-    if (m.v) cudaFree(m.v);
+    dev_free(m.rp);
+    dev_free(m.ci);
+    dev_free(m.v);
     spmv_plan_free(m.plan);
     m = CsrMat{};
 }
 
 mps_status alloc_csr(CsrMat& m, uint32_t n_rows, uint32_t n_cols, uint64_t nnz,
-                     unsigned* err) {
+                     unsigned* err, cudaStream_t s) {
     m.n_rows = n_rows;
     m.n_cols = n_cols;
     m.nnz = nnz;
     m.err = err;
     const size_t nz = nnz + kCsrPad;
-    MPS_CUDA(cudaMalloc(&m.rp, ((size_t)n_rows + 1 + kCsrPad) * sizeof(int32_t)));
-    MPS_CUDA(cudaMalloc(&m.ci, nz * sizeof(int32_t)));
-    MPS_CUDA(cudaMalloc(&m.v, nz * sizeof(float)));
+    MPS_CUDA(dev_alloc(&m.rp, ((size_t)n_rows + 1 + kCsrPad) * sizeof(int32_t), s));
+    MPS_CUDA(dev_alloc(&m.ci, nz * sizeof(int32_t), s));
+    MPS_CUDA(dev_alloc(&m.v, nz * sizeof(float), s));
     return MPS_OK;
 }
 
@@ -113,7 +164,7 @@ static mps_status check_shape(uint64_t nnz, uint32_t n_rows, uint32_t n_cols) {
 mps_status build_from_keys(CsrMat& m, const uint64_t* keys, const uint32_t* payload,
                                   uint64_t nnz, uint32_t n_rows, uint32_t n_cols, unsigned* d_err,
                                   cudaStream_t s, bool plan) {
-    mps_status st = alloc_csr(m, n_rows, n_cols, nnz, d_err);
+    mps_status st = alloc_csr(m, n_rows, n_cols, nnz, d_err, s);
     if (st != MPS_OK) return st;
     MPS_CUDA(cudaMemsetAsync(d_err, 0, sizeof(unsigned), s));
     MPS_CUDA(sort_to_csr(keys, payload, nnz, n_rows, n_cols, m.rp, m.ci, (uint32_t*)m.v, d_err, s));
@@ -164,7 +215,7 @@ mps_status mps_csr_create_from_keys(const uint64_t* d_keys, const float* d_vals,
     if (st != MPS_OK) return st;
     if (nnz && (!d_keys || !d_vals)) return fail(MPS_ERR_ARG, "keys / values are null");
     mps_csr* h = new mps_csr();
-    MPS_CUDA(cudaMalloc(&h->d_err, sizeof(unsigned)));
+    MPS_CUDA(dev_alloc(&h->d_err, sizeof(unsigned), stream));
     st = build_from_keys(h->A, d_keys, reinterpret_cast<const uint32_t*>(d_vals), nnz, n_rows,
                          n_cols, h->d_err, stream);
     if (st != MPS_OK) {
@@ -184,8 +235,8 @@ mps_status mps_csr_create_from_csr(const int32_t* d_row_ptr, const int32_t* d_co
     if (st != MPS_OK) return st;
     if (!d_row_ptr || (nnz && (!d_col_ind || !d_vals))) return fail(MPS_ERR_ARG, "null CSR array");
     mps_csr* h = new mps_csr();
-    MPS_CUDA(cudaMalloc(&h->d_err, sizeof(unsigned)));
-    st = alloc_csr(h->A, n_rows, n_cols, nnz, h->d_err);
+    MPS_CUDA(dev_alloc(&h->d_err, sizeof(unsigned), stream));
+    st = alloc_csr(h->A, n_rows, n_cols, nnz, h->d_err, stream);
     if (st != MPS_OK) {
         mps_csr_destroy(h);
         return st;
@@ -214,7 +265,7 @@ mps_status mps_test_sort_lookback_timeout(const uint64_t* d_keys, const float* d
     CsrMat m;
     unsigned* d_err = nullptr;
     MPS_CUDA(cudaMalloc(&d_err, sizeof(unsigned)));
-    st = alloc_csr(m, n_rows, n_cols, nnz, d_err);
+    st = alloc_csr(m, n_rows, n_cols, nnz, d_err, s);
     cudaError_t e = cudaSuccess;
     if (st == MPS_OK) {
         e = cudaMemsetAsync(d_err, 0, sizeof(unsigned), s);
@@ -237,8 +288,8 @@ mps_status mps_csr_destroy(mps_csr* h) {
     fsai_product_free(h);
     csr_free(h->G);
     csr_free(h->Gt);
-    if (h->vb) cudaFree(h->vb);
-    if (h->d_err) cudaFree(h->d_err);
+    dev_free(h->vb);
+    dev_free(h->d_err);
     fsai_work_free(h->fw);
     h->H.destroy();
     delete h;
@@ -362,7 +413,7 @@ mps_status mps_csr_spmv_dot(const mps_csr* hc, const float* d_x, const float* d_
                             double* d_dot, cudaStream_t s) {
     mps_csr* h = const_cast<mps_csr*>(hc);
     if (!h || !d_x || !d_w || !d_y || !d_dot) return fail(MPS_ERR_ARG, "null argument");
-    MPS_CUDA(h->H.ensure(h->A.n_rows));
+    MPS_CUDA(h->H.ensure(h->A.n_rows, s));
     MPS_CUDA(spmv_dot_launch(h->A, d_x, d_w, d_y, d_dot, h->H.ws.partials, h->H.ws.counters + 12, s));
     return MPS_OK;
 }
@@ -381,7 +432,7 @@ cudaError_t factor_plans_follow(mps_csr* h, cudaStream_t s) {
 }
 
 mps_status prepare_precond(mps_csr* h, const mps_solve_opts* o, cudaStream_t s) {
-    MPS_CUDA(h->H.ensure(h->A.n_rows));
+    MPS_CUDA(h->H.ensure(h->A.n_rows, s));
     const int pc = o ? o->precond : 0;
     if (pc != MPS_PRECOND_NONE && !(o && o->reference_compat)) {
         if (pc == MPS_PRECOND_FSAI && !h->has_fsai)
@@ -389,7 +440,7 @@ mps_status prepare_precond(mps_csr* h, const mps_solve_opts* o, cudaStream_t s) 
         if (pc != MPS_PRECOND_JACOBI && pc != MPS_PRECOND_FSAI)
             return fail(MPS_ERR_ARG, "unknown preconditioner");
         if (!h->H.dinv) {
-            MPS_CUDA(cudaMalloc(&h->H.dinv, h->H.ws.n_pad * sizeof(float)));
+            MPS_CUDA(dev_alloc(&h->H.dinv, h->H.ws.n_pad * sizeof(float), s));
             MPS_CUDA(cudaMemsetAsync(h->H.dinv, 0, h->H.ws.n_pad * sizeof(float), s));
             MPS_CUDA(diag_inv_launch(h->A, h->H.dinv, s));
             h->H.drop_graphs();   // graphs captured the previous (null) diagonal
@@ -445,7 +496,7 @@ mps_status mps_csr_set_fsai(mps_csr* h, const int32_t* d_g_row_ptr, const int32_
     fsai_work_free(h->fw);   // a network factor (if any) is replaced
     h->has_fsai = false;
     h->H.drop_graphs();
-    mps_status st = alloc_csr(h->G, n, n, g_nnz, h->d_err);
+    mps_status st = alloc_csr(h->G, n, n, g_nnz, h->d_err, s);
     if (st != MPS_OK) return st;
     MPS_CUDA(cudaMemcpyAsync(h->G.rp, d_g_row_ptr, ((size_t)n + 1) * 4, cudaMemcpyDeviceToDevice, s));
     MPS_CUDA(cudaMemcpyAsync(h->G.ci, d_g_col_ind, g_nnz * 4, cudaMemcpyDeviceToDevice, s));
@@ -537,7 +588,7 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
     SolverHost& H = h->H;
     const int n = (int)h->A.n_rows;
     if (bf16 && !h->vb) {
-        MPS_CUDA(cudaMalloc(&h->vb, (h->A.nnz + kCsrPad) * sizeof(__nv_bfloat16)));
+        MPS_CUDA(dev_alloc(&h->vb, (h->A.nnz + kCsrPad) * sizeof(__nv_bfloat16), s));
         MPS_CUDA(to_bf16_launch(h->A.v, h->vb, h->A.nnz, s));
     }
     double* scal = nullptr;   // [0] = ||b||^2, [1] = ||r||^2

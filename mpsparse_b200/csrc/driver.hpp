@@ -130,7 +130,9 @@ struct SolverHost {
         return Ctx{ws.sc, ws.partials, ws.counters, h, use, hif};
     }
 
-    cudaError_t ensure(size_t n_rows) {
+    // Work vectors, FP64 partial sums, counters and scalars (device, from the
+    // library pool, on stream s) and the pinned scalar mirrors.
+    cudaError_t ensure(size_t n_rows, cudaStream_t s) {
         n = (int)n_rows;
         const size_t n_pad = (n_rows + 3) & ~size_t(3);
         if (ws.sc && ws.n_pad >= n_pad) return cudaSuccess;
@@ -138,27 +140,32 @@ struct SolverHost {
         cudaError_t e;
         float* block = nullptr;
         const size_t nv = sizeof(ws.vec) / sizeof(ws.vec[0]);
-        if ((e = cudaMalloc(&block, nv * (n_pad ? n_pad : 4) * sizeof(float))) != cudaSuccess) return e;
-        if ((e = cudaMemset(block, 0, nv * (n_pad ? n_pad : 4) * sizeof(float))) != cudaSuccess) return e;
+        const size_t vbytes = nv * (n_pad ? n_pad : 4) * sizeof(float);
+        if ((e = dev_alloc(&block, vbytes, s)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(block, 0, vbytes, s)) != cudaSuccess) return e;
         for (size_t i = 0; i < nv; ++i) ws.vec[i] = block + i * (n_pad ? n_pad : 4);
-        if ((e = cudaMalloc(&ws.partials, 4 * kMaxPartials * sizeof(double))) != cudaSuccess) return e;
-        if ((e = cudaMalloc(&ws.counters, 16 * sizeof(unsigned))) != cudaSuccess) return e;
-        if ((e = cudaMemset(ws.counters, 0, 16 * sizeof(unsigned))) != cudaSuccess) return e;
-        if ((e = cudaMalloc(&ws.sc, sizeof(DevScalars))) != cudaSuccess) return e;
-        if ((e = cudaMemset(ws.sc, 0, sizeof(DevScalars))) != cudaSuccess) return e;
-        if ((e = cudaMalloc(&ws.d_params, sizeof(SolveParams))) != cudaSuccess) return e;
-        if ((e = cudaMallocHost(&ws.h_sc, sizeof(DevScalars))) != cudaSuccess) return e;
-        if ((e = cudaMallocHost(&h_params, sizeof(SolveParams))) != cudaSuccess) return e;
-        if ((e = cudaMallocHost(&h_aux, 4 * sizeof(double))) != cudaSuccess) return e;
-        if (!cap && (e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)) != cudaSuccess) return e;
-        if (!cap_branch && (e = cudaStreamCreateWithFlags(&cap_branch, cudaStreamNonBlocking)) != cudaSuccess)
-            return e;
+        if ((e = dev_alloc(&ws.partials, 4 * kMaxPartials * sizeof(double), s)) != cudaSuccess) return e;
+        if ((e = dev_alloc(&ws.counters, 16 * sizeof(unsigned), s)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(ws.counters, 0, 16 * sizeof(unsigned), s)) != cudaSuccess) return e;
+        if ((e = dev_alloc(&ws.sc, sizeof(DevScalars), s)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(ws.sc, 0, sizeof(DevScalars), s)) != cudaSuccess) return e;
+        if ((e = dev_alloc(&ws.d_params, sizeof(SolveParams), s)) != cudaSuccess) return e;
+        static_assert(sizeof(DevScalars) + sizeof(SolveParams) + 4 * sizeof(double) + 512 <= 4096,
+                      "scalar mirrors fit one pinned block");
+        unsigned char* pin = static_cast<unsigned char*>(pinned_block_get(4096));
+        if (!pin) return cudaErrorMemoryAllocation;
+        ws.h_sc = reinterpret_cast<DevScalars*>(pin);
+        h_params = reinterpret_cast<SolveParams*>(pin + ((sizeof(DevScalars) + 255) & ~size_t(255)));
+        h_aux = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(h_params) +
+                                          ((sizeof(SolveParams) + 255) & ~size_t(255)));
+        if (!cap && !(cap = capture_stream_get())) return cudaErrorUnknown;
+        if (!cap_branch && !(cap_branch = capture_stream_get())) return cudaErrorUnknown;
         ws.n_pad = n_pad ? n_pad : 4;
         return cudaSuccess;
     }
-    cudaError_t ensure_ir() {
+    cudaError_t ensure_ir(cudaStream_t s) {
         if (v64) return cudaSuccess;
-        return cudaMalloc(&v64, 2 * ws.n_pad * sizeof(double));
+        return dev_alloc(&v64, 2 * ws.n_pad * sizeof(double), s);
     }
     double* x64() const { return v64; }
     double* b64() const { return v64 + ws.n_pad; }
@@ -176,16 +183,14 @@ struct SolverHost {
     }
     void release() {
         drop_graphs();
-        if (ws.vec[0]) cudaFree(ws.vec[0]);
-        if (ws.partials) cudaFree(ws.partials);
-        if (ws.counters) cudaFree(ws.counters);
-        if (ws.sc) cudaFree(ws.sc);
-        if (ws.d_params) cudaFree(ws.d_params);
-        if (ws.h_sc) cudaFreeHost(ws.h_sc);
-        if (h_params) cudaFreeHost(h_params);
-        if (h_aux) cudaFreeHost(h_aux);
-        if (dinv) cudaFree(dinv);
-        if (v64) cudaFree(v64);
+        dev_free(ws.vec[0]);
+        dev_free(ws.partials);
+        dev_free(ws.counters);
+        dev_free(ws.sc);
+        dev_free(ws.d_params);
+        pinned_block_put(ws.h_sc);      // one block holds all three mirrors
+        dev_free(dinv);
+        dev_free(v64);
         v64 = nullptr;
         ws = Workspace{};
         h_params = nullptr;
@@ -194,8 +199,8 @@ struct SolverHost {
     }
     void destroy() {
         release();
-        if (cap) cudaStreamDestroy(cap);
-        if (cap_branch) cudaStreamDestroy(cap_branch);
+        capture_stream_put(cap);
+        capture_stream_put(cap_branch);
         cap = nullptr;
         cap_branch = nullptr;
     }
@@ -674,7 +679,7 @@ mps_status run_solve(SolverKind kind, const Op& op, const PrecondOps<Op>& pc, So
     const int precond = P.precond;
     MPS_CUDA(cudaMemcpyAsync(H.ws.d_params, H.h_params, sizeof(SolveParams), cudaMemcpyHostToDevice, s));
     if (ir) {
-        MPS_CUDA(H.ensure_ir());
+        MPS_CUDA(H.ensure_ir(s));
         MPS_CUDA(cudaMemcpyAsync(H.b64(), d_b64, (size_t)H.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     } else {
         MPS_CUDA(cudaMemcpyAsync(H.v(vB), d_b, (size_t)H.n * sizeof(float), cudaMemcpyDeviceToDevice, s));

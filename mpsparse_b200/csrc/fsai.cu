@@ -255,16 +255,16 @@ int g1(long n) {
 }  // namespace
 
 void fsai_work_free(FsaiWork& w) {
-    cudaFree(w.g_row);
-    cudaFree(w.g_aidx);
-    cudaFree(w.perm);
-    cudaFree(w.X);
-    cudaFree(w.out);
-    cudaFree(w.dgdo);
-    cudaFree(w.grad);
-    cudaFree(w.rinfo);
-    cudaFree(w.d_loss);
-    cudaFree(w.vec);
+    dev_free(w.g_row);
+    dev_free(w.g_aidx);
+    dev_free(w.perm);
+    dev_free(w.X);
+    dev_free(w.out);
+    dev_free(w.dgdo);
+    dev_free(w.grad);
+    dev_free(w.rinfo);
+    dev_free(w.d_loss);
+    dev_free(w.vec);
     w = FsaiWork{};
 }
 
@@ -303,20 +303,20 @@ static mps_status fsai_prepare(mps_csr* h, cudaStream_t s) {
     int nnz_g = 0;
     MPS_CUDA(cudaMemcpyAsync(&nnz_g, grp_tmp + n, 4, cudaMemcpyDeviceToHost, s));
     MPS_CUDA(cudaStreamSynchronize(s));
-    mps_status st = alloc_csr(h->G, n, n, (uint64_t)nnz_g, h->d_err);
+    mps_status st = alloc_csr(h->G, n, n, (uint64_t)nnz_g, h->d_err, s);
     if (st != MPS_OK) return st;
     MPS_CUDA(cudaMemcpyAsync(h->G.rp, grp_tmp, ((size_t)n + 1) * 4, cudaMemcpyDeviceToDevice, s));
     const size_t nz = (size_t)nnz_g + kCsrPad;
-    MPS_CUDA(cudaMalloc(&w.g_row, nz * 4));
-    MPS_CUDA(cudaMalloc(&w.g_aidx, nz * 4));
-    MPS_CUDA(cudaMalloc(&w.perm, nz * 4));
-    MPS_CUDA(cudaMalloc(&w.X, nz * kNF * 2));
-    MPS_CUDA(cudaMalloc(&w.out, nz * 4));
-    MPS_CUDA(cudaMalloc(&w.dgdo, nz * 4));
-    MPS_CUDA(cudaMalloc(&w.grad, nz * 4));
-    MPS_CUDA(cudaMalloc(&w.rinfo, (size_t)n * 48));
-    MPS_CUDA(cudaMalloc(&w.d_loss, 8));
-    MPS_CUDA(cudaMalloc(&w.vec, 6 * ((size_t)n + 4) * 4));
+    MPS_CUDA(dev_alloc(&w.g_row, nz * 4, s));
+    MPS_CUDA(dev_alloc(&w.g_aidx, nz * 4, s));
+    MPS_CUDA(dev_alloc(&w.perm, nz * 4, s));
+    MPS_CUDA(dev_alloc(&w.X, nz * kNF * 2, s));
+    MPS_CUDA(dev_alloc(&w.out, nz * 4, s));
+    MPS_CUDA(dev_alloc(&w.dgdo, nz * 4, s));
+    MPS_CUDA(dev_alloc(&w.grad, nz * 4, s));
+    MPS_CUDA(dev_alloc(&w.rinfo, (size_t)n * 48, s));
+    MPS_CUDA(dev_alloc(&w.d_loss, 8, s));
+    MPS_CUDA(dev_alloc(&w.vec, 6 * ((size_t)n + 4) * 4, s));
     g_fill_kernel<<<g1(n), 256, 0, s>>>(A.rp, A.ci, n, h->G.rp, h->G.ci, w.g_row, w.g_aidx);
     // (G's SpMV plan is built below, with G^T's, by factor_plans_follow)
     // G^T: sort (col << 32 | row) keys with the G index as payload
@@ -574,7 +574,7 @@ static mps_status probe_grad(mps_csr* h, const float* V, int k, uint64_t seed, i
     FsaiWork& w = h->fw;
     const int n = (int)h->A.n_rows;
     const long nz = (long)w.nnz_g;
-    MPS_CUDA(h->H.ensure(n));
+    MPS_CUDA(h->H.ensure(n, s));
     float* v = w.vec;
     float* u = v + (n + 4);
     float* ww = u + (n + 4);

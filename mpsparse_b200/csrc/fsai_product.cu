@@ -183,11 +183,11 @@ mps_status product_pattern(mps_csr* h, bool forced, cudaStream_t s) {
         return MPS_OK;
     }
     const size_t ez = (size_t)(E ? E : 1);
-    mps_status st = alloc_csr(h->M, (uint32_t)n, (uint32_t)n, nnz_m, h->d_err);
+    mps_status st = alloc_csr(h->M, (uint32_t)n, (uint32_t)n, nnz_m, h->d_err, s);
     if (st == MPS_OK) {
-        cudaError_t e = cudaMalloc(&fp.seg, ((size_t)nnz_m + 1) * 4);
-        if (e == cudaSuccess) e = cudaMalloc(&fp.pa, ez * 4);
-        if (e == cudaSuccess) e = cudaMalloc(&fp.pb, ez * 4);
+        cudaError_t e = dev_alloc(&fp.seg, ((size_t)nnz_m + 1) * 4, s);
+        if (e == cudaSuccess) e = dev_alloc(&fp.pa, ez * 4, s);
+        if (e == cudaSuccess) e = dev_alloc(&fp.pb, ez * 4, s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(h->M.rp, mrp, nb * 4, cudaMemcpyDeviceToDevice, s);
         if (e == cudaSuccess) e = cudaMemsetAsync(fp.seg, 0, ((size_t)nnz_m + 1) * 4, s);
         if (e == cudaSuccess) {
@@ -212,9 +212,9 @@ mps_status product_pattern(mps_csr* h, bool forced, cudaStream_t s) {
 
 void fsai_product_free(mps_csr* h) {
     FsaiProduct& fp = h->fp;
-    if (fp.seg) cudaFree(fp.seg);
-    if (fp.pa) cudaFree(fp.pa);
-    if (fp.pb) cudaFree(fp.pb);
+    dev_free(fp.seg);
+    dev_free(fp.pa);
+    dev_free(fp.pb);
     fp = FsaiProduct{};
     csr_free(h->M);
     if (h->use_m) h->H.drop_graphs();

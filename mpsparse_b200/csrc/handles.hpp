@@ -50,7 +50,8 @@ struct mps_csr {
 
 namespace mps {
 void csr_free(CsrMat& m);
-mps_status alloc_csr(CsrMat& m, uint32_t n_rows, uint32_t n_cols, uint64_t nnz, unsigned* err);
+mps_status alloc_csr(CsrMat& m, uint32_t n_rows, uint32_t n_cols, uint64_t nnz, unsigned* err,
+                     cudaStream_t s);
 mps_status build_from_keys(CsrMat& m, const uint64_t* keys, const uint32_t* payload, uint64_t nnz,
                            uint32_t n_rows, uint32_t n_cols, unsigned* d_err, cudaStream_t s, bool plan = true);
 mps_status prepare_precond(mps_csr* h, const mps_solve_opts* o, cudaStream_t s);

@@ -35,6 +35,32 @@ inline cudaError_t stream_alloc(T** p, size_t bytes, cudaStream_t s) {
     return cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, pool, s);
 }
 
+// Long-lived buffers of handles (matrix arrays, tile plans, solver and
+// factor work areas) come from the same pool: a fresh handle then costs no
+// driver allocation, and destroying one returns its memory to the pool
+// instead of unmapping it.  Allocated on the stream of the call that creates
+// the buffer (ordered before its first use there); dev_free synchronises the
+// device first, as cudaFree does, so no kernel on any stream still reads
+// the buffer when it goes back to the pool.
+template <class T>
+inline cudaError_t dev_alloc(T** p, size_t bytes, cudaStream_t s) {
+    return stream_alloc(p, bytes ? bytes : 16, s);
+}
+inline void dev_free(void* p) {
+    if (!p) return;
+    cudaDeviceSynchronize();
+    cudaFreeAsync(p, cudaStreamLegacy);
+}
+
+// Pinned host blocks (the solvers' scalar mirrors) and non-blocking capture
+// streams are kept per process / per device and handed to the next handle:
+// pinning host memory and creating streams cost far more than a solve's
+// other set-up.
+void* pinned_block_get(size_t bytes);    // up to 4 KB, zeroed
+void pinned_block_put(void* p);
+cudaStream_t capture_stream_get();       // on the current device
+void capture_stream_put(cudaStream_t s);
+
 // ---- device scalar block of one solve --------------------------------------
 // One instance lives in device memory per handle; the host mirrors it into
 // pinned memory at the end of a solve.

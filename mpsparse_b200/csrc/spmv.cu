@@ -107,8 +107,8 @@ int default_tile_nnz(uint64_t nnz, uint32_t n_rows) {
 }
 
 void spmv_plan_free(SpmvPlan& p) {
-    if (p.d_tile_row) cudaFree(p.d_tile_row);
-    if (p.d_meta) cudaFree(p.d_meta);
+    dev_free(p.d_tile_row);
+    dev_free(p.d_meta);
     p = SpmvPlan{};
 }
 
@@ -150,11 +150,11 @@ cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s, int stages,
     p.grid_s = p.ntiles < num_sms() * 6 ? p.ntiles : num_sms() * 6;
     if (p.grid_s < 1) p.grid_s = 1;
     // tile_row has 2 spare ints at the end for the plan statistics
-    cudaError_t e = cudaMalloc(&p.d_tile_row, (size_t)(p.ntiles + 3) * sizeof(int));
+    cudaError_t e = dev_alloc(&p.d_tile_row, (size_t)(p.ntiles + 3) * sizeof(int), s);
     if (e != cudaSuccess) return e;
-    e = cudaMalloc(&p.d_meta, (size_t)p.ntiles * sizeof(int4));
+    e = dev_alloc(&p.d_meta, (size_t)p.ntiles * sizeof(int4), s);
     if (e != cudaSuccess) {
-        cudaFree(p.d_tile_row);
+        dev_free(p.d_tile_row);
         return e;
     }
     plan_tiles_kernel<<<(p.ntiles + 1 + 255) / 256, 256, 0, s>>>(A.rp, (int)A.n_rows, tile_nnz,
@@ -170,8 +170,8 @@ cudaError_t spmv_plan_build(CsrMat& A, int tile_nnz, cudaStream_t s, int stages,
     if (e == cudaSuccess) e = cudaMemcpyAsync(stats, d_stats, sizeof(stats), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
-        cudaFree(p.d_tile_row);
-        cudaFree(p.d_meta);
+        dev_free(p.d_tile_row);
+        dev_free(p.d_meta);
         return e;
     }
     // Staging buffers sized to the largest tile (plus the 16-byte rounding
