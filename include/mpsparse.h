@@ -214,9 +214,19 @@ typedef struct {
     int32_t outer_iters;      /* refinement sweeps (restart) or residual replacements */
     int32_t inner_iters;      /* total inner CG iterations */
     int32_t converged;
-    int32_t reserved;
+    int32_t persistent;       /* 1: the solve ran as one persistent kernel
+                                 (see mps_csr_set_persistent) */
     double rel_resid;         /* FP64 true residual at exit */
 } mps_ir_info;
+
+/* Reliable-update FSAI-PCG in product form (M = G^T G) runs as ONE
+ * cooperative kernel -- one CTA per SM holding its rows of A and M in shared
+ * memory, grid barriers between the steps of an iteration -- whenever those
+ * rows fit (about 200 KB per SM; e.g. 2D 5-point systems up to ~300k rows);
+ * otherwise, or with enable = 0, as the graph of two kernels per iteration.
+ * Default 1.  Both forms compute the same iterates up to the grouping of the
+ * FP64 partial sums.  No reference counterpart. */
+mps_status mps_csr_set_persistent(mps_csr* A, int32_t enable);
 
 mps_status mps_csr_cg_mixed(mps_csr* A, const double* d_b, double* d_x, const mps_ir_opts* opts,
                             mps_ir_info* info, cudaStream_t stream);

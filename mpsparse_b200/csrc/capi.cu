@@ -282,12 +282,19 @@ mps_status mps_test_sort_lookback_timeout(const uint64_t* d_keys, const float* d
     return st;
 }
 
+mps_status mps_csr_set_persistent(mps_csr* h, int32_t enable) {
+    if (!h) return fail(MPS_ERR_ARG, "null handle");
+    h->persistent = enable ? 1 : 0;
+    return MPS_OK;
+}
+
 mps_status mps_csr_destroy(mps_csr* h) {
     if (!h) return MPS_OK;
     csr_free(h->A);
     fsai_product_free(h);
     csr_free(h->G);
     csr_free(h->Gt);
+    persist_plan_free(h);
     dev_free(h->vb);
     dev_free(h->d_err);
     fsai_work_free(h->fw);
@@ -625,7 +632,31 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
         ro.max_iter = cap > (1L << 30) ? (1 << 30) : (int)cap;
         mps_solve_info ii{};
         int rep = 0;
-        st = run_solve(kCG, inner, pc, H, nullptr, nullptr, &ro, &ii, s, 0, d_b, d_x, inner_tol, &rep, true);
+        bool persisted = false;
+        if (h->persistent && !io.host_loop && o.precond == MPS_PRECOND_FSAI && h->has_fsai && h->use_m) {
+            // one cooperative kernel for the whole solve when the rows of A
+            // and M fit one CTA per SM (fsai_persistent.cu); the parameters
+            // are the ones run_solve would upload
+            SolveParams& P = *H.h_params;
+            P.delta = inner_tol;
+            P.tol = tol;
+            P.omega = 0.01;
+            P.max_iter = ro.max_iter;
+            P.compat = 0;
+            P.precond = MPS_PRECOND_FSAI;
+            P.stall_window = ro.stall_window > 0 ? ro.stall_window : 400;
+            MPS_CUDA(cudaMemcpyAsync(H.ws.d_params, H.h_params, sizeof(SolveParams), cudaMemcpyHostToDevice, s));
+            const cudaError_t pe = persist_solve(h, d_b, d_x, s);
+            if (pe == cudaSuccess) {
+                MPS_CUDA(cudaMemcpyAsync(H.ws.h_sc, H.ws.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
+                persisted = true;
+            } else if (pe != cudaErrorNotSupported) {
+                cudaFreeAsync(scal, s);
+                return cuda_fail(pe, "persistent FSAI-PCG");
+            }
+        }
+        if (!persisted)
+            st = run_solve(kCG, inner, pc, H, nullptr, nullptr, &ro, &ii, s, 0, d_b, d_x, inner_tol, &rep, true);
         if (st == MPS_OK) {
             spmv_tiles<double, double, false, EpiResid64><<<h->A.plan.grid, kNT, smem, s>>>(
                 view, d_x, EpiResid64{d_b, r32, scal + 1, H.ws.counters + 14, H.ws.partials});
@@ -646,7 +677,7 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
             info->outer_iters = rep;
             info->inner_iters = ii.iters;
             info->converged = ii.converged && rel <= tol;
-            info->reserved = 0;
+            info->persistent = persisted ? 1 : 0;
             info->rel_resid = rel;
         }
         return st;
@@ -689,7 +720,7 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
         info->outer_iters = outer;
         info->inner_iters = inner_total;
         info->converged = converged;
-        info->reserved = 0;
+        info->persistent = 0;
         info->rel_resid = rel;
     }
     return st;

@@ -1,0 +1,489 @@
+// fsai_persistent.cu -- reliable-update FSAI-PCG (product form: z = M r with
+// M = G^T G) as one cooperative kernel, for matrices whose rows of A and M
+// fit the shared memory of one CTA per SM.
+//
+// The graph form of the same solve (driver.hpp, build_graph_nested) runs two
+// grid-wide kernels per iteration; on an L2-resident system (512^2: 1.3 M
+// nonzeros in A, 1.8 M in M) each kernel is bound by its fixed latency --
+// launch, tile copies, the last-CTA reduction -- not by bytes.  Here one CTA
+// per SM keeps its block of rows of A and of M in shared memory for the whole
+// solve and the two dependent steps of an iteration are separated by grid
+// barriers instead of kernel boundaries:
+//   step 1  p = z + beta p_old (formed on the fly), q = A p, p.q      -> alpha
+//   step 2  r' = r - alpha q (on the fly), z = M r', x += alpha p (FP64),
+//           r'.r', r'.D^-1 r', r'.z                                  -> beta
+// plus, when due, the residual replacement r = (float)(b - A x) in FP64 and
+// z = M r.  The arithmetic of every row is the graph form's (same products,
+// same order of additions, same FP32 / FP64 rounding points); only the FP64
+// sums of the per-CTA partials group differently.  Every CTA sums all
+// partials itself in one fixed order, so all CTAs take the same decisions
+// from the same bits and reach the same barriers.
+//
+// Safety: the launch is cooperative (the runtime refuses a grid that cannot
+// be co-resident); rows are assigned by blockIdx (no SM ids); every barrier
+// wait is bounded and a timeout raises an abort word that releases every
+// other waiter; the host checks the per-CTA shared-memory footprint before
+// choosing this form.
+#include <algorithm>
+#include <vector>
+
+#include "handles.hpp"
+
+namespace mps {
+namespace {
+
+constexpr int kPNT = 1024;                       // threads per CTA
+constexpr size_t kPSmemBudget = 200 * 1024;      // matrix rows per CTA (dynamic shared memory)
+constexpr unsigned kGridSpinLimit = 1u << 22;    // polls of one barrier wait (about a second)
+constexpr int kBarWords = 3;
+
+struct PersistDev {
+    const int* a_rp;
+    const int* a_ci;
+    const float* a_v;
+    const int* m_rp;
+    const int* m_ci;
+    const float* m_v;
+    const int* row_start;   // gridDim.x + 1 row boundaries
+    const float* dinv;      // Jacobi diagonal (fallback, and the r.D^-1 r sums)
+    const double* b;        // FP64 right-hand side
+    double* x;              // FP64 solution
+    float* r0;              // residual pair (current one by iteration parity)
+    float* r1;
+    float* p0;              // direction pair
+    float* p1;
+    float* q;
+    float* z;
+    double* part;           // partial sums: 4 slots x 3 sums x gridDim.x
+    unsigned* bar;          // [0] arrivals, [1] generation, [2] abort (zeroed before launch)
+    unsigned* err;
+    DevScalars* sc_out;     // the final scalars (read back by the host)
+    const SolveParams* prm;
+    int n;
+};
+
+struct PersistShared {
+    DevScalars S;                 // this CTA's copy of the solver scalars
+    double red[3 * (kPNT / 32)];
+    double tot[3];
+    unsigned gen;
+    int ok;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned ld_volatile_u32(const unsigned* p) {
+    return *reinterpret_cast<const volatile unsigned*>(p);
+}
+
+// Grid barrier: arrival counter + generation word.  Thread 0 arrives after a
+// release fence; the last arrival resets the counter and bumps the
+// generation; the others poll the generation (bounded; a raised abort word
+// ends the wait at once).  false: this CTA gave up (timeout or abort).
+__device__ bool grid_barrier(const PersistDev& P, PersistShared& sh) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned g = sh.gen;
+        int ok = 1;
+        __threadfence();
+        const unsigned t = atomicAdd(P.bar, 1u);
+        if (t == gridDim.x - 1) {
+            *reinterpret_cast<volatile unsigned*>(P.bar) = 0u;
+            __threadfence();
+            atomicAdd(P.bar + 1, 1u);
+        } else {
+            unsigned spins = 0;
+            while (ld_acquire_u32(P.bar + 1) == g) {
+                if (ld_volatile_u32(P.bar + 2)) {
+                    ok = 0;
+                    break;
+                }
+                if (++spins > kGridSpinLimit) {
+                    atomicOr(P.err, kErrTimeout);
+                    atomicExch(P.bar + 2, 1u);
+                    ok = 0;
+                    break;
+                }
+                if (spins > 64) __nanosleep(128);
+            }
+        }
+        __threadfence();
+        sh.gen = g + 1;
+        sh.ok = ok;
+    }
+    __syncthreads();
+    return sh.ok != 0;
+}
+
+// Block totals of NS per-thread FP64 sums -> slot, grid barrier, then every
+// CTA sums all CTAs' partials in one fixed order (warp 0: strided sequential
+// sums per lane, then the butterfly) into tot.
+template <int NS>
+__device__ bool reduce_all(const PersistDev& P, PersistShared& sh, int slot, double (&acc)[NS],
+                           double (&tot)[NS]) {
+    block_sum_n<kPNT, NS>(acc, sh.red);
+    const int G = gridDim.x;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int j = 0; j < NS; ++j) P.part[(slot * 3 + j) * G + blockIdx.x] = acc[j];
+    }
+    if (!grid_barrier(P, sh)) return false;
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            double s = 0.0;
+            for (int c = threadIdx.x; c < G; c += 32) s += __ldcg(P.part + (slot * 3 + j) * G + c);
+            s = warp_sum(s);
+            if (threadIdx.x == 0) sh.tot[j] = s;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NS; ++j) tot[j] = sh.tot[j];
+    return true;
+}
+
+// Row li of a block of a CSR held in shared memory times a gathered vector:
+// the products rounded to FP32 first, then added in column order (the tile
+// kernels' arithmetic).
+template <class F>
+__device__ __forceinline__ float row_f32(const int* rp, const int* ci, const float* v, int li, F gather) {
+    float s = 0.f;
+    const int e = rp[li + 1];
+    for (int k = rp[li]; k < e; ++k) s = __fadd_rn(s, __fmul_rn(v[k], gather(ci[k])));
+    return s;
+}
+
+__global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
+    extern __shared__ __align__(16) unsigned char psmem[];
+    __shared__ PersistShared sh;
+    const int tid = threadIdx.x;
+    const int r0 = P.row_start[blockIdx.x], r1 = P.row_start[blockIdx.x + 1];
+    const int R = r1 - r0;
+    const int a0 = P.a_rp[r0], na = P.a_rp[r1] - a0;
+    const int m0 = P.m_rp[r0], nm = P.m_rp[r1] - m0;
+    // shared layout: arp[R+1] | mrp[R+1] | aci[na] | mci[nm] | av[na] | mv[nm]
+    int* arp = reinterpret_cast<int*>(psmem);
+    int* mrp = arp + (R + 1);
+    int* aci = mrp + (R + 1);
+    int* mci = aci + na;
+    float* av = reinterpret_cast<float*>(mci + nm);
+    float* mv = av + na;
+    for (int i = tid; i <= R; i += kPNT) {
+        arp[i] = P.a_rp[r0 + i] - a0;
+        mrp[i] = P.m_rp[r0 + i] - m0;
+    }
+    for (int k = tid; k < na; k += kPNT) {
+        aci[k] = P.a_ci[a0 + k];
+        av[k] = P.a_v[a0 + k];
+    }
+    for (int k = tid; k < nm; k += kPNT) {
+        mci[k] = P.m_ci[m0 + k];
+        mv[k] = P.m_v[m0 + k];
+    }
+    if (tid == 0) {
+        sh.gen = 0;
+        sh.ok = 1;
+        sh.S = DevScalars{};
+    }
+    __syncthreads();
+    DevScalars& S = sh.S;
+    const Ctx cx{&sh.S, nullptr, nullptr, {}, 0, {}};
+    const float* dinv = P.dinv;
+
+    // ---- start: x = 0, r = (float)b; ||b||^2 -----------------------------
+    const int mode0 = P.prm->precond;
+    {
+        double acc[2] = {0.0, 0.0};
+        for (int li = tid; li < R; li += kPNT) {
+            const int i = r0 + li;
+            const double bd = __ldg(P.b + i);
+            const float bf = (float)bd;
+            P.x[i] = 0.0;
+            P.r0[i] = bf;
+            if (mode0 == 1) {
+                const float zz = bf * dinv[i];
+                acc[1] += (double)bf * bf * dinv[i];
+                P.p0[i] = zz;
+            }
+            acc[0] += bd * bd;
+        }
+        double tot[2];
+        if (!reduce_all<2>(P, sh, 0, acc, tot)) goto out;
+        if (tid == 0) cg_init_scalars(cx, P.prm, P.n, mode0, tot[0], tot[1]);
+        __syncthreads();
+    }
+    // z = M r, r.z -> the first direction (fsai_beta restarts it)
+    if (!S.done && S.mode == 2) {
+        double acc[1] = {0.0};
+        const float* rc = P.r0;
+        for (int li = tid; li < R; li += kPNT) {
+            const float s = row_f32(mrp, mci, mv, li, [&](int c) { return __ldcg(rc + c); });
+            const int i = r0 + li;
+            P.z[i] = s;
+            acc[0] += (double)__ldcg(rc + i) * (double)s;
+        }
+        double tot[1];
+        if (!reduce_all<1>(P, sh, 1, acc, tot)) goto out;
+        if (tid == 0) fsai_beta(&S, tot[0]);
+        __syncthreads();
+    }
+
+    while (!S.done) {
+        if (!S.replace) {
+            // ---- step 1: p = z + beta p_old on the fly, q = A p, p.q -------
+            {
+                const bool odd = S.iter & 1;
+                float* pn = odd ? P.p1 : P.p0;
+                const float* po = odd ? P.p0 : P.p1;
+                const float* rc = odd ? P.r1 : P.r0;
+                const float beta = (float)S.beta;
+                const bool jac = S.mode == 1;
+                auto dir = [&](int c) {
+                    const float zc = jac ? __ldcg(rc + c) * __ldg(dinv + c) : __ldcg(P.z + c);
+                    return beta != 0.f ? fmaf(beta, __ldcg(po + c), zc) : zc;
+                };
+                double acc[1] = {0.0};
+                for (int li = tid; li < R; li += kPNT) {
+                    const float s = row_f32(arp, aci, av, li, dir);
+                    const int i = r0 + li;
+                    const float pv = dir(i);
+                    pn[i] = pv;
+                    P.q[i] = s;
+                    acc[0] += (double)pv * (double)s;
+                }
+                double tot[1];
+                if (!reduce_all<1>(P, sh, 0, acc, tot)) goto out;
+                if (tid == 0) {
+                    const double pq = tot[0];
+                    S.pq = pq;
+                    if (!(pq > 0.0) || !isfinite(pq)) {
+                        S.breakdown = 1;
+                        S.done = 1;
+                        S.alpha = 0.0;
+                    } else {
+                        S.alpha = S.rz / pq;
+                    }
+                }
+                __syncthreads();
+                if (S.done) break;
+            }
+            // ---- step 2: r' = r - alpha q on the fly, z = M r', x += alpha p
+            {
+                const bool odd = S.iter & 1;
+                const float* rc = odd ? P.r1 : P.r0;
+                float* rn = odd ? P.r0 : P.r1;
+                const float* pc = odd ? P.p1 : P.p0;
+                const double a = S.alpha;
+                const float af = (float)a;
+                auto res = [&](int c) { return fmaf(-af, __ldcg(P.q + c), __ldcg(rc + c)); };
+                double acc[3] = {0.0, 0.0, 0.0};
+                for (int li = tid; li < R; li += kPNT) {
+                    const float s = row_f32(mrp, mci, mv, li, res);
+                    const int i = r0 + li;
+                    const float rv = res(i);
+                    rn[i] = rv;
+                    P.x[i] = fma(a, (double)__ldcg(pc + i), __ldcg(P.x + i));
+                    P.z[i] = s;
+                    acc[0] += (double)rv * rv;
+                    acc[1] += (double)rv * rv * dinv[i];
+                    acc[2] += (double)rv * (double)s;
+                }
+                double tot[3];
+                if (!reduce_all<3>(P, sh, 1, acc, tot)) goto out;
+                if (tid == 0) {
+                    cg_finalize_ir(&S, tot[0], tot[1]);
+                    if (!S.replace && !S.done && S.mode == 2) fsai_beta(&S, tot[2]);
+                }
+                __syncthreads();
+            }
+        } else {
+            // ---- replacement: r = (float)(b - A x) in FP64 ------------------
+            {
+                float* rw = (S.iter & 1) ? P.r1 : P.r0;
+                double acc[2] = {0.0, 0.0};
+                for (int li = tid; li < R; li += kPNT) {
+                    double s = 0.0;
+                    const int e = arp[li + 1];
+                    for (int k = arp[li]; k < e; ++k)
+                        s = __dadd_rn(s, __dmul_rn((double)av[k], __ldcg(P.x + aci[k])));
+                    const int i = r0 + li;
+                    const double rt = __ldg(P.b + i) - s;
+                    const float rf = (float)rt;
+                    rw[i] = rf;
+                    acc[0] += rt * rt;
+                    acc[1] += (double)rf * rf * dinv[i];
+                }
+                double tot[2];
+                if (!reduce_all<2>(P, sh, 2, acc, tot)) goto out;
+                if (tid == 0) {
+                    S.replace = 0;
+                    ++S.replaced;
+                    const double rr = tot[0];
+                    S.rr = rr;
+                    S.rr_ref = rr;
+                    if (!isfinite(rr)) {
+                        S.breakdown = 1;
+                        S.done = 1;
+                    } else if (rr <= S.tol2) {
+                        S.converged = 1;
+                        S.done = 1;
+                    } else if (S.iter >= S.max_iter) {
+                        S.done = 1;
+                    } else {
+                        cg_direction(&S, rr, tot[1]);
+                        if (S.mode == 2) S.refresh = 1;
+                    }
+                }
+                __syncthreads();
+            }
+            // z = M r of the replaced residual
+            if (!S.done && S.mode == 2 && S.refresh) {
+                const float* rc = (S.iter & 1) ? P.r1 : P.r0;
+                double acc[1] = {0.0};
+                for (int li = tid; li < R; li += kPNT) {
+                    const float s = row_f32(mrp, mci, mv, li, [&](int c) { return __ldcg(rc + c); });
+                    const int i = r0 + li;
+                    P.z[i] = s;
+                    acc[0] += (double)__ldcg(rc + i) * (double)s;
+                }
+                double tot[1];
+                if (!reduce_all<1>(P, sh, 3, acc, tot)) goto out;
+                if (tid == 0) {
+                    S.refresh = 0;
+                    fsai_beta(&S, tot[0]);
+                }
+                __syncthreads();
+            }
+        }
+    }
+out:
+    if (tid == 0 && blockIdx.x == 0) {
+        if (!sh.ok) S.err |= kErrTimeout;
+        *P.sc_out = S;
+    }
+}
+
+}  // namespace
+
+// Row blocks of A and M for one CTA per SM, balanced by their shared-memory
+// bytes; false when a block would not fit (the graph form is used then).
+cudaError_t persist_plan_build(mps_csr* h, cudaStream_t s) {
+    PersistPlan& pp = h->pp;
+    pp.state = -1;
+    if (!h->use_m || !h->M.rp || h->A.n_rows != h->M.n_rows) return cudaSuccess;
+    const int n = (int)h->A.n_rows;
+    std::vector<int> arp(n + 1), mrp(n + 1);
+    cudaError_t e = cudaMemcpyAsync(arp.data(), h->A.rp, (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(mrp.data(), h->M.rp, (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaFuncSetAttribute(fsai_pcg_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kPSmemBudget);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fsai_pcg_persistent, kPNT, kPSmemBudget);
+    if (e != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        return cudaSuccess;   // not eligible
+    }
+    // at least 128 rows per CTA; one CTA per SM at most
+    int grid = std::min(num_sms(), std::max(1, n / 128));
+    // bytes of row i: two row-pointer words + 8 per nonzero of A and of M
+    auto bytes_to = [&](int i) {   // rows [0, i)
+        return 8.0 * i + 8.0 * ((double)arp[i] + (double)mrp[i]);
+    };
+    const double total = bytes_to(n);
+    std::vector<int> start(grid + 1);
+    start[0] = 0;
+    start[grid] = n;
+    int lo = 0;
+    for (int c = 1; c < grid; ++c) {
+        const double target = total * c / grid;
+        int a = lo, bnd = n;
+        while (a < bnd) {   // first row whose prefix reaches the target
+            const int mid = a + (bnd - a) / 2;
+            if (bytes_to(mid) < target) a = mid + 1;
+            else bnd = mid;
+        }
+        start[c] = a;
+        lo = a;
+    }
+    size_t worst = 0;
+    for (int c = 0; c < grid; ++c) {
+        const int rows = start[c + 1] - start[c];
+        if (rows < 0) return cudaSuccess;
+        const size_t b = 4 * (2 * (size_t)rows + 2) +
+                         8 * ((size_t)(arp[start[c + 1]] - arp[start[c]]) +
+                              (size_t)(mrp[start[c + 1]] - mrp[start[c]]));
+        worst = std::max(worst, b);
+    }
+    if (worst > kPSmemBudget) return cudaSuccess;   // rows do not fit: not eligible
+    dev_free(pp.d_row_start);
+    pp.d_row_start = nullptr;
+    // grid + 1 boundaries, then the barrier's three words
+    e = dev_alloc(&pp.d_row_start, (size_t)(grid + 1 + kBarWords) * 4, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(pp.d_row_start, start.data(), (size_t)(grid + 1) * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    pp.grid = grid;
+    pp.smem = ((worst + 15) / 16) * 16;
+    pp.state = 1;
+    return cudaSuccess;
+}
+
+void persist_plan_free(mps_csr* h) {
+    dev_free(h->pp.d_row_start);
+    h->pp = PersistPlan{};
+}
+
+// The reliable-update FSAI-PCG solve (x64 = FP64 solution, b64 = FP64 rhs,
+// both of n entries) as one cooperative launch; the final scalars land in
+// H.ws.sc like the graph form's.  Returns cudaErrorNotSupported when the
+// plan says the matrix is not eligible.
+cudaError_t persist_solve(mps_csr* h, const double* b64, double* x64, cudaStream_t s) {
+    if (h->pp.state == 0) {
+        const cudaError_t e = persist_plan_build(h, s);
+        if (e != cudaSuccess) return e;
+    }
+    if (h->pp.state != 1) return cudaErrorNotSupported;
+    SolverHost& H = h->H;
+    PersistDev P{};
+    P.a_rp = h->A.rp;
+    P.a_ci = h->A.ci;
+    P.a_v = h->A.v;
+    P.m_rp = h->M.rp;
+    P.m_ci = h->M.ci;
+    P.m_v = h->M.v;
+    P.row_start = h->pp.d_row_start;
+    P.dinv = H.dinv;
+    P.b = b64;
+    P.x = x64;
+    P.r0 = H.v(vR);
+    P.r1 = H.v(vR1);
+    P.p0 = H.v(vP);
+    P.p1 = H.v(vP1);
+    P.q = H.v(vQ);
+    P.z = H.v(vW);
+    P.part = H.ws.partials;
+    P.bar = reinterpret_cast<unsigned*>(h->pp.d_row_start + h->pp.grid + 1);
+    P.err = h->d_err;
+    P.sc_out = H.ws.sc;
+    P.prm = H.ws.d_params;
+    P.n = (int)h->A.n_rows;
+    static_assert(4 * 3 * 1024 <= 4 * kMaxPartials, "partial slots");
+    cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(fsai_pcg_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)h->pp.smem);
+    if (e != cudaSuccess) return e;
+    void* args[] = {&P};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(fsai_pcg_persistent), dim3(h->pp.grid),
+                                       dim3(kPNT), args, h->pp.smem, s);
+}
+
+}  // namespace mps

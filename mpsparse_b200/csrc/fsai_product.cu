@@ -216,6 +216,7 @@ void fsai_product_free(mps_csr* h) {
     dev_free(fp.pa);
     dev_free(fp.pb);
     fp = FsaiProduct{};
+    persist_plan_free(h);
     csr_free(h->M);
     if (h->use_m) h->H.drop_graphs();
     h->use_m = false;

@@ -32,6 +32,15 @@ struct FsaiProduct {
     int32_t* pb = nullptr;     // index of g_kj
 };
 
+// Row blocks of the persistent FSAI-PCG form (fsai_persistent.cu): one CTA
+// per SM holds its rows of A and M in shared memory.
+struct PersistPlan {
+    int state = 0;                 // 0 not built, 1 eligible, -1 rows do not fit
+    int grid = 0;
+    size_t smem = 0;               // dynamic shared memory per CTA
+    int* d_row_start = nullptr;    // grid + 1 row boundaries, then the barrier's words
+};
+
 }  // namespace mps
 
 struct mps_csr {
@@ -46,6 +55,8 @@ struct mps_csr {
     mps::FsaiProduct fp;
     int32_t fsai_apply = 0;    // MPS_FSAI_APPLY_*
     bool use_m = false;        // PCG applies z = M r (else z = G^T (G r))
+    mps::PersistPlan pp;       // persistent form of reliable-update FSAI-PCG
+    int32_t persistent = 1;    // 1: use the persistent form when the rows fit
 };
 
 namespace mps {
@@ -66,4 +77,8 @@ void fsai_product_free(mps_csr* h);
 // Status of a device error word (range / timeout bits) after `what`.
 mps_status device_error(unsigned err, const char* what);
 mps_status fsai_factor_changed(mps_csr* h, cudaStream_t s);
+// Persistent FSAI-PCG (fsai_persistent.cu): plan (built on first use, freed
+// with M's pattern) and the solve; cudaErrorNotSupported: not eligible.
+void persist_plan_free(mps_csr* h);
+cudaError_t persist_solve(mps_csr* h, const double* b64, double* x64, cudaStream_t s);
 }  // namespace mps

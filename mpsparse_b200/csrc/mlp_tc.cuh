@@ -277,7 +277,9 @@ struct MlpBwdSmem {
     MlpPacked w;
     __nv_bfloat16 xd[kMlpRows * 128];   // [x (16) | 0 (48) | dz1 (64)], canonical K = 128
     __nv_bfloat16 hd[kMlpRows * 128];   // [h1 (64) | dz2 (64)],          canonical K = 128
-    float gb1[kNH], gb2[kNH], gw3[kNH], gb3;
+    // per-warp sums over the CTA's rows (each lane owns two columns of its warp's row)
+    float gb1[kMlpThreads / 32][kNH], gb2[kMlpThreads / 32][kNH], gw3[kMlpThreads / 32][kNH];
+    float gb3[kMlpThreads / 32];
     unsigned long long bar;
     unsigned taddr;
     int abort;
@@ -286,13 +288,30 @@ struct MlpBwdSmem {
 // (about 85 KB) admits no third.
 constexpr int kMlpBwdCtasPerSm = 2;
 
-// Warp-reduce 64 per-row values and add them to a shared accumulator.
-__device__ __forceinline__ void warp_accum64(const float* v, float* acc) {
+// Sum 64 per-row values over the warp's 32 rows by a butterfly
+// reduce-scatter: in each of five rounds a lane keeps half of its values and
+// sends the other half to its partner (32 + 16 + 8 + 4 + 2 independent
+// shuffles in all, against 5 dependent ones for each of 64 separate
+// reductions), ending with the totals of columns 2*lane and 2*lane + 1, which
+// it adds to its warp's row of the accumulator (no atomics).  v is consumed.
+template <int N>
+__device__ __forceinline__ void rs_round(float* v, bool upper, int w) {
 #pragma unroll
-    for (int i = 0; i < 64; ++i) {
-        const float s = warp_sum(v[i]);
-        if ((threadIdx.x & 31) == 0) atomicAdd(&acc[i], s);
+    for (int i = 0; i < N / 2; ++i) {
+        const float keep = upper ? v[i + N / 2] : v[i];
+        const float send = upper ? v[i] : v[i + N / 2];
+        v[i] = keep + __shfl_xor_sync(kFull, send, w);
     }
+}
+__device__ __forceinline__ void warp_accum64(float* v, float* acc_row) {
+    const int lane = threadIdx.x & 31;
+    rs_round<64>(v, lane & 16, 16);
+    rs_round<32>(v, lane & 8, 8);
+    rs_round<16>(v, lane & 4, 4);
+    rs_round<8>(v, lane & 2, 2);
+    rs_round<4>(v, lane & 1, 1);
+    acc_row[2 * lane] += v[0];
+    acc_row[2 * lane + 1] += v[1];
 }
 
 // grad (FP32, parameter layout W1, b1, W2, b2, w3, b3) += d loss / d params
@@ -304,9 +323,10 @@ mlp_backward_tc(const MlpPacked* __restrict__ wg, const __nv_bfloat16* __restric
     MlpBwdSmem& S = *reinterpret_cast<MlpBwdSmem*>(mlp_smem);
     const int tid = threadIdx.x, warp = tid >> 5;
     load_packed(wg, &S.w);
-    for (int i = tid; i < kNH; i += kMlpThreads) S.gb1[i] = S.gb2[i] = S.gw3[i] = 0.f;
+    for (int i = tid; i < (kMlpThreads / 32) * kNH; i += kMlpThreads)
+        (&S.gb1[0][0])[i] = (&S.gb2[0][0])[i] = (&S.gw3[0][0])[i] = 0.f;
+    if (tid < kMlpThreads / 32) S.gb3[tid] = 0.f;
     if (tid == 0) {
-        S.gb3 = 0.f;
         mbar_init(&S.bar, 1);
         S.abort = 0;
         fence_mbar_init();
@@ -392,13 +412,13 @@ mlp_backward_tc(const MlpPacked* __restrict__ wg, const __nv_bfloat16* __restric
                 h2[i] = live ? d * gelu_f(z) : 0.f;              // dw3 contribution
                 v[i] = live ? d * S.w.w3[i] * gelu_d(z) : 0.f;   // dz2
             }
-            warp_accum64(h2, S.gw3);
-            warp_accum64(v, S.gb2);
-            const float sd = warp_sum(d);
-            if ((tid & 31) == 0) atomicAdd(&S.gb3, sd);
-        }
 #pragma unroll
-        for (int c = 0; c < 8; ++c) store_bf16x8(S.hd + canon(tid, 64 + 8 * c, 128), v + 8 * c);
+            for (int c = 0; c < 8; ++c) store_bf16x8(S.hd + canon(tid, 64 + 8 * c, 128), v + 8 * c);
+            warp_accum64(h2, S.gw3[warp]);
+            warp_accum64(v, S.gb2[warp]);
+            const float sd = warp_sum(d);
+            if ((tid & 31) == 0) S.gb3[warp] += sd;
+        }
         fence_proxy_async();
         tc_fence_before();
         __syncthreads();
@@ -424,9 +444,9 @@ mlp_backward_tc(const MlpPacked* __restrict__ wg, const __nv_bfloat16* __restric
         tmem_ld64(T_D2 + lane_off, v);                    // dh1
 #pragma unroll
         for (int i = 0; i < 64; ++i) v[i] = live ? v[i] * gelu_d(z1[i] + S.w.b1[i]) : 0.f;
-        warp_accum64(v, S.gb1);
 #pragma unroll
         for (int c = 0; c < 8; ++c) store_bf16x8(S.xd + canon(tid, 64 + 8 * c, 128), v + 8 * c);
+        warp_accum64(v, S.gb1[warp]);
         fence_proxy_async();
         tc_fence_before();
         __syncthreads();
@@ -469,11 +489,23 @@ mlp_backward_tc(const MlpPacked* __restrict__ wg, const __nv_bfloat16* __restric
         }
         __syncthreads();
         for (int i = tid; i < kNH; i += kMlpThreads) {
-            atomicAdd(&gb1[i], S.gb1[i]);
-            atomicAdd(&gb2[i], S.gb2[i]);
-            atomicAdd(&gw3[i], S.gw3[i]);
+            float a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll
+            for (int k = 0; k < kMlpThreads / 32; ++k) {
+                a1 += S.gb1[k][i];
+                a2 += S.gb2[k][i];
+                a3 += S.gw3[k][i];
+            }
+            atomicAdd(&gb1[i], a1);
+            atomicAdd(&gb2[i], a2);
+            atomicAdd(&gw3[i], a3);
         }
-        if (tid == 0) atomicAdd(gb3, S.gb3);
+        if (tid == 0) {
+            float a = 0.f;
+#pragma unroll
+            for (int k = 0; k < kMlpThreads / 32; ++k) a += S.gb3[k];
+            atomicAdd(gb3, a);
+        }
     }
     tc_fence_before();
     __syncthreads();

@@ -314,8 +314,10 @@ public:
         d["inner_iters"] = info.inner_iters;
         d["converged"] = (bool)info.converged;
         d["rel_resid"] = info.rel_resid;
+        d["persistent"] = (bool)info.persistent;
         return d;
     }
+    void set_persistent(bool enable) { check(mps_csr_set_persistent(h_, enable ? 1 : 0), "set_persistent"); }
 
     void set_fsai(torch::Tensor rp, torch::Tensor ci, torch::Tensor v) {
         c10::cuda::CUDAGuard g(device_);
@@ -738,6 +740,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         .def("attach_fsai", &CsrTensor::attach_fsai, py::arg("model"))
         .def("set_fsai_apply", &CsrTensor::set_fsai_apply, py::arg("mode"))
         .def("fsai_apply", &CsrTensor::fsai_apply)
+        .def("set_persistent", &CsrTensor::set_persistent, py::arg("enable"),
+             "reliable-update FSAI-PCG as one persistent kernel when the rows fit (default on)")
         .def("fsai_product", &CsrTensor::fsai_product)
         .def("fsai_train_step", &CsrTensor::fsai_train_step, py::arg("model"), py::arg("n_probes") = 4,
              py::arg("extra") = py::none(), py::arg("lr") = 1e-3, py::arg("seed") = 0)

@@ -68,6 +68,7 @@ def test_product_and_split_reach_the_same_solution(mps, oracle):
 def test_product_graph_matches_host_loop(mps):
     c, A = _learned(mps, 160, 120, 22)
     A.set_fsai_apply("product")
+    A.set_persistent(False)            # the graph form (the persistent one: test_gpu_persistent)
     b = torch.from_numpy(W.rhs(c.n, 5).astype(np.float64)).cuda()
     xs, infos = [], []
     for host_loop in (False, True):

@@ -60,6 +60,7 @@ def test_fsai_graph_matches_host_loop(mps, oracle):
     e = torch.empty(0)
     A = mps.spmv.csr_tensor(torch.from_numpy(c.keys()), torch.from_numpy(c.vals), e, e, e, c.n, c.n)
     LearnedFsai.load().attach(A)
+    A.set_persistent(False)            # the graph form (the persistent one: test_gpu_persistent)
     b = torch.from_numpy(W.rhs(c.n, 4).astype(np.float64)).cuda()
     xs, infos = [], []
     for host_loop in (False, True):

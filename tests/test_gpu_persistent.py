@@ -1,0 +1,94 @@
+"""Reliable-update FSAI-PCG as one persistent cooperative kernel
+(fsai_persistent.cu) against the graph form of the same solve and the FP64
+oracle.
+
+The two forms compute every row identically; only the FP64 sums of the
+per-CTA partials group differently, so their iterates agree to rounding
+early on and their iteration counts within a few percent at the end.
+Tolerances: first iterates within 1e-6 relative of the graph form's;
+final answers by the FP64 true residual (<= tol, checked by the oracle);
+solutions of the two forms within 100 * tol of each other."""
+import numpy as np
+import pytest
+import torch
+
+from mpsparse_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _learned(mps, nx, ny, seed):
+    from mpsparse_b200.fsai import LearnedFsai
+    c = W.lognormal_diffusion_2d(nx, ny, 1.5, 8.0, seed)
+    e = torch.empty(0)
+    A = mps.spmv.csr_tensor(torch.from_numpy(c.keys()), torch.from_numpy(c.vals), e, e, e, c.n, c.n)
+    LearnedFsai.load().attach(A)
+    A.set_fsai_apply("product")
+    return c, A
+
+
+def _solve(A, b, persistent, **kw):
+    A.set_persistent(persistent)
+    x = torch.zeros(b.numel(), dtype=torch.float64, device="cuda")
+    info = A.cg_mixed(b, x, precond="fsai", **kw)
+    return x, info
+
+
+@pytest.mark.parametrize("shape", [(160, 120), (64, 64), (512, 512)])
+def test_persistent_matches_graph_form(mps, oracle, shape):
+    c, A = _learned(mps, *shape, 31)
+    b = torch.from_numpy(W.rhs(c.n, 8).astype(np.float64)).cuda()
+    xg, ig = _solve(A, b, False, tol=1e-9, inner_tol=1e-3, max_inner=40000)
+    xp, ip = _solve(A, b, True, tol=1e-9, inner_tol=1e-3, max_inner=40000)
+    assert ip["persistent"] and not ig["persistent"]
+    assert ip["converged"] and ig["converged"]
+    Ao = oracle.Csr(*c.to_csr(), c.n)
+    bh = b.cpu().numpy()
+    assert oracle.true_residual(Ao, bh, xp.cpu().numpy()) <= 1e-9 * 1.01
+    assert abs(ip["inner_iters"] - ig["inner_iters"]) <= 0.05 * ig["inner_iters"] + 3, (ip, ig)
+    rel = float((xp - xg).norm() / xg.norm())
+    assert rel <= 1e-7, rel
+
+
+def test_persistent_first_iterates(mps):
+    """Capped at a few iterations (no replacement yet), the two forms return
+    the same x to within FP32 rounding of the partial sums' grouping."""
+    c, A = _learned(mps, 160, 120, 32)
+    b = torch.from_numpy(W.rhs(c.n, 9).astype(np.float64)).cuda()
+    for k in (1, 2, 5, 20):
+        xg, ig = _solve(A, b, False, tol=1e-30, inner_tol=1e-30, max_inner=k, max_outer=1)
+        xp, ip = _solve(A, b, True, tol=1e-30, inner_tol=1e-30, max_inner=k, max_outer=1)
+        assert ip["persistent"] and ip["inner_iters"] == ig["inner_iters"] == k, (k, ip, ig)
+        assert float((xp - xg).norm() / xg.norm()) <= 1e-6, k
+
+
+def test_persistent_stall_fallback(mps):
+    """A deliberately poor (but SPD) factor: the stall watch switches to
+    Jacobi inside the persistent kernel as in the graph form, and the solve
+    still reaches its FP64 target."""
+    c = W.lognormal_diffusion_2d(64, 64, 1.5, 8.0, 7)
+    e = torch.empty(0)
+    A = mps.spmv.csr_tensor(torch.from_numpy(c.keys()), torch.from_numpy(c.vals), e, e, e, c.n, c.n)
+    n = c.n
+    rp, ci, _ = c.to_csr()
+    rows_all = np.repeat(np.arange(n), np.diff(rp))
+    keep = ci <= rows_all
+    rows, gci = rows_all[keep], ci[keep]
+    gv = np.where(gci == rows, 1.0, 5.0 * np.random.default_rng(0).standard_normal(keep.sum()))
+    grp = np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=n))]).astype(np.int32)
+    A.set_fsai_apply("product")
+    A.set_fsai(torch.from_numpy(grp), torch.from_numpy(gci.astype(np.int32)),
+               torch.from_numpy(gv.astype(np.float32)))
+    b = torch.from_numpy(W.rhs(n, 1).astype(np.float64)).cuda()
+    A.set_persistent(True)
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    info = A.cg_mixed(b, x, tol=1e-8, inner_tol=1e-3, max_inner=20000, precond="fsai")
+    assert info["persistent"] and info["converged"] and info["rel_resid"] <= 1e-8
+
+
+def test_rows_too_large_fall_back_to_graph_form(mps):
+    """Rows of A and M beyond the per-SM shared memory: the graph form runs."""
+    c, A = _learned(mps, 700, 700, 33)
+    b = torch.from_numpy(W.rhs(c.n, 2).astype(np.float64)).cuda()
+    x, info = _solve(A, b, True, tol=1e-6, inner_tol=1e-4, max_inner=40000)
+    assert not info["persistent"] and info["converged"]
