@@ -126,7 +126,7 @@ struct SortSmem {
 // One LSD pass.  FIRST: input keys are packed (row<<32|col) and are compacted
 // on load.  LAST: the output is col_ind (low col_bits of the compact key).
 template <bool FIRST, bool LAST>
-__global__ void __launch_bounds__(kSortNT, 2)
+__global__ void __launch_bounds__(kSortNT, 3)
 sort_onesweep(const unsigned long long* __restrict__ kin, const unsigned* __restrict__ vin,
               unsigned long long* __restrict__ kout, int32_t* __restrict__ col_out,
               unsigned* __restrict__ vout, uint64_t nnz, KeyShape ks, int shift,
@@ -380,10 +380,17 @@ cudaError_t sort_to_csr(const uint64_t* keys, const uint32_t* payload, uint64_t 
         cudaGetDevice(&dev);
         const unsigned long long bit = dev >= 0 && dev < 64 ? 1ull << dev : 0ull;
         if (!bit || !(attr_done.load() & bit)) {
-            cudaFuncSetAttribute(sort_onesweep<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            cudaFuncSetAttribute(sort_onesweep<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            cudaFuncSetAttribute(sort_onesweep<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            cudaFuncSetAttribute(sort_onesweep<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            // three CTAs per SM (80 registers, 3 x 59 KB): the largest
+            // shared-memory carve-out
+            auto opt_in = [&](const void* k) {
+                cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     cudaSharedmemCarveoutMaxShared);
+            };
+            opt_in(reinterpret_cast<const void*>(sort_onesweep<true, true>));
+            opt_in(reinterpret_cast<const void*>(sort_onesweep<true, false>));
+            opt_in(reinterpret_cast<const void*>(sort_onesweep<false, true>));
+            opt_in(reinterpret_cast<const void*>(sort_onesweep<false, false>));
             attr_done.fetch_or(bit);
         }
         const unsigned long long* kin = (const unsigned long long*)keys;
