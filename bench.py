@@ -366,6 +366,38 @@ def run_ours(args, rank, world, dev):
     return out
 
 
+def learned_only(args, dev):
+    """The headline solve alone (attach the learned factor, mixed-precision
+    FSAI-PCG to 1e-6) on warmup + steps held-out 512^2 systems, CUDA events
+    per solve: a short command for profilers."""
+    import torch
+    import mpsparse_b200 as mps
+    from mpsparse_b200.fsai import LearnedFsai
+    fsai = LearnedFsai.load()
+    e = torch.empty(0)
+    stream = torch.cuda.current_stream()
+    out = {"ms": [], "iters": [], "persistent": []}
+    for i in range(args.warmup + args.steps):
+        coo, b = c4_system(TEST_SEED0 + i)
+        A = mps.spmv.csr_tensor(torch.from_numpy(coo.keys()), torch.from_numpy(coo.vals), e, e, e,
+                                coo.n, coo.n, fill_outputs=False)
+        b64 = torch.from_numpy(b).double().to(dev)
+        for rep in range(2):                 # the second solve is timed (graph / plan set-up done)
+            x = torch.zeros(coo.n, dtype=torch.float64, device=dev)
+            a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fsai.attach(A)
+            info = A.cg_mixed(b64, x, tol=TOL, inner_tol=args.inner_tol, max_inner=args.max_iter,
+                              precond="fsai")
+            z.record(stream)
+            torch.cuda.synchronize()
+        if i >= args.warmup:
+            out["ms"].append(a.elapsed_time(z))
+            out["iters"].append(info["inner_iters"])
+            out["persistent"].append(bool(info["persistent"]))
+    return out
+
+
 def mlp_leg(A, dev):
     """The learned factor's network on the tensor cores: forward and backward
     passes over the features of a 512^2 system's G (785,408 nonzeros = rows
@@ -931,6 +963,8 @@ def main():
     ap.add_argument("--batch-systems", type=int, default=4096)
     ap.add_argument("--only-spmv", action="store_true",
                     help="only the 256^3 (or --c3-grid) SpMV measurement; for ncu captures")
+    ap.add_argument("--only-learned", action="store_true",
+                    help="only the learned solve on warmup + steps systems (for profilers)")
     ap.add_argument("--only-mlp", action="store_true",
                     help="only the network forward/backward timing on one 512^2 system's factor")
     ap.add_argument("--solver", default="learned", choices=["learned", "plain"],
@@ -961,6 +995,9 @@ def main():
     if args.only_spmv:
         ctx = C3Context(args, local)
         print(json.dumps({"spmv": spmv_c3(args, local, ctx)}))
+        return
+    if args.only_learned:
+        print(json.dumps({"learned": learned_only(args, local)}))
         return
     if args.only_mlp:
         import mpsparse_b200 as mps
