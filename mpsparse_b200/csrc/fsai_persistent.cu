@@ -131,14 +131,14 @@ __device__ bool reduce_all(const PersistDev& P, PersistShared& sh, int slot, dou
         for (int j = 0; j < NS; ++j) P.part[(slot * 3 + j) * G + blockIdx.x] = acc[j];
     }
     if (!grid_barrier(P, sh)) return false;
-    if (threadIdx.x < 32) {
-#pragma unroll
-        for (int j = 0; j < NS; ++j) {
-            double s = 0.0;
-            for (int c = threadIdx.x; c < G; c += 32) s += __ldcg(P.part + (slot * 3 + j) * G + c);
-            s = warp_sum(s);
-            if (threadIdx.x == 0) sh.tot[j] = s;
-        }
+    // warp j sums partial j (the NS sums in parallel, each in a fixed order)
+    const int w = threadIdx.x >> 5;
+    if (w < NS) {
+        const double* src = P.part + (slot * 3 + w) * G;
+        double s = 0.0;
+        for (int c = threadIdx.x & 31; c < G; c += 32) s += __ldcg(src + c);
+        s = warp_sum(s);
+        if ((threadIdx.x & 31) == 0) sh.tot[w] = s;
     }
     __syncthreads();
 #pragma unroll
@@ -155,6 +155,36 @@ __device__ __forceinline__ float row_f32(const int* rp, const int* ci, const flo
     const int e = rp[li + 1];
     for (int k = rp[li]; k < e; ++k) s = __fadd_rn(s, __fmul_rn(v[k], gather(ci[k])));
     return s;
+}
+
+// Rows li0 and (when has1) li1 at once, each summed in its own column
+// order exactly as row_f32 does: the gathers of both rows are issued four at
+// a time before their products are added, so the two rows' gather latencies
+// overlap instead of adding up.
+template <class F>
+__device__ __forceinline__ void row_pair_f32(const int* rp, const int* ci, const float* v, int li0,
+                                             int li1, bool has1, F gather, float& s0, float& s1) {
+    const int b0 = rp[li0], e0 = rp[li0 + 1];
+    const int b1 = has1 ? rp[li1] : 0, e1 = has1 ? rp[li1 + 1] : 0;
+    s0 = 0.f;
+    s1 = 0.f;
+    const int len = max(e0 - b0, e1 - b1);
+    for (int k = 0; k < len; k += 4) {
+        float g0[4], g1[4], w0[4], w1[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const bool in0 = b0 + k + u < e0, in1 = b1 + k + u < e1;
+            w0[u] = in0 ? v[b0 + k + u] : 0.f;
+            w1[u] = in1 ? v[b1 + k + u] : 0.f;
+            g0[u] = in0 ? gather(ci[b0 + k + u]) : 0.f;
+            g1[u] = in1 ? gather(ci[b1 + k + u]) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (b0 + k + u < e0) s0 = __fadd_rn(s0, __fmul_rn(w0[u], g0[u]));
+            if (b1 + k + u < e1) s1 = __fadd_rn(s1, __fmul_rn(w1[u], g1[u]));
+        }
+    }
 }
 
 __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
@@ -247,13 +277,20 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                     return beta != 0.f ? fmaf(beta, __ldcg(po + c), zc) : zc;
                 };
                 double acc[1] = {0.0};
-                for (int li = tid; li < R; li += kPNT) {
-                    const float s = row_f32(arp, aci, av, li, dir);
+                auto own = [&](int li, float s) {
                     const int i = r0 + li;
                     const float pv = dir(i);
                     pn[i] = pv;
                     P.q[i] = s;
                     acc[0] += (double)pv * (double)s;
+                };
+                for (int li = tid; li < R; li += 2 * kPNT) {
+                    const int lj = li + kPNT;
+                    const bool has1 = lj < R;
+                    float s0, s1;
+                    row_pair_f32(arp, aci, av, li, lj, has1, dir, s0, s1);
+                    own(li, s0);
+                    if (has1) own(lj, s1);
                 }
                 double tot[1];
                 if (!reduce_all<1>(P, sh, 0, acc, tot)) goto out;
@@ -281,8 +318,7 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                 const float af = (float)a;
                 auto res = [&](int c) { return fmaf(-af, __ldcg(P.q + c), __ldcg(rc + c)); };
                 double acc[3] = {0.0, 0.0, 0.0};
-                for (int li = tid; li < R; li += kPNT) {
-                    const float s = row_f32(mrp, mci, mv, li, res);
+                auto own = [&](int li, float s) {
                     const int i = r0 + li;
                     const float rv = res(i);
                     rn[i] = rv;
@@ -291,6 +327,14 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                     acc[0] += (double)rv * rv;
                     acc[1] += (double)rv * rv * dinv[i];
                     acc[2] += (double)rv * (double)s;
+                };
+                for (int li = tid; li < R; li += 2 * kPNT) {
+                    const int lj = li + kPNT;
+                    const bool has1 = lj < R;
+                    float s0, s1;
+                    row_pair_f32(mrp, mci, mv, li, lj, has1, res, s0, s1);
+                    own(li, s0);
+                    if (has1) own(lj, s1);
                 }
                 double tot[3];
                 if (!reduce_all<3>(P, sh, 1, acc, tot)) goto out;
