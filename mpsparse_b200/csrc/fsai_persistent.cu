@@ -55,7 +55,7 @@ struct PersistDev {
     float* q;
     float* z;
     double* part;           // partial sums: 4 slots x 3 sums x gridDim.x
-    unsigned* bar;          // [0] arrivals, [1] generation, [2] abort (zeroed before launch)
+    unsigned* bar;          // [0] arrivals (monotonic), [1] unused, [2] abort (zeroed before launch)
     unsigned* err;
     DevScalars* sc_out;     // the final scalars (read back by the host)
     const SolveParams* prm;
@@ -79,24 +79,29 @@ __device__ __forceinline__ unsigned ld_volatile_u32(const unsigned* p) {
     return *reinterpret_cast<const volatile unsigned*>(p);
 }
 
-// Grid barrier: arrival counter + generation word.  Thread 0 arrives after a
-// release fence; the last arrival resets the counter and bumps the
-// generation; the others poll the generation (bounded; a raised abort word
-// ends the wait at once).  false: this CTA gave up (timeout or abort).
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+// Grid barrier on one monotonic arrival counter: barrier k (k = 1, 2, ...)
+// is passed once the counter reaches k * gridDim.x.  Thread 0 arrives with a
+// release-acquire add (its CTA's writes are published, the CTA's later reads
+// see everyone's); the CTAs that are not last poll the counter with acquire
+// loads (bounded; a raised abort word ends the wait at once).  No reset and
+// no second word, so the last arrival adds nothing to the critical path.
+// The counter may wrap: targets are compared by signed difference.
+// false: this CTA gave up (timeout or abort).
 __device__ bool grid_barrier(const PersistDev& P, PersistShared& sh) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned g = sh.gen;
+        const unsigned target = (sh.gen + 1) * gridDim.x;
         int ok = 1;
-        __threadfence();
-        const unsigned t = atomicAdd(P.bar, 1u);
-        if (t == gridDim.x - 1) {
-            *reinterpret_cast<volatile unsigned*>(P.bar) = 0u;
-            __threadfence();
-            atomicAdd(P.bar + 1, 1u);
-        } else {
+        const unsigned old = atom_add_acq_rel(P.bar, 1u);
+        if (old + 1 != target) {
             unsigned spins = 0;
-            while (ld_acquire_u32(P.bar + 1) == g) {
+            while ((int)(ld_acquire_u32(P.bar) - target) < 0) {
                 if (ld_volatile_u32(P.bar + 2)) {
                     ok = 0;
                     break;
@@ -110,8 +115,7 @@ __device__ bool grid_barrier(const PersistDev& P, PersistShared& sh) {
                 if (spins > 64) __nanosleep(128);
             }
         }
-        __threadfence();
-        sh.gen = g + 1;
+        sh.gen = sh.gen + 1;
         sh.ok = ok;
     }
     __syncthreads();
