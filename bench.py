@@ -242,7 +242,7 @@ def run_ours(args, rank, world, dev):
                           precond="fsai", host_loop=args.host_loop)
         return x, {"iters": info["inner_iters"], "outer": info["outer_iters"],
                    "converged": info["converged"], "rel_resid": info["rel_resid"],
-                   "form": A.fsai_apply()["form"]}
+                   "form": A.fsai_apply()["form"], "persistent": bool(info["persistent"])}
 
     if args.solver == "learned":
         from mpsparse_b200.fsai import LearnedFsai, DEFAULT_WEIGHTS
@@ -321,6 +321,10 @@ def run_ours(args, rank, world, dev):
         # iterations per loop body, so after each replacement (and at the
         # stop) about 7.5 iterations' kernels return at once: 15 launches
         def per_solve(i):
+            if i.get("persistent"):
+                # attach (forward, value map, G^T gather, G^T G values),
+                # ||b||^2, the persistent solve, the FP64 true residual
+                return 4 + 1 + 1 + 1
             if i.get("form") == "product":
                 rounds = max(i["outer"], 1)
                 return 4 + 1 + 2 + 2 * i["iters"] + 2 * rounds + 15 * rounds + 1

@@ -508,7 +508,7 @@ mps_status mps_csr_set_fsai(mps_csr* h, const int32_t* d_g_row_ptr, const int32_
     MPS_CUDA(cudaMemcpyAsync(h->G.rp, d_g_row_ptr, ((size_t)n + 1) * 4, cudaMemcpyDeviceToDevice, s));
     MPS_CUDA(cudaMemcpyAsync(h->G.ci, d_g_col_ind, g_nnz * 4, cudaMemcpyDeviceToDevice, s));
     MPS_CUDA(cudaMemcpyAsync(h->G.v, d_g_vals, g_nnz * 4, cudaMemcpyDeviceToDevice, s));
-    MPS_CUDA(spmv_plan_build(h->G, 0, s));
+    // (G's SpMV plan is built below, with G^T's, by factor_plans_follow)
     // G^T through the same radix sort on (col<<32 | row) keys.
     unsigned long long* keys = nullptr;
     MPS_CUDA(stream_alloc(&keys, (g_nnz ? g_nnz : 1) * 8, s));
