@@ -77,13 +77,17 @@ typedef struct {
     double true_resid;        /* ||b - A x|| / ||b|| of the returned x, recomputed on the
                                  GPU after the solve in FP64 (FP64 products and sums
                                  over the stored FP32 matrix and x) */
+    int32_t persistent;       /* 1: the solve ran as one persistent kernel
+                                 (CG / Jacobi-PCG on a CSR whose rows fit one CTA
+                                 per SM; see mps_csr_set_persistent) */
+    int32_t reserved;
 } mps_solve_info;
 
 /* Fill opts with the defaults (tol 1e-6, max_iter 2000, graphs on). */
 void mps_solve_opts_default(mps_solve_opts* opts);
 const char* mps_last_error_string(void);
 const char* mps_status_string(mps_status s);
-/* 2: mps_solve_info carries stop_rule_met and true_resid. */
+/* 3: mps_solve_info carries stop_rule_met, true_resid and persistent. */
 int32_t mps_abi_version(void);
 
 /* ---- COO -> CSR ------------------------------------------------------- */
@@ -219,13 +223,15 @@ typedef struct {
     double rel_resid;         /* FP64 true residual at exit */
 } mps_ir_info;
 
-/* Reliable-update FSAI-PCG in product form (M = G^T G) runs as ONE
- * cooperative kernel -- one CTA per SM holding its rows of A and M in shared
- * memory, grid barriers between the steps of an iteration -- whenever those
- * rows fit (about 200 KB per SM; e.g. 2D 5-point systems up to ~300k rows);
- * otherwise, or with enable = 0, as the graph of two kernels per iteration.
- * Default 1.  Both forms compute the same iterates up to the grouping of the
- * FP64 partial sums.  No reference counterpart. */
+/* Reliable-update FSAI-PCG in product form (M = G^T G), and plain CG /
+ * Jacobi-PCG (mps_csr_cg without reference_compat or host_loop), run as ONE
+ * cooperative kernel -- one CTA per SM holding its rows of A (and M) in
+ * shared memory, grid barriers between the steps of an iteration --
+ * whenever those rows fit (about 200 KB per SM; e.g. 2D 5-point systems up
+ * to ~300k rows with M, ~1M rows without); otherwise, or with enable = 0, as
+ * the CUDA graph of two or three kernels per iteration.  Default 1.  Both
+ * forms compute the same iterates up to the grouping of the FP64 partial
+ * sums.  No reference counterpart. */
 mps_status mps_csr_set_persistent(mps_csr* A, int32_t enable);
 
 mps_status mps_csr_cg_mixed(mps_csr* A, const double* d_b, double* d_x, const mps_ir_opts* opts,
@@ -269,7 +275,11 @@ mps_status mps_fsai_model_create(const float* h_params, mps_fsai_model** out);
 mps_status mps_fsai_model_destroy(mps_fsai_model* m);
 mps_status mps_fsai_model_get(const mps_fsai_model* m, float* h_params);
 mps_status mps_fsai_model_set(mps_fsai_model* m, const float* h_params);
-/* Build G = net(A) on tril(A) and attach it for MPS_PRECOND_FSAI. */
+/* Build G = net(A) on tril(A) and attach it for MPS_PRECOND_FSAI.  Does
+ * not synchronise after the first attach on A (the first one builds the
+ * pattern and plans): a bounded tensor-core wait of the network that gave up
+ * is reported as MPS_ERR_TIMEOUT by the next solve on A (and by
+ * mps_fsai_model_status). */
 mps_status mps_fsai_attach(mps_csr* A, const mps_fsai_model* m, cudaStream_t stream);
 /* One training step on system A: n_probes Rademacher probes plus n_extra
  * caller vectors (d_extra, n_extra x n, e.g. CG residuals of A); loss

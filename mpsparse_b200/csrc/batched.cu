@@ -647,7 +647,9 @@ mps_status mps_batch_attach_fsai(mps_batch* B, const mps_fsai_model* m, cudaStre
         cudaGraphExecDestroy(B->exec);
         B->exec = nullptr;
     }
-    return mps_fsai_attach(B->A, m, s);
+    const mps_status st = mps_fsai_attach(B->A, m, s);
+    if (st != MPS_OK) return st;
+    return mps_fsai_model_status(m, s);   // the batch solve does not read the handle's error words
 }
 
 mps_status mps_batch_set_precond(mps_batch* B, const int8_t* h_kind) {

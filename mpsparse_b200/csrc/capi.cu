@@ -179,7 +179,7 @@ mps_status build_from_keys(CsrMat& m, const uint64_t* keys, const uint32_t* payl
 
 extern "C" {
 
-int32_t mps_abi_version(void) { return 2; }
+int32_t mps_abi_version(void) { return 3; }
 
 void mps_solve_opts_default(mps_solve_opts* o) {
     if (!o) return;
@@ -215,7 +215,8 @@ mps_status mps_csr_create_from_keys(const uint64_t* d_keys, const float* d_vals,
     if (st != MPS_OK) return st;
     if (nnz && (!d_keys || !d_vals)) return fail(MPS_ERR_ARG, "keys / values are null");
     mps_csr* h = new mps_csr();
-    MPS_CUDA(dev_alloc(&h->d_err, sizeof(unsigned), stream));
+    MPS_CUDA(dev_alloc(&h->d_err, 2 * sizeof(unsigned), stream));
+    MPS_CUDA(cudaMemsetAsync(h->d_err, 0, 2 * sizeof(unsigned), stream));
     st = build_from_keys(h->A, d_keys, reinterpret_cast<const uint32_t*>(d_vals), nnz, n_rows,
                          n_cols, h->d_err, stream);
     if (st != MPS_OK) {
@@ -235,7 +236,8 @@ mps_status mps_csr_create_from_csr(const int32_t* d_row_ptr, const int32_t* d_co
     if (st != MPS_OK) return st;
     if (!d_row_ptr || (nnz && (!d_col_ind || !d_vals))) return fail(MPS_ERR_ARG, "null CSR array");
     mps_csr* h = new mps_csr();
-    MPS_CUDA(dev_alloc(&h->d_err, sizeof(unsigned), stream));
+    MPS_CUDA(dev_alloc(&h->d_err, 2 * sizeof(unsigned), stream));
+    MPS_CUDA(cudaMemsetAsync(h->d_err, 0, 2 * sizeof(unsigned), stream));
     st = alloc_csr(h->A, n_rows, n_cols, nnz, h->d_err, stream);
     if (st != MPS_OK) {
         mps_csr_destroy(h);
@@ -294,7 +296,7 @@ mps_status mps_csr_destroy(mps_csr* h) {
     fsai_product_free(h);
     csr_free(h->G);
     csr_free(h->Gt);
-    persist_plan_free(h);
+    persist_plan_free_all(h);
     dev_free(h->vb);
     dev_free(h->d_err);
     fsai_work_free(h->fw);
@@ -459,6 +461,54 @@ mps_status prepare_precond(mps_csr* h, const mps_solve_opts* o, cudaStream_t s) 
 
 extern "C" {
 
+// A handle's error words: [0] bounded waits of its own kernels (cleared at
+// the start of each call), [1] the learned network's bounded waits, folded
+// in by an attach (which does not synchronise) and reported -- then cleared
+// -- by the next solve.
+static mps_status solve_errors(mps_csr* h, const unsigned* e2, mps_status st, cudaStream_t s) {
+    if (st != MPS_OK) return st;
+    if (e2[1] & kErrTimeout) {
+        cudaMemsetAsync(h->d_err + 1, 0, sizeof(unsigned), s);
+        return fail(MPS_ERR_TIMEOUT, "FSAI network: a tensor-core wait gave up (in the attach before this solve)");
+    }
+    if (e2[0] & kErrTimeout)
+        return fail(MPS_ERR_TIMEOUT, "a bounded device wait gave up (SpMV bulk copy or grid barrier)");
+    return MPS_OK;
+}
+
+// Plain CG / Jacobi-PCG as one persistent cooperative kernel when A's rows
+// fit one CTA per SM (fsai_persistent.cu); *ran = false: not eligible, the
+// graph form runs instead.  Same parameters, result places and report as
+// run_solve.
+static mps_status csr_cg_persistent(mps_csr* h, const float* b, float* x, const mps_solve_opts& o,
+                                    mps_solve_info* info, cudaStream_t s, bool* ran) {
+    *ran = false;
+    SolverHost& H = h->H;
+    const size_t n = h->A.n_rows;
+    SolveParams& P = *H.h_params;
+    P.delta = 0.0;
+    P.tol = o.tol > 0 ? o.tol : 1e-6;
+    P.omega = o.omega != 0 ? o.omega : 0.01;
+    P.max_iter = o.max_iter > 0 ? o.max_iter : 2000;
+    P.compat = 0;
+    P.precond = o.precond;
+    P.stall_window = o.stall_window > 0 ? o.stall_window : 400;
+    MPS_CUDA(cudaMemcpyAsync(H.ws.d_params, H.h_params, sizeof(SolveParams), cudaMemcpyHostToDevice, s));
+    MPS_CUDA(cudaMemcpyAsync(H.v(vB), b, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    const cudaError_t pe = persist_cg_solve(h, s);
+    if (pe == cudaErrorNotSupported) return MPS_OK;
+    if (pe != cudaSuccess) return cuda_fail(pe, "persistent CG");
+    *ran = true;
+    MPS_CUDA(cudaMemcpyAsync(x, H.v(vX), n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    const CsrOp op{&h->A, nullptr};
+    MPS_CUDA(op.true_resid(x, H.v(vB), &H.ws.sc->true_rr, H.ws.counters + 11, H.ws.partials, s));
+    MPS_CUDA(cudaMemcpyAsync(H.ws.h_sc, H.ws.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
+    MPS_CUDA(cudaStreamSynchronize(s));
+    const mps_status st = solve_report(kCG, H, info, nullptr, true);
+    if (info) info->persistent = 1;
+    return st;
+}
+
 static mps_status csr_solve(SolverKind kind, mps_csr* h, const float* b, float* x,
                             const mps_solve_opts* o, mps_solve_info* info, cudaStream_t s) {
     if (!h || !b || !x) return fail(MPS_ERR_ARG, "null argument");
@@ -470,12 +520,18 @@ static mps_status csr_solve(SolverKind kind, mps_csr* h, const float* b, float* 
     PrecondOps<CsrOp> pc{h->has_fsai ? &g : nullptr, h->has_fsai ? &gt : nullptr,
                          h->has_fsai && h->use_m ? &mm : nullptr};
     MPS_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), s));
-    st = run_solve(kind, op, pc, h->H, b, x, o, info, s);
-    unsigned err = 0;
-    MPS_CUDA(cudaMemcpy(&err, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
-    if (st == MPS_OK && (err & kErrTimeout))
-        return fail(MPS_ERR_TIMEOUT, "SpMV: a bulk-copy wait gave up");
-    return st;
+    mps_solve_opts oo;
+    mps_solve_opts_default(&oo);
+    if (o) oo = *o;
+    bool ran = false;
+    if (kind == kCG && h->persistent && !oo.reference_compat && !oo.host_loop &&
+        (oo.precond == MPS_PRECOND_NONE || oo.precond == MPS_PRECOND_JACOBI))
+        st = csr_cg_persistent(h, b, x, oo, info, s, &ran);
+    if (st != MPS_OK) return st;
+    if (!ran) st = run_solve(kind, op, pc, h->H, b, x, o, info, s);
+    unsigned err[2] = {0, 0};
+    MPS_CUDA(cudaMemcpy(err, h->d_err, sizeof(err), cudaMemcpyDeviceToHost));
+    return solve_errors(h, err, st, s);
 }
 
 mps_status mps_csr_cg(mps_csr* h, const float* b, float* x, const mps_solve_opts* o,
@@ -665,12 +721,12 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
         if (st == MPS_OK) {
             unsigned* h_err = reinterpret_cast<unsigned*>(H.h_aux + 2);
             MPS_CUDA(cudaMemcpyAsync(H.h_aux, scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
-            MPS_CUDA(cudaMemcpyAsync(h_err, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+            MPS_CUDA(cudaMemcpyAsync(h_err, h->d_err, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
             MPS_CUDA(cudaStreamSynchronize(s));
             st = solve_report(kCG, H, &ii, &rep);
             const double bnorm = std::sqrt(H.h_aux[0]);
             rel = bnorm > 0 ? std::sqrt(H.h_aux[1]) / bnorm : std::sqrt(H.h_aux[1]);
-            if (st == MPS_OK && (*h_err & kErrTimeout)) st = fail(MPS_ERR_TIMEOUT, "SpMV: a bulk-copy wait gave up");
+            st = solve_errors(h, h_err, st, s);
         }
         cudaFreeAsync(scal, s);
         if (info) {
@@ -711,10 +767,9 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
     }
     cudaFreeAsync(scal, s);
     {
-        unsigned err = 0;
-        MPS_CUDA(cudaMemcpy(&err, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
-        if (st == MPS_OK && (err & kErrTimeout))
-            st = fail(MPS_ERR_TIMEOUT, "SpMV: a bulk-copy wait gave up");
+        unsigned err[2] = {0, 0};
+        MPS_CUDA(cudaMemcpy(err, h->d_err, sizeof(err), cudaMemcpyDeviceToHost));
+        st = solve_errors(h, err, st, s);
     }
     if (info) {
         info->outer_iters = outer;

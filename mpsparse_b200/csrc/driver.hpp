@@ -633,6 +633,8 @@ inline mps_status solve_report(SolverKind kind, const SolverHost& H, mps_solve_i
     const DevScalars& r = *H.ws.h_sc;
     if (info) {
         info->iters = r.iter;
+        info->persistent = 0;
+        info->reserved = 0;
         info->stop_rule_met = r.converged;
         info->breakdown = r.breakdown;
         info->stalled = r.stalled;

@@ -399,6 +399,11 @@ static mps_status fsai_values(mps_csr* h, const mps_fsai_model* m, cudaStream_t 
     return MPS_OK;
 }
 
+static __global__ void fold_error_kernel(const unsigned* __restrict__ src, unsigned* dst) {
+    const unsigned e = *src;
+    if (e) atomicOr(dst, e);
+}
+
 static mps_status model_error(const mps_fsai_model* m, cudaStream_t s) {
     unsigned e = 0;
     MPS_CUDA(cudaMemcpyAsync(&e, m->err, 4, cudaMemcpyDeviceToHost, s));
@@ -487,8 +492,10 @@ mps_status mps_fsai_attach(mps_csr* h, const mps_fsai_model* m, cudaStream_t s) 
     if (st != MPS_OK) return st;
     st = fsai_values(h, m, s);
     if (st != MPS_OK) return st;
-    st = model_error(m, s);
-    if (st != MPS_OK) return st;
+    // no synchronisation: the network's error word is folded into the
+    // handle's second error word and reported by the next solve
+    fold_error_kernel<<<1, 1, 0, s>>>(m->err, h->d_err + 1);
+    MPS_CUDA(cudaGetLastError());
     h->has_fsai = true;
     return fsai_factor_changed(h, s);
 }

@@ -60,6 +60,8 @@ struct PersistDev {
     DevScalars* sc_out;     // the final scalars (read back by the host)
     const SolveParams* prm;
     int n;
+    const float* b32;       // CG form: FP32 right-hand side
+    float* x32;             // CG form: FP32 solution
 };
 
 struct PersistShared {
@@ -415,34 +417,150 @@ out:
     }
 }
 
+
+// Plain CG and Jacobi-PCG (FP32 x and vectors: the drop-in cgd) as one
+// cooperative kernel over A's rows held in shared memory.  Per iteration:
+//   step 1  p = z + beta p_old on the fly (z = r, or D^-1 r), q = A p, p.q  -> alpha
+//   step 2  x += alpha p, r -= alpha q, r.r (and r.D^-1 r)                  -> beta, stop
+// with the per-element arithmetic of the graph form's three kernels
+// (EpiCgPq, cg_update_xr, cg_update_p) and its stop rule (cg_finalize_xr).
+__global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
+    extern __shared__ __align__(16) unsigned char psmem[];
+    __shared__ PersistShared sh;
+    const int tid = threadIdx.x;
+    const int r0 = P.row_start[blockIdx.x], r1 = P.row_start[blockIdx.x + 1];
+    const int R = r1 - r0;
+    const int a0 = P.a_rp[r0], na = P.a_rp[r1] - a0;
+    // shared layout: arp[R+1] | aci[na] | av[na]
+    int* arp = reinterpret_cast<int*>(psmem);
+    int* aci = arp + (R + 1);
+    float* av = reinterpret_cast<float*>(aci + na);
+    for (int i = tid; i <= R; i += kPNT) arp[i] = P.a_rp[r0 + i] - a0;
+    for (int k = tid; k < na; k += kPNT) {
+        aci[k] = P.a_ci[a0 + k];
+        av[k] = P.a_v[a0 + k];
+    }
+    if (tid == 0) {
+        sh.gen = 0;
+        sh.ok = 1;
+        sh.S = DevScalars{};
+    }
+    __syncthreads();
+    DevScalars& S = sh.S;
+    const Ctx cx{&sh.S, nullptr, nullptr, {}, 0, {}};
+    const int mode0 = P.prm->precond;            // 0 none, 1 Jacobi
+    const float* dinv = mode0 == 1 ? P.dinv : nullptr;
+    float* r = P.r0;
+    {
+        // x = 0, r = b; b.b and b.D^-1 b
+        double acc[2] = {0.0, 0.0};
+        for (int li = tid; li < R; li += kPNT) {
+            const int i = r0 + li;
+            const float bf = P.b32[i];
+            P.x32[i] = 0.f;
+            r[i] = bf;
+            if (dinv) acc[1] += (double)bf * bf * dinv[i];
+            acc[0] += (double)bf * bf;
+        }
+        double tot[2];
+        if (!reduce_all<2>(P, sh, 0, acc, tot)) goto out;
+        if (tid == 0) cg_init_scalars(cx, P.prm, P.n, mode0, tot[0], tot[1]);
+        __syncthreads();
+    }
+    while (!S.done) {
+        // ---- step 1: p = z + beta p_old on the fly, q = A p, p.q ----------
+        {
+            const bool odd = S.iter & 1;
+            float* pn = odd ? P.p1 : P.p0;
+            const float* po = odd ? P.p0 : P.p1;
+            const float beta = (float)S.beta;
+            const bool jac = S.mode == 1;
+            auto dir = [&](int c) {
+                const float zc = jac ? __ldcg(r + c) * __ldg(P.dinv + c) : __ldcg(r + c);
+                return beta != 0.f ? fmaf(beta, __ldcg(po + c), zc) : zc;
+            };
+            double acc[1] = {0.0};
+            auto own = [&](int li, float sv) {
+                const int i = r0 + li;
+                const float pv = dir(i);
+                pn[i] = pv;
+                P.q[i] = sv;
+                acc[0] += (double)pv * (double)sv;
+            };
+            for (int li = tid; li < R; li += 2 * kPNT) {
+                const int lj = li + kPNT;
+                const bool has1 = lj < R;
+                float s0, s1;
+                row_pair_f32(arp, aci, av, li, lj, has1, dir, s0, s1);
+                own(li, s0);
+                if (has1) own(lj, s1);
+            }
+            double tot[1];
+            if (!reduce_all<1>(P, sh, 0, acc, tot)) goto out;
+            if (tid == 0) {
+                const double pq = tot[0];
+                S.pq = pq;
+                if (!(pq > 0.0) || !isfinite(pq)) {
+                    S.breakdown = 1;
+                    S.done = 1;
+                    S.alpha = 0.0;
+                } else {
+                    S.alpha = S.rz / pq;
+                }
+            }
+            __syncthreads();
+            if (S.done) break;
+        }
+        // ---- step 2: x += alpha p, r -= alpha q, r.r, r.D^-1 r -------------
+        {
+            const float* pc = (S.iter & 1) ? P.p1 : P.p0;
+            const float a = (float)S.alpha;
+            double acc[2] = {0.0, 0.0};
+            for (int li = tid; li < R; li += kPNT) {
+                const int i = r0 + li;
+                P.x32[i] = fmaf(a, __ldcg(pc + i), __ldcg(P.x32 + i));
+                const float rv = fmaf(-a, __ldcg(P.q + i), __ldcg(r + i));
+                r[i] = rv;
+                acc[0] += (double)rv * rv;
+                if (dinv) acc[1] += (double)rv * rv * dinv[i];
+            }
+            double tot[2];
+            if (!reduce_all<2>(P, sh, 1, acc, tot)) goto out;
+            if (tid == 0) cg_finalize_xr(&S, tot[0], tot[1]);
+            __syncthreads();
+        }
+    }
+out:
+    if (tid == 0 && blockIdx.x == 0) {
+        if (!sh.ok) S.err |= kErrTimeout;
+        *P.sc_out = S;
+    }
+}
+
 }  // namespace
 
 // Row blocks of A and M for one CTA per SM, balanced by their shared-memory
 // bytes; false when a block would not fit (the graph form is used then).
-cudaError_t persist_plan_build(mps_csr* h, cudaStream_t s) {
-    PersistPlan& pp = h->pp;
+// Row blocks for one CTA per SM over A's rows (and M's when mrp is given),
+// balanced by their shared-memory bytes; pp.state = -1 when a block would
+// not fit or the kernel cannot be made resident (the graph form runs then).
+static cudaError_t plan_rows(PersistPlan& pp, const std::vector<int>& arp, const std::vector<int>* mrp,
+                             int n, const void* kernel, cudaStream_t s) {
     pp.state = -1;
-    if (!h->use_m || !h->M.rp || h->A.n_rows != h->M.n_rows) return cudaSuccess;
-    const int n = (int)h->A.n_rows;
-    std::vector<int> arp(n + 1), mrp(n + 1);
-    cudaError_t e = cudaMemcpyAsync(arp.data(), h->A.rp, (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(mrp.data(), h->M.rp, (size_t)(n + 1) * 4, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaFuncSetAttribute(fsai_pcg_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kPSmemBudget);
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kPSmemBudget);
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fsai_pcg_persistent, kPNT, kPSmemBudget);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPNT, kPSmemBudget);
     if (e != cudaSuccess || per_sm < 1) {
         cudaGetLastError();
         return cudaSuccess;   // not eligible
     }
+    const int words = mrp ? 2 : 1;   // row-pointer words per row
     // at least 128 rows per CTA; one CTA per SM at most
-    int grid = std::min(num_sms(), std::max(1, n / 128));
-    // bytes of row i: two row-pointer words + 8 per nonzero of A and of M
+    const int grid = std::min(num_sms(), std::max(1, n / 128));
     auto bytes_to = [&](int i) {   // rows [0, i)
-        return 8.0 * i + 8.0 * ((double)arp[i] + (double)mrp[i]);
+        return 4.0 * words * i + 8.0 * ((double)arp[i] + (mrp ? (double)(*mrp)[i] : 0.0));
     };
     const double total = bytes_to(n);
     std::vector<int> start(grid + 1);
@@ -464,9 +582,8 @@ cudaError_t persist_plan_build(mps_csr* h, cudaStream_t s) {
     for (int c = 0; c < grid; ++c) {
         const int rows = start[c + 1] - start[c];
         if (rows < 0) return cudaSuccess;
-        const size_t b = 4 * (2 * (size_t)rows + 2) +
-                         8 * ((size_t)(arp[start[c + 1]] - arp[start[c]]) +
-                              (size_t)(mrp[start[c + 1]] - mrp[start[c]]));
+        size_t b = 4 * (size_t)words * ((size_t)rows + 1) + 8 * (size_t)(arp[start[c + 1]] - arp[start[c]]);
+        if (mrp) b += 8 * (size_t)((*mrp)[start[c + 1]] - (*mrp)[start[c]]);
         worst = std::max(worst, b);
     }
     if (worst > kPSmemBudget) return cudaSuccess;   // rows do not fit: not eligible
@@ -484,9 +601,82 @@ cudaError_t persist_plan_build(mps_csr* h, cudaStream_t s) {
     return cudaSuccess;
 }
 
+static cudaError_t host_row_ptr(const CsrMat& m, std::vector<int>& out, cudaStream_t s) {
+    out.resize((size_t)m.n_rows + 1);
+    cudaError_t e = cudaMemcpyAsync(out.data(), m.rp, out.size() * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e;
+}
+
+// Plan of the FSAI form (rows of A and M).
+cudaError_t persist_plan_build(mps_csr* h, cudaStream_t s) {
+    h->pp.state = -1;
+    if (!h->use_m || !h->M.rp || h->A.n_rows != h->M.n_rows) return cudaSuccess;
+    std::vector<int> arp, mrp;
+    cudaError_t e = host_row_ptr(h->A, arp, s);
+    if (e == cudaSuccess) e = host_row_ptr(h->M, mrp, s);
+    if (e != cudaSuccess) return e;
+    return plan_rows(h->pp, arp, &mrp, (int)h->A.n_rows,
+                     reinterpret_cast<const void*>(fsai_pcg_persistent), s);
+}
+
+// Plan of the CG form (rows of A only).
+cudaError_t persist_plan_build_a(mps_csr* h, cudaStream_t s) {
+    h->pp_a.state = -1;
+    if (h->A.n_rows != h->A.n_cols) return cudaSuccess;
+    std::vector<int> arp;
+    const cudaError_t e = host_row_ptr(h->A, arp, s);
+    if (e != cudaSuccess) return e;
+    return plan_rows(h->pp_a, arp, nullptr, (int)h->A.n_rows, reinterpret_cast<const void*>(cg_persistent), s);
+}
+
+// Plain CG / Jacobi-PCG as one cooperative launch: b is H.v(vB), x lands in
+// H.v(vX) and the final scalars in H.ws.sc (the graph form's places); the
+// parameters must be in H.ws.d_params.  cudaErrorNotSupported: A's rows do
+// not fit (the graph form runs then).
+cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s) {
+    if (h->pp_a.state == 0) {
+        const cudaError_t e = persist_plan_build_a(h, s);
+        if (e != cudaSuccess) return e;
+    }
+    if (h->pp_a.state != 1) return cudaErrorNotSupported;
+    SolverHost& H = h->H;
+    PersistDev P{};
+    P.a_rp = h->A.rp;
+    P.a_ci = h->A.ci;
+    P.a_v = h->A.v;
+    P.row_start = h->pp_a.d_row_start;
+    P.dinv = H.dinv;
+    P.r0 = H.v(vR);
+    P.p0 = H.v(vP);
+    P.p1 = H.v(vP1);
+    P.q = H.v(vQ);
+    P.part = H.ws.partials;
+    P.bar = reinterpret_cast<unsigned*>(h->pp_a.d_row_start + h->pp_a.grid + 1);
+    P.err = h->d_err;
+    P.sc_out = H.ws.sc;
+    P.prm = H.ws.d_params;
+    P.n = (int)h->A.n_rows;
+    P.b32 = H.v(vB);
+    P.x32 = H.v(vX);
+    cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(cg_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->pp_a.smem);
+    if (e != cudaSuccess) return e;
+    void* args[] = {&P};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(cg_persistent), dim3(h->pp_a.grid),
+                                       dim3(kPNT), args, h->pp_a.smem, s);
+}
+
 void persist_plan_free(mps_csr* h) {
     dev_free(h->pp.d_row_start);
     h->pp = PersistPlan{};
+}
+
+void persist_plan_free_all(mps_csr* h) {
+    persist_plan_free(h);
+    dev_free(h->pp_a.d_row_start);
+    h->pp_a = PersistPlan{};
 }
 
 // The reliable-update FSAI-PCG solve (x64 = FP64 solution, b64 = FP64 rhs,

@@ -55,7 +55,8 @@ struct mps_csr {
     mps::FsaiProduct fp;
     int32_t fsai_apply = 0;    // MPS_FSAI_APPLY_*
     bool use_m = false;        // PCG applies z = M r (else z = G^T (G r))
-    mps::PersistPlan pp;       // persistent form of reliable-update FSAI-PCG
+    mps::PersistPlan pp;       // persistent form of reliable-update FSAI-PCG (rows of A and M)
+    mps::PersistPlan pp_a;     // persistent form of plain CG / Jacobi-PCG (rows of A)
     int32_t persistent = 1;    // 1: use the persistent form when the rows fit
 };
 
@@ -80,5 +81,7 @@ mps_status fsai_factor_changed(mps_csr* h, cudaStream_t s);
 // Persistent FSAI-PCG (fsai_persistent.cu): plan (built on first use, freed
 // with M's pattern) and the solve; cudaErrorNotSupported: not eligible.
 void persist_plan_free(mps_csr* h);
+void persist_plan_free_all(mps_csr* h);
 cudaError_t persist_solve(mps_csr* h, const double* b64, double* x64, cudaStream_t s);
+cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s);
 }  // namespace mps

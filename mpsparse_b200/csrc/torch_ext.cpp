@@ -51,6 +51,7 @@ py::dict info_dict(const mps_solve_info& i) {
     d["rel_resid"] = i.rel_resid;
     d["stop_rule_met"] = (bool)i.stop_rule_met;
     d["true_resid"] = i.true_resid;
+    d["persistent"] = (bool)i.persistent;
     return d;
 }
 

@@ -19,7 +19,8 @@ class SolveOpts(C.Structure):
 class SolveInfo(C.Structure):
     _fields_ = [("iters", C.c_int32), ("converged", C.c_int32), ("breakdown", C.c_int32),
                 ("stalled", C.c_int32), ("compat_snapshot", C.c_int32), ("stop_rule_met", C.c_int32),
-                ("rel_resid", C.c_double), ("true_resid", C.c_double)]
+                ("rel_resid", C.c_double), ("true_resid", C.c_double), ("persistent", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 def declared_symbols():

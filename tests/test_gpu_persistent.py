@@ -92,3 +92,71 @@ def test_rows_too_large_fall_back_to_graph_form(mps):
     b = torch.from_numpy(W.rhs(c.n, 2).astype(np.float64)).cuda()
     x, info = _solve(A, b, True, tol=1e-6, inner_tol=1e-4, max_inner=40000)
     assert not info["persistent"] and info["converged"]
+
+
+def _cg_system(mps, c):
+    e = torch.empty(0)
+    return mps.spmv.csr_tensor(torch.from_numpy(c.keys()), torch.from_numpy(c.vals), e, e, e, c.n, c.n)
+
+
+@pytest.mark.parametrize("precond", ["none", "jacobi"])
+def test_persistent_cg_matches_graph_form_and_oracle(mps, oracle, precond):
+    """Plain CG / Jacobi-PCG (the drop-in cgd) as one persistent kernel:
+    the first iterates agree with the graph form's and the FP64 oracle's
+    (1e-5 relative, the cgd iterate bar), and converged solves need the same
+    iterations within 2 and reach the same FP64 true residual bar."""
+    from tests.helpers import assert_solved_fp32
+    c = W.lognormal_diffusion_2d(96, 80, 1.0, 6.0, 12) if precond == "jacobi" else W.laplacian_2d(128)
+    A = _cg_system(mps, c)
+    Ao = oracle.Csr(*c.to_csr(), c.n)
+    b = W.rhs(c.n, 5)
+    bt = torch.from_numpy(b).cuda()
+    for k in (1, 2, 5, 20):
+        xs = []
+        for persistent in (True, False):
+            A.set_persistent(persistent)
+            x = torch.zeros(c.n, device="cuda")
+            info = A.cgd(bt, x, tol=1e-300, max_iter=k, precond=precond)
+            assert info["iters"] == k and info["persistent"] == persistent
+            xs.append(x.cpu().numpy().astype(np.float64))
+        xo, _ = oracle.cg(Ao, b, tol=0.0, max_iter=k, precond=None if precond == "none" else "jacobi")
+        for xk in xs:
+            assert np.linalg.norm(xk - xo) / np.linalg.norm(xo) <= 1e-5, k
+    infos = []
+    for persistent in (True, False):
+        A.set_persistent(persistent)
+        x = torch.zeros(c.n, device="cuda")
+        info = A.cgd(bt, x, tol=1e-6, max_iter=20000, precond=precond)
+        assert info["stop_rule_met"] and info["persistent"] == persistent
+        assert_solved_fp32(oracle, Ao, b, x.cpu().numpy(), 1e-6, info)
+        infos.append(info)
+    assert abs(infos[0]["iters"] - infos[1]["iters"]) <= 2, infos
+
+
+def test_persistent_cg_edge_cases(mps):
+    """b = 0 returns x = 0 at once; a non-finite b is rejected; the handle
+    stays usable (the same rules as the graph form)."""
+    c = W.laplacian_2d(64)
+    A = _cg_system(mps, c)
+    A.set_persistent(True)
+    x = torch.ones(c.n, device="cuda")
+    info = A.cgd(torch.zeros(c.n, device="cuda"), x)
+    assert info["persistent"] and info["converged"] and info["iters"] == 0
+    assert float(x.abs().max()) == 0.0
+    bad = torch.ones(c.n, device="cuda")
+    bad[3] = float("inf")
+    with pytest.raises(RuntimeError, match="non-finite"):
+        A.cgd(bad, x)
+    info = A.cgd(torch.ones(c.n, device="cuda"), x, max_iter=3, tol=1e-300)
+    assert info["iters"] == 3 and info["persistent"]
+
+
+def test_persistent_cg_falls_back_for_large_rows(mps):
+    """A's rows beyond the per-SM shared memory (1024^2 Laplacian, 5.2 M
+    nonzeros): the graph form runs."""
+    c = W.laplacian_2d(1024)
+    A = _cg_system(mps, c)
+    b = torch.from_numpy(W.rhs(c.n, 1)).cuda()
+    x = torch.zeros(c.n, device="cuda")
+    info = A.cgd(b, x, tol=1e-3, max_iter=200)
+    assert not info["persistent"] and info["iters"] > 0

@@ -60,6 +60,7 @@ def test_cg_converges_true_residual(mps, oracle, c1):
 
 def test_cg_graph_host_loop_and_reruns_bitwise(mps, c1):
     A = _csr_tensor(mps, c1)
+    A.set_persistent(False)            # the graph form (the persistent one: test_gpu_persistent)
     b = torch.from_numpy(W.rhs(c1.n, 3)).cuda()
     xs = []
     for host_loop in (False, True, False):
