@@ -689,9 +689,11 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
         mps_solve_info ii{};
         int rep = 0;
         bool persisted = false;
-        if (h->persistent && !io.host_loop && o.precond == MPS_PRECOND_FSAI && h->has_fsai && h->use_m) {
+        const bool fsai_pc = o.precond == MPS_PRECOND_FSAI && h->has_fsai && h->use_m;
+        const bool plain_pc = o.precond == MPS_PRECOND_NONE || o.precond == MPS_PRECOND_JACOBI;
+        if (h->persistent && !io.host_loop && (fsai_pc || plain_pc)) {
             // one cooperative kernel for the whole solve when the rows of A
-            // and M fit one CTA per SM (fsai_persistent.cu); the parameters
+            // (and M) fit one CTA per SM (fsai_persistent.cu); the parameters
             // are the ones run_solve would upload
             SolveParams& P = *H.h_params;
             P.delta = inner_tol;
@@ -699,16 +701,16 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
             P.omega = 0.01;
             P.max_iter = ro.max_iter;
             P.compat = 0;
-            P.precond = MPS_PRECOND_FSAI;
+            P.precond = o.precond;
             P.stall_window = ro.stall_window > 0 ? ro.stall_window : 400;
             MPS_CUDA(cudaMemcpyAsync(H.ws.d_params, H.h_params, sizeof(SolveParams), cudaMemcpyHostToDevice, s));
-            const cudaError_t pe = persist_solve(h, d_b, d_x, s);
+            const cudaError_t pe = fsai_pc ? persist_solve(h, d_b, d_x, s) : persist_cg_solve(h, s, d_b, d_x);
             if (pe == cudaSuccess) {
                 MPS_CUDA(cudaMemcpyAsync(H.ws.h_sc, H.ws.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
                 persisted = true;
             } else if (pe != cudaErrorNotSupported) {
                 cudaFreeAsync(scal, s);
-                return cuda_fail(pe, "persistent FSAI-PCG");
+                return cuda_fail(pe, fsai_pc ? "persistent FSAI-PCG" : "persistent CG");
             }
         }
         if (!persisted)

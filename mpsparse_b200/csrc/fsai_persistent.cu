@@ -247,8 +247,10 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
             }
             acc[0] += bd * bd;
         }
+        // slot 3: consecutive reductions never share a slot (with Jacobi the
+        // first p.q goes to slot 0 while late CTAs may still read this one)
         double tot[2];
-        if (!reduce_all<2>(P, sh, 0, acc, tot)) goto out;
+        if (!reduce_all<2>(P, sh, 3, acc, tot)) goto out;
         if (tid == 0) cg_init_scalars(cx, P.prm, P.n, mode0, tot[0], tot[1]);
         __syncthreads();
     }
@@ -424,6 +426,10 @@ out:
 //   step 2  x += alpha p, r -= alpha q, r.r (and r.D^-1 r)                  -> beta, stop
 // with the per-element arithmetic of the graph form's three kernels
 // (EpiCgPq, cg_update_xr, cg_update_p) and its stop rule (cg_finalize_xr).
+// IR (reliable updates, cg_mixed without FSAI): x accumulated in FP64
+// (P.x), b in FP64 (P.b), the stop rule of cg_finalize_ir, and -- when due --
+// the residual replacement r = (float)(b - A x) in FP64 in the same kernel.
+template <bool IR>
 __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
     extern __shared__ __align__(16) unsigned char psmem[];
     __shared__ PersistShared sh;
@@ -456,18 +462,68 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
         double acc[2] = {0.0, 0.0};
         for (int li = tid; li < R; li += kPNT) {
             const int i = r0 + li;
-            const float bf = P.b32[i];
-            P.x32[i] = 0.f;
-            r[i] = bf;
-            if (dinv) acc[1] += (double)bf * bf * dinv[i];
-            acc[0] += (double)bf * bf;
+            if constexpr (IR) {
+                const double bd = __ldg(P.b + i);
+                const float bf = (float)bd;
+                P.x[i] = 0.0;
+                r[i] = bf;
+                if (dinv) acc[1] += (double)bf * bf * dinv[i];
+                acc[0] += bd * bd;
+            } else {
+                const float bf = P.b32[i];
+                P.x32[i] = 0.f;
+                r[i] = bf;
+                if (dinv) acc[1] += (double)bf * bf * dinv[i];
+                acc[0] += (double)bf * bf;
+            }
         }
+        // slot 3: consecutive reductions never share a slot (the first
+        // iteration's p.q goes to slot 0 while late CTAs may still read
+        // this one)
         double tot[2];
-        if (!reduce_all<2>(P, sh, 0, acc, tot)) goto out;
+        if (!reduce_all<2>(P, sh, 3, acc, tot)) goto out;
         if (tid == 0) cg_init_scalars(cx, P.prm, P.n, mode0, tot[0], tot[1]);
         __syncthreads();
     }
     while (!S.done) {
+        if (IR && S.replace) {
+            // ---- replacement: r = (float)(b - A x) in FP64 ------------------
+            double acc[2] = {0.0, 0.0};
+            for (int li = tid; li < R; li += kPNT) {
+                double sd = 0.0;
+                const int e = arp[li + 1];
+                for (int k = arp[li]; k < e; ++k)
+                    sd = __dadd_rn(sd, __dmul_rn((double)av[k], __ldcg(P.x + aci[k])));
+                const int i = r0 + li;
+                const double rt = __ldg(P.b + i) - sd;
+                const float rf = (float)rt;
+                r[i] = rf;
+                acc[0] += rt * rt;
+                acc[1] += (double)rf * rf * (dinv ? dinv[i] : 1.f);
+            }
+            double tot[2];
+            if (!reduce_all<2>(P, sh, 2, acc, tot)) goto out;
+            if (tid == 0) {
+                S.replace = 0;
+                ++S.replaced;
+                const double rr = tot[0];
+                S.rr = rr;
+                S.rr_ref = rr;
+                if (!isfinite(rr)) {
+                    S.breakdown = 1;
+                    S.done = 1;
+                } else if (rr <= S.tol2) {
+                    S.converged = 1;
+                    S.done = 1;
+                } else if (S.iter >= S.max_iter) {
+                    S.done = 1;
+                } else {
+                    cg_direction(&S, rr, tot[1]);
+                }
+            }
+            __syncthreads();
+            continue;
+        }
         // ---- step 1: p = z + beta p_old on the fly, q = A p, p.q ----------
         {
             const bool odd = S.iter & 1;
@@ -514,11 +570,13 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
         // ---- step 2: x += alpha p, r -= alpha q, r.r, r.D^-1 r -------------
         {
             const float* pc = (S.iter & 1) ? P.p1 : P.p0;
-            const float a = (float)S.alpha;
+            const double a64 = S.alpha;
+            const float a = (float)a64;
             double acc[2] = {0.0, 0.0};
             for (int li = tid; li < R; li += kPNT) {
                 const int i = r0 + li;
-                P.x32[i] = fmaf(a, __ldcg(pc + i), __ldcg(P.x32 + i));
+                if constexpr (IR) P.x[i] = fma(a64, (double)__ldcg(pc + i), __ldcg(P.x + i));
+                else P.x32[i] = fmaf(a, __ldcg(pc + i), __ldcg(P.x32 + i));
                 const float rv = fmaf(-a, __ldcg(P.q + i), __ldcg(r + i));
                 r[i] = rv;
                 acc[0] += (double)rv * rv;
@@ -526,7 +584,10 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
             }
             double tot[2];
             if (!reduce_all<2>(P, sh, 1, acc, tot)) goto out;
-            if (tid == 0) cg_finalize_xr(&S, tot[0], tot[1]);
+            if (tid == 0) {
+                if constexpr (IR) cg_finalize_ir(&S, tot[0], tot[1]);
+                else cg_finalize_xr(&S, tot[0], tot[1]);
+            }
             __syncthreads();
         }
     }
@@ -627,14 +688,16 @@ cudaError_t persist_plan_build_a(mps_csr* h, cudaStream_t s) {
     std::vector<int> arp;
     const cudaError_t e = host_row_ptr(h->A, arp, s);
     if (e != cudaSuccess) return e;
-    return plan_rows(h->pp_a, arp, nullptr, (int)h->A.n_rows, reinterpret_cast<const void*>(cg_persistent), s);
+    return plan_rows(h->pp_a, arp, nullptr, (int)h->A.n_rows,
+                     reinterpret_cast<const void*>(cg_persistent<false>), s);
 }
 
 // Plain CG / Jacobi-PCG as one cooperative launch: b is H.v(vB), x lands in
-// H.v(vX) and the final scalars in H.ws.sc (the graph form's places); the
-// parameters must be in H.ws.d_params.  cudaErrorNotSupported: A's rows do
-// not fit (the graph form runs then).
-cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s) {
+// H.v(vX) and the final scalars in H.ws.sc (the graph form's places); with
+// b64 / x64 given, the reliable-update form (FP64 b and x, the caller's
+// buffers).  The parameters must be in H.ws.d_params.
+// cudaErrorNotSupported: A's rows do not fit (the graph form runs then).
+cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s, const double* b64, double* x64) {
     if (h->pp_a.state == 0) {
         const cudaError_t e = persist_plan_build_a(h, s);
         if (e != cudaSuccess) return e;
@@ -659,13 +722,16 @@ cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s) {
     P.n = (int)h->A.n_rows;
     P.b32 = H.v(vB);
     P.x32 = H.v(vX);
+    P.b = b64;
+    P.x = x64;
+    const void* k = b64 ? reinterpret_cast<const void*>(cg_persistent<true>)
+                        : reinterpret_cast<const void*>(cg_persistent<false>);
     cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(cg_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->pp_a.smem);
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->pp_a.smem);
     if (e != cudaSuccess) return e;
     void* args[] = {&P};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(cg_persistent), dim3(h->pp_a.grid),
-                                       dim3(kPNT), args, h->pp_a.smem, s);
+    return cudaLaunchCooperativeKernel(k, dim3(h->pp_a.grid), dim3(kPNT), args, h->pp_a.smem, s);
 }
 
 void persist_plan_free(mps_csr* h) {

@@ -160,3 +160,43 @@ def test_persistent_cg_falls_back_for_large_rows(mps):
     x = torch.zeros(c.n, device="cuda")
     info = A.cgd(b, x, tol=1e-3, max_iter=200)
     assert not info["persistent"] and info["iters"] > 0
+
+
+@pytest.mark.parametrize("precond", ["none", "jacobi"])
+def test_persistent_reliable_cg_matches_graph_form(mps, oracle, precond):
+    """cg_mixed without FSAI (FP32 recurrences, FP64 x, residual
+    replacement) as one persistent kernel: the first iterates agree with
+    the graph form's (1e-6 relative; only the grouping of the FP64 partial
+    sums differs), and converged solves reach the FP64 target checked by
+    the oracle, with iteration and replacement counts close to the graph
+    form's."""
+    c = W.lognormal_diffusion_2d(96, 80, 1.0, 6.0, 14) if precond == "jacobi" else W.laplacian_2d(128)
+    A = _cg_system(mps, c)
+    Ao = oracle.Csr(*c.to_csr(), c.n)
+    b = torch.from_numpy(W.rhs(c.n, 6).astype(np.float64)).cuda()
+    for k in (1, 2, 5, 20):
+        xs = []
+        for persistent in (True, False):
+            A.set_persistent(persistent)
+            x = torch.zeros(c.n, dtype=torch.float64, device="cuda")
+            info = A.cg_mixed(b, x, tol=1e-30, inner_tol=1e-30, max_inner=k, max_outer=1, precond=precond)
+            assert info["persistent"] == persistent and info["inner_iters"] == k, (k, info)
+            xs.append(x)
+        assert float((xs[0] - xs[1]).norm() / xs[1].norm()) <= 1e-6, k
+    infos, sols = [], []
+    for persistent in (True, False):
+        A.set_persistent(persistent)
+        x = torch.zeros(c.n, dtype=torch.float64, device="cuda")
+        info = A.cg_mixed(b, x, tol=1e-9, inner_tol=1e-3, max_inner=40000, precond=precond)
+        assert info["persistent"] == persistent and info["converged"], info
+        assert oracle.true_residual(Ao, b.cpu().numpy(), x.cpu().numpy()) <= 1e-9 * 1.01
+        infos.append(info)
+        sols.append(x)
+    ip, ig = infos
+    assert abs(ip["inner_iters"] - ig["inner_iters"]) <= 0.05 * ig["inner_iters"] + 3, infos
+    assert float((sols[0] - sols[1]).norm() / sols[1].norm()) <= 1e-7
+    # b = 0: x = 0 at once, on the persistent form too
+    A.set_persistent(True)
+    x = torch.ones(c.n, dtype=torch.float64, device="cuda")
+    info = A.cg_mixed(torch.zeros_like(b), x, precond=precond)
+    assert info["persistent"] and info["converged"] and float(x.abs().max()) == 0.0
