@@ -96,13 +96,18 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
         bulk_g2s(base + (size_t)A.cap * (BF16 ? 6 : 8), A.rp + r0, br, &bar[b]);
     };
 
-    // Thread 0 keeps the metadata of the next tiles in registers (loaded
-    // ahead) and publishes each tile's through shared memory when it issues
-    // the tile's copy.
+    // Thread 0 loads the metadata of the next two tiles ahead into shared
+    // memory (s_ahead, by cp.async: no registers held across the loop, no
+    // wait on the load) and publishes each tile's through s_meta when it
+    // issues the tile's copy.  At tile it, slot it & 1 holds tile
+    // it + NB - 1 (issued next) and the other slot tile it + NB.
+    __shared__ int4 s_ahead[2];
     const int4 none = make_int4(0, 0, 0, 0);
     const int t0 = blockIdx.x, G = gridDim.x;
-    int4 m_ahead = none;           // metadata of tile it + NB - 1 (issued next)
-    int4 m_ahead2 = none;          // tile it + NB
+    auto fetch_meta = [&](int ti, int slot) {   // thread 0
+        if (ti < A.ntiles) cp_async16(&s_ahead[slot], A.meta + ti);
+        else s_ahead[slot] = none;
+    };
     unsigned issued = 0;           // thread 0: buffers the prologue filled
     auto prologue = [&]() {        // barriers and the first NB - 1 copies
         if (threadIdx.x != 0) return;
@@ -120,8 +125,8 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
             }
             s_meta[i] = mi;
         }
-        m_ahead = t0 + (NB - 1) * G < A.ntiles ? A.meta[t0 + (NB - 1) * G] : none;
-        m_ahead2 = t0 + NB * G < A.ntiles ? A.meta[t0 + NB * G] : none;
+        fetch_meta(t0 + (NB - 1) * G, 0);
+        fetch_meta(t0 + NB * G, 1);
     };
     if constexpr (PRE) {
         prologue();
@@ -147,10 +152,11 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
     // Issue the copy of tile it + NB - 1 into the buffer tile it - 1 used.
     auto issue_ahead = [&](int t, int it) {   // one thread
         const int bn = (it + NB - 1) % NB;
-        if (t + (NB - 1) * G < A.ntiles && staged(m_ahead)) issue(m_ahead, bn);
-        s_meta[bn] = m_ahead;
-        m_ahead = m_ahead2;
-        m_ahead2 = t + (NB + 1) * G < A.ntiles ? A.meta[t + (NB + 1) * G] : none;
+        cp_async_wait_all();
+        const int4 ma = s_ahead[it & 1];
+        if (t + (NB - 1) * G < A.ntiles && staged(ma)) issue(ma, bn);
+        s_meta[bn] = ma;
+        fetch_meta(t + (NB + 1) * G, it & 1);
     };
     unsigned phase_bits = 0u;      // completed-phase parity per buffer (uniform)
     int it = 0;
@@ -163,6 +169,11 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
         const int4 m = s_meta[b];
         const int rs = m.x, re = m.y, k0 = m.z, k1 = m.w;
         const bool stg = rs < re && staged(m);
+        // long rows (over 16 nonzeros on average): products first, then one
+        // warp per row; short rows: one thread per row forms and adds its own
+        // products (same products, same order), with no product phase and no
+        // barrier between the phases
+        const bool two_phase = stg && (k1 - k0) > 16 * (re - rs);
         unsigned char* base = smem + (size_t)b * bb;
         const int a0 = k0 & ~(GA - 1), r0 = rs & ~3;
         if (stg) {
@@ -172,6 +183,8 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
                 timed_out = 1 + (b << 1) + (par << 3);
             }
             phase_bits ^= 1u << b;
+        }
+        if (two_phase) {
             const int* cols = reinterpret_cast<const int*>(base);
             float* prod = reinterpret_cast<float*>(base);
             // products: U independent gathers in flight per thread (the staged
@@ -198,18 +211,17 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
                     if (kb + u * NT < k1) prod[kb + u * NT - a0] = v[u] * xv[u];
             }
         }
-        // Products visible.  With NB >= 3, every thread is past tile it - 1,
-        // so its buffer takes the copy of tile it + NB - 1.
-        __syncthreads();
+        // Products visible (two-phase tiles).  With NB >= 3, every thread is
+        // past tile it - 1, so its buffer takes the copy of tile it + NB - 1.
+        if (NB >= 3 || two_phase) __syncthreads();
         if constexpr (NB >= 3) {
             if (threadIdx.x == 0) issue_ahead(t, it);
         }
         if (rs < re) {
             if (stg) {
-                const float* prod = reinterpret_cast<const float*>(base);
                 const int* rps = reinterpret_cast<const int*>(base + (size_t)A.cap * (BF16 ? 6 : 8));
-                const int nrows = re - rs;
-                if ((k1 - k0) > 16 * nrows) {
+                if (two_phase) {
+                    const float* prod = reinterpret_cast<const float*>(base);
                     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
                     for (int r = rs + wid; r < re; r += NT / 32) {
                         const int bgn = rps[r - r0] - a0, end = rps[r + 1 - r0] - a0;
@@ -219,11 +231,39 @@ spmv_stream(CsrStreamDev A, const float* __restrict__ x, Epi epi) {
                         if (lane == 0) epi.row(r, s, acc);
                     }
                 } else {
-                    for (int r = rs + threadIdx.x; r < re; r += NT) {
-                        const int bgn = rps[r - r0] - a0, end = rps[r + 1 - r0] - a0;
-                        float s = 0.f;
-                        for (int k = bgn; k < end; ++k) s += prod[k];
-                        epi.row(r, s, acc);
+                    // rows r and r + NT together: the gathers of both rows are
+                    // issued four at a time before their products are added,
+                    // so a thread's two rows cost one gather round trip (only
+                    // the gathered values stay live; the matrix values are
+                    // read from shared memory as they are multiplied)
+                    const int* cols = reinterpret_cast<const int*>(base);
+                    const unsigned char* vbase = base + (size_t)A.cap * 4;
+                    auto val = [&](int i) {
+                        if constexpr (BF16) return bf16_to_f(reinterpret_cast<const __nv_bfloat16*>(vbase)[i]);
+                        else return reinterpret_cast<const float*>(vbase)[i];
+                    };
+                    for (int r = rs + threadIdx.x; r < re; r += 2 * NT) {
+                        const int r2 = r + NT;
+                        const bool has2 = r2 < re;
+                        const int b1 = rps[r - r0] - a0, e1 = rps[r + 1 - r0] - a0;
+                        const int b2 = has2 ? rps[r2 - r0] - a0 : 0, e2 = has2 ? rps[r2 + 1 - r0] - a0 : 0;
+                        float s1 = 0.f, s2 = 0.f;
+                        const int len = max(e1 - b1, e2 - b2);
+                        for (int k = 0; k < len; k += 4) {
+                            float g1[4], g2[4];
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) {
+                                g1[u] = b1 + k + u < e1 ? epi_x(epi, x, cols[b1 + k + u]) : 0.f;
+                                g2[u] = b2 + k + u < e2 ? epi_x(epi, x, cols[b2 + k + u]) : 0.f;
+                            }
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) {
+                                if (b1 + k + u < e1) s1 = __fadd_rn(s1, __fmul_rn(val(b1 + k + u), g1[u]));
+                                if (b2 + k + u < e2) s2 = __fadd_rn(s2, __fmul_rn(val(b2 + k + u), g2[u]));
+                            }
+                        }
+                        epi.row(r, s1, acc);
+                        if (has2) epi.row(r2, s2, acc);
                     }
                 }
             } else {

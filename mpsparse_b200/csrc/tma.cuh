@@ -63,5 +63,14 @@ __device__ __forceinline__ void fence_proxy_async() {
 __device__ __forceinline__ void fence_mbar_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
+// 16-byte asynchronous global -> shared copy (both addresses 16-byte aligned);
+// cp_async_wait_all: this thread's earlier cp_async16 copies have landed.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_all;" ::: "memory");
+}
 
 }  // namespace mps
