@@ -253,20 +253,29 @@ def run_ours(args, rank, world, dev):
         headline = solve_plain
         solver_name = "plain FP32 CG (drop-in cgd)"
 
+    host_ms = {}
+
     def timed(fn):
-        times, infos, xs = [], [], []
+        times, infos, xs, hms = [], [], [], []
         for i in range(nsys):
             flush_l2(flush)
             ev0 = torch.cuda.Event(enable_timing=True)
             ev1 = torch.cuda.Event(enable_timing=True)
+            h0 = time.perf_counter()
             ev0.record(stream)
             x, info = fn(i)
             ev1.record(stream)
+            h1 = time.perf_counter()
             torch.cuda.synchronize()
             if i >= warm:
                 times.append(ev0.elapsed_time(ev1))
                 infos.append(info)
                 xs.append(x)
+                hms.append(round((h1 - h0) * 1e3, 3))
+        # host time from recording the first event to recording the last: a
+        # step whose device time exceeds its kernels' time by a host stall
+        # (the process descheduled between launches) shows it here too
+        host_ms[fn.__name__] = hms
         return times, infos, xs
 
     # per-handle setup (workspace, CUDA-graph capture, the FSAI pattern and
@@ -341,6 +350,7 @@ def run_ours(args, rank, world, dev):
         "iters_mean": statistics.mean(iters),
         "true_resid_max": max(resid),
         "step_ms": [round(t, 3) for t in times],
+        "step_host_ms": host_ms.get(headline.__name__),
         "plain_cg": {"ms_per_solve": statistics.mean(ptimes), "step_ms": [round(t, 3) for t in ptimes],
                      "iters_mean": statistics.mean(i["iters"] for i in pinfos),
                      "true_resid_max": max(presid),
@@ -760,7 +770,8 @@ def c1_leg(dev, flush):
             "mixed_precision_cg": {"ms": ms_mp, "iters": imp["inner_iters"],
                                    "replacements": imp["outer_iters"],
                                    "true_resid": imp["rel_resid"],
-                                   "converged_fp64": bool(imp["converged"])},
+                                   "converged_fp64": bool(imp["converged"]),
+                                   "persistent": bool(imp["persistent"])},
             "reference_compat": {"iters": ic["iters"], "oracle_iters": ioc["iters"],
                                  "true_resid": ic["true_resid"],
                                  "rel_diff_vs_oracle": _rel(xc.cpu().numpy(), xoc)},

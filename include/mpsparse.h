@@ -199,7 +199,10 @@ mps_status mps_csr_richardson(mps_csr* A, const float* d_b, float* d_x,
  * counterpart (the reference solves in FP32 only). */
 typedef struct {
     double tol;               /* outer relative residual target (0: 1e-10) */
-    double inner_tol;         /* inner relative reduction per sweep (0: 1e-3) */
+    double inner_tol;         /* inner relative reduction per sweep (0: 1e-3 with FP32
+                                 values; 0.1 with BF16 values, whose operator differs
+                                 from A by about 2^-9 relative, so one sweep cannot
+                                 gain much more than that) */
     int32_t max_outer;        /* 0: 50 */
     int32_t max_inner;        /* 0: 2000 */
     int32_t value_bits;       /* 32 or 16 */

@@ -633,10 +633,10 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
     mps_ir_opts o{};
     if (o_in) o = *o_in;
     const double tol = o.tol > 0 ? o.tol : 1e-10;
-    const double inner_tol = o.inner_tol > 0 ? o.inner_tol : 1e-3;
+    const bool bf16 = o.value_bits == 16;
+    const double inner_tol = o.inner_tol > 0 ? o.inner_tol : (bf16 ? 0.1 : 1e-3);
     const int max_outer = o.max_outer > 0 ? o.max_outer : 50;
     const int max_inner = o.max_inner > 0 ? o.max_inner : 2000;
-    const bool bf16 = o.value_bits == 16;
     if (o.value_bits != 0 && o.value_bits != 16 && o.value_bits != 32)
         return fail(MPS_ERR_ARG, "value_bits must be 16 or 32");
     mps_solve_opts io;

@@ -733,7 +733,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
              py::arg("tol") = 0.0, py::arg("reference_compat") = false,
              py::arg("host_loop") = false)
         .def("cg_mixed", &CsrTensor::cg_mixed, py::arg("b"), py::arg("x"), py::arg("tol") = 1e-10,
-             py::arg("inner_tol") = 1e-3, py::arg("max_outer") = 50, py::arg("max_inner") = 2000,
+             py::arg("inner_tol") = 0.0, py::arg("max_outer") = 50, py::arg("max_inner") = 2000,
              py::arg("value_bits") = 32, py::arg("precond") = "none", py::arg("host_loop") = false,
              py::arg("ir_mode") = "auto")
         .def("set_fsai", &CsrTensor::set_fsai, py::arg("row_ptr"), py::arg("col_ind"),

@@ -131,3 +131,23 @@ def test_mixed_zero_and_nonfinite_rhs(mps, precond):
     b[c.n // 2] = 1.0
     info = A.cg_mixed(b, x, tol=1e-8, precond=precond)
     assert info["converged"]
+
+
+def test_bf16_default_inner_tol(mps, oracle):
+    """BF16 values: the default sweep target (0.1) reaches 1e-10 with fewer
+    FP32 iterations than asking each sweep for 1e-3, which a BF16-valued
+    operator (about 2^-9 relative from A) cannot deliver without many
+    wasted iterations."""
+    c = W.lognormal_diffusion_3d(48, 1.0, 8.0, 2)
+    e = torch.empty(0)
+    A = mps.spmv.csr_tensor(torch.from_numpy(c.keys()), torch.from_numpy(c.vals), e, e, e, c.n, c.n)
+    b = torch.from_numpy(W.rhs(c.n, 4).astype(np.float64)).cuda()
+    x = torch.zeros(c.n, dtype=torch.float64, device="cuda")
+    dflt = A.cg_mixed(b, x, tol=1e-10, value_bits=16)
+    assert dflt["converged"] and dflt["rel_resid"] <= 1e-10
+    Ao = oracle.Csr(*c.to_csr(), c.n)
+    assert oracle.true_residual(Ao, b.cpu().numpy(), x.cpu().numpy()) <= 1.5e-10
+    x.zero_()
+    tight = A.cg_mixed(b, x, tol=1e-10, value_bits=16, inner_tol=1e-3, max_inner=20000, max_outer=200)
+    assert tight["converged"]
+    assert dflt["inner_iters"] < tight["inner_iters"], (dflt, tight)
