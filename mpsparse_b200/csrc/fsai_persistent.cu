@@ -35,6 +35,8 @@ namespace {
 constexpr int kPNT = 1024;                       // threads per CTA
 constexpr size_t kPSmemBudget = 200 * 1024;      // matrix rows per CTA (dynamic shared memory)
 constexpr unsigned kGridSpinLimit = 1u << 22;    // polls of one barrier wait (about a second)
+constexpr int kCountWord = 0;                    // barrier words: [0] arrivals (monotonic),
+constexpr int kAbortWord = 2;                    // [2] abort
 constexpr int kBarWords = 3;
 
 struct PersistDev {
@@ -72,84 +74,114 @@ struct PersistShared {
     int ok;
 };
 
+// Vectors that other CTAs of the same launch write (p, q, r, z, x): plain
+// weak loads, cached in L1.  Every such read follows a grid barrier
+// (reduce_all): the writers' stores precede their CTA's release (bar.sync,
+// then thread 0's release add on the counter), and the reader's warp 0
+// acquires the counter before the bar.sync that releases its CTA, so by the
+// PTX memory model the weak loads observe those stores; within one step no
+// CTA writes a vector it gathers.
+template <class T>
+__device__ __forceinline__ T ldv(const T* p) {
+    return *p;
+}
+
+__device__ __forceinline__ unsigned ld_volatile_u32(const unsigned* p) {
+    return *reinterpret_cast<const volatile unsigned*>(p);
+}
+
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     unsigned v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ unsigned ld_volatile_u32(const unsigned* p) {
-    return *reinterpret_cast<const volatile unsigned*>(p);
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
-    unsigned old;
-    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-    return old;
-}
-
-// Grid barrier on one monotonic arrival counter: barrier k (k = 1, 2, ...)
-// is passed once the counter reaches k * gridDim.x.  Thread 0 arrives with a
-// release-acquire add (its CTA's writes are published, the CTA's later reads
-// see everyone's); the CTAs that are not last poll the counter with acquire
-// loads (bounded; a raised abort word ends the wait at once).  No reset and
-// no second word, so the last arrival adds nothing to the critical path.
-// The counter may wrap: targets are compared by signed difference.
+// Grid-wide FP64 sums of NS per-thread values, fused with the grid barrier.
+//   1. block sums (warp butterflies, then warp 0 over the warp totals);
+//   2. thread 0 stores the CTA's NS totals in partial slot `slot` and arrives
+//      on the grid's monotonic counter with a release add (no return value
+//      to wait for); reduction k (k = 1, 2, ...) is complete once the
+//      counter reaches k * gridDim.x (compared by signed difference: the
+//      counter may wrap);
+//   3. warp 0 polls the counter with acquire loads (one address: one request
+//      per poll for the warp) and then sums all CTAs' partials -- lane l the
+//      partials l, l + 32, ..., then a butterfly -- so every CTA adds the same
+//      partials in the same order and gets the same bits;
+//   4. one bar.sync hands the totals to the CTA.
+// Consecutive reductions must use different slots: a CTA may store its next
+// partials while a slower CTA still reads these.  The wait is bounded
+// (kGridSpinLimit polls, back-off after 64); a timeout raises the error word
+// and the abort word, and the abort word ends every other CTA's wait.
 // false: this CTA gave up (timeout or abort).
-__device__ bool grid_barrier(const PersistDev& P, PersistShared& sh) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned target = (sh.gen + 1) * gridDim.x;
-        int ok = 1;
-        const unsigned old = atom_add_acq_rel(P.bar, 1u);
-        if (old + 1 != target) {
-            unsigned spins = 0;
-            while ((int)(ld_acquire_u32(P.bar) - target) < 0) {
-                if (ld_volatile_u32(P.bar + 2)) {
-                    ok = 0;
-                    break;
-                }
-                if (++spins > kGridSpinLimit) {
-                    atomicOr(P.err, kErrTimeout);
-                    atomicExch(P.bar + 2, 1u);
-                    ok = 0;
-                    break;
-                }
-                if (spins > 64) __nanosleep(128);
-            }
-        }
-        sh.gen = sh.gen + 1;
-        sh.ok = ok;
-    }
-    __syncthreads();
-    return sh.ok != 0;
-}
-
-// Block totals of NS per-thread FP64 sums -> slot, grid barrier, then every
-// CTA sums all CTAs' partials in one fixed order (warp 0: strided sequential
-// sums per lane, then the butterfly) into tot.
 template <int NS>
 __device__ bool reduce_all(const PersistDev& P, PersistShared& sh, int slot, double (&acc)[NS],
                            double (&tot)[NS]) {
-    block_sum_n<kPNT, NS>(acc, sh.red);
-    const int G = gridDim.x;
-    if (threadIdx.x == 0) {
+    constexpr int W = kPNT / 32;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
-        for (int j = 0; j < NS; ++j) P.part[(slot * 3 + j) * G + blockIdx.x] = acc[j];
+    for (int j = 0; j < NS; ++j) acc[j] = warp_sum(acc[j]);
+    if (lane == 0) {
+#pragma unroll
+        for (int j = 0; j < NS; ++j) sh.red[j * W + w] = acc[j];
     }
-    if (!grid_barrier(P, sh)) return false;
-    // warp j sums partial j (the NS sums in parallel, each in a fixed order)
-    const int w = threadIdx.x >> 5;
-    if (w < NS) {
-        const double* src = P.part + (slot * 3 + w) * G;
-        double s = 0.0;
-        for (int c = threadIdx.x & 31; c < G; c += 32) s += __ldcg(src + c);
-        s = warp_sum(s);
-        if ((threadIdx.x & 31) == 0) sh.tot[w] = s;
+    __syncthreads();
+    if (w == 0) {
+        const int G = gridDim.x;
+        const unsigned target = (sh.gen + 1) * (unsigned)G;
+        double bt[NS];
+#pragma unroll
+        for (int j = 0; j < NS; ++j) bt[j] = warp_sum(lane < W ? sh.red[j * W + lane] : 0.0);
+        if (lane == 0) {
+#pragma unroll
+            for (int j = 0; j < NS; ++j) P.part[(slot * 3 + j) * G + blockIdx.x] = bt[j];
+            red_release_add(P.bar + kCountWord, 1u);
+        }
+        __syncwarp();
+        int ok = 1;
+        unsigned spins = 0;
+        while ((int)(ld_acquire_u32(P.bar + kCountWord) - target) < 0) {
+            if (ld_volatile_u32(P.bar + kAbortWord)) {
+                ok = 0;
+                break;
+            }
+            if (++spins > kGridSpinLimit) {
+                if (lane == 0) {
+                    atomicOr(P.err, kErrTimeout);
+                    atomicExch(P.bar + kAbortWord, 1u);
+                }
+                ok = 0;
+                break;
+            }
+            if (spins > 64) __nanosleep(128);
+        }
+        ok = __all_sync(0xffffffffu, ok);
+        if (ok) {
+            double s[NS];
+#pragma unroll
+            for (int j = 0; j < NS; ++j) s[j] = 0.0;
+            for (int c = lane; c < G; c += 32) {
+#pragma unroll
+                for (int j = 0; j < NS; ++j) s[j] += __ldcg(P.part + (slot * 3 + j) * G + c);
+            }
+#pragma unroll
+            for (int j = 0; j < NS; ++j) s[j] = warp_sum(s[j]);
+            if (lane == 0) {
+#pragma unroll
+                for (int j = 0; j < NS; ++j) sh.tot[j] = s[j];
+            }
+        }
+        if (lane == 0) {
+            sh.gen = sh.gen + 1;
+            sh.ok = ok;
+        }
     }
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < NS; ++j) tot[j] = sh.tot[j];
-    return true;
+    return sh.ok != 0;
 }
 
 // Row li of a block of a CSR held in shared memory times a gathered vector:
@@ -259,10 +291,10 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
         double acc[1] = {0.0};
         const float* rc = P.r0;
         for (int li = tid; li < R; li += kPNT) {
-            const float s = row_f32(mrp, mci, mv, li, [&](int c) { return __ldcg(rc + c); });
+            const float s = row_f32(mrp, mci, mv, li, [&](int c) { return ldv(rc + c); });
             const int i = r0 + li;
             P.z[i] = s;
-            acc[0] += (double)__ldcg(rc + i) * (double)s;
+            acc[0] += (double)ldv(rc + i) * (double)s;
         }
         double tot[1];
         if (!reduce_all<1>(P, sh, 1, acc, tot)) goto out;
@@ -281,8 +313,8 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                 const float beta = (float)S.beta;
                 const bool jac = S.mode == 1;
                 auto dir = [&](int c) {
-                    const float zc = jac ? __ldcg(rc + c) * __ldg(dinv + c) : __ldcg(P.z + c);
-                    return beta != 0.f ? fmaf(beta, __ldcg(po + c), zc) : zc;
+                    const float zc = jac ? ldv(rc + c) * __ldg(dinv + c) : ldv(P.z + c);
+                    return beta != 0.f ? fmaf(beta, ldv(po + c), zc) : zc;
                 };
                 double acc[1] = {0.0};
                 auto own = [&](int li, float s) {
@@ -324,13 +356,13 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                 const float* pc = odd ? P.p1 : P.p0;
                 const double a = S.alpha;
                 const float af = (float)a;
-                auto res = [&](int c) { return fmaf(-af, __ldcg(P.q + c), __ldcg(rc + c)); };
+                auto res = [&](int c) { return fmaf(-af, ldv(P.q + c), ldv(rc + c)); };
                 double acc[3] = {0.0, 0.0, 0.0};
                 auto own = [&](int li, float s) {
                     const int i = r0 + li;
                     const float rv = res(i);
                     rn[i] = rv;
-                    P.x[i] = fma(a, (double)__ldcg(pc + i), __ldcg(P.x + i));
+                    P.x[i] = fma(a, (double)ldv(pc + i), ldv(P.x + i));
                     P.z[i] = s;
                     acc[0] += (double)rv * rv;
                     acc[1] += (double)rv * rv * dinv[i];
@@ -361,7 +393,7 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                     double s = 0.0;
                     const int e = arp[li + 1];
                     for (int k = arp[li]; k < e; ++k)
-                        s = __dadd_rn(s, __dmul_rn((double)av[k], __ldcg(P.x + aci[k])));
+                        s = __dadd_rn(s, __dmul_rn((double)av[k], ldv(P.x + aci[k])));
                     const int i = r0 + li;
                     const double rt = __ldg(P.b + i) - s;
                     const float rf = (float)rt;
@@ -397,10 +429,10 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                 const float* rc = (S.iter & 1) ? P.r1 : P.r0;
                 double acc[1] = {0.0};
                 for (int li = tid; li < R; li += kPNT) {
-                    const float s = row_f32(mrp, mci, mv, li, [&](int c) { return __ldcg(rc + c); });
+                    const float s = row_f32(mrp, mci, mv, li, [&](int c) { return ldv(rc + c); });
                     const int i = r0 + li;
                     P.z[i] = s;
-                    acc[0] += (double)__ldcg(rc + i) * (double)s;
+                    acc[0] += (double)ldv(rc + i) * (double)s;
                 }
                 double tot[1];
                 if (!reduce_all<1>(P, sh, 3, acc, tot)) goto out;
@@ -493,7 +525,7 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
                 double sd = 0.0;
                 const int e = arp[li + 1];
                 for (int k = arp[li]; k < e; ++k)
-                    sd = __dadd_rn(sd, __dmul_rn((double)av[k], __ldcg(P.x + aci[k])));
+                    sd = __dadd_rn(sd, __dmul_rn((double)av[k], ldv(P.x + aci[k])));
                 const int i = r0 + li;
                 const double rt = __ldg(P.b + i) - sd;
                 const float rf = (float)rt;
@@ -532,8 +564,8 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
             const float beta = (float)S.beta;
             const bool jac = S.mode == 1;
             auto dir = [&](int c) {
-                const float zc = jac ? __ldcg(r + c) * __ldg(P.dinv + c) : __ldcg(r + c);
-                return beta != 0.f ? fmaf(beta, __ldcg(po + c), zc) : zc;
+                const float zc = jac ? ldv(r + c) * __ldg(P.dinv + c) : ldv(r + c);
+                return beta != 0.f ? fmaf(beta, ldv(po + c), zc) : zc;
             };
             double acc[1] = {0.0};
             auto own = [&](int li, float sv) {
@@ -575,9 +607,9 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
             double acc[2] = {0.0, 0.0};
             for (int li = tid; li < R; li += kPNT) {
                 const int i = r0 + li;
-                if constexpr (IR) P.x[i] = fma(a64, (double)__ldcg(pc + i), __ldcg(P.x + i));
-                else P.x32[i] = fmaf(a, __ldcg(pc + i), __ldcg(P.x32 + i));
-                const float rv = fmaf(-a, __ldcg(P.q + i), __ldcg(r + i));
+                if constexpr (IR) P.x[i] = fma(a64, (double)ldv(pc + i), ldv(P.x + i));
+                else P.x32[i] = fmaf(a, ldv(pc + i), ldv(P.x32 + i));
+                const float rv = fmaf(-a, ldv(P.q + i), ldv(r + i));
                 r[i] = rv;
                 acc[0] += (double)rv * rv;
                 if (dinv) acc[1] += (double)rv * rv * dinv[i];
@@ -650,7 +682,7 @@ static cudaError_t plan_rows(PersistPlan& pp, const std::vector<int>& arp, const
     if (worst > kPSmemBudget) return cudaSuccess;   // rows do not fit: not eligible
     dev_free(pp.d_row_start);
     pp.d_row_start = nullptr;
-    // grid + 1 boundaries, then the barrier's three words
+    // grid + 1 boundaries, then the barrier words
     e = dev_alloc(&pp.d_row_start, (size_t)(grid + 1 + kBarWords) * 4, s);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(pp.d_row_start, start.data(), (size_t)(grid + 1) * 4, cudaMemcpyHostToDevice, s);
