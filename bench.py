@@ -1064,7 +1064,7 @@ def main():
                 "config": {"workload": WORKLOAD, "solver": res["solver"], "tol": TOL,
                            "l2": "flushed between steps (256 MB write)",
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-                "step_ms": res["step_ms"],
+                "step_ms": res["step_ms"], "step_host_ms": res["step_host_ms"],
                 "iters_mean": res["iters_mean"], "outer_mean": res["outer_mean"],
                 "true_resid_max": res["true_resid_max"],
                 "setup_ms_first_solve": res["setup_ms_first_solve"],

@@ -25,6 +25,7 @@
 // other waiter; the host checks the per-CTA shared-memory footprint before
 // choosing this form.
 #include <algorithm>
+#include <climits>
 #include <vector>
 
 #include "handles.hpp"
@@ -47,6 +48,7 @@ struct PersistDev {
     const int* m_ci;
     const float* m_v;
     const int* row_start;   // gridDim.x + 1 row boundaries
+    const int* win;         // per CTA [lo, hi): the columns its rows of A and M reach
     const float* dinv;      // Jacobi diagonal (fallback, and the r.D^-1 r sums)
     const double* b;        // FP64 right-hand side
     double* x;              // FP64 solution
@@ -225,6 +227,7 @@ __device__ __forceinline__ void row_pair_f32(const int* rp, const int* ci, const
     }
 }
 
+template <bool WIN>
 __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
     extern __shared__ __align__(16) unsigned char psmem[];
     __shared__ PersistShared sh;
@@ -240,6 +243,11 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
     int* mci = aci + na;
     float* av = reinterpret_cast<float*>(mci + nm);
     float* mv = av + na;
+    // WIN: the multiplied vector over the CTA's column window, staged once
+    // per step (coalesced loads) so the row sums read shared memory only
+    const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
+    float* win = mv + nm;
+    auto wg = [&](int c) { return win[c - wlo]; };
     for (int i = tid; i <= R; i += kPNT) {
         arp[i] = P.a_rp[r0 + i] - a0;
         mrp[i] = P.m_rp[r0 + i] - m0;
@@ -317,9 +325,13 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                     return beta != 0.f ? fmaf(beta, ldv(po + c), zc) : zc;
                 };
                 double acc[1] = {0.0};
+                if constexpr (WIN) {
+                    for (int k = wlo + tid; k < whi; k += kPNT) win[k - wlo] = dir(k);
+                    __syncthreads();
+                }
                 auto own = [&](int li, float s) {
                     const int i = r0 + li;
-                    const float pv = dir(i);
+                    const float pv = WIN ? win[i - wlo] : dir(i);
                     pn[i] = pv;
                     P.q[i] = s;
                     acc[0] += (double)pv * (double)s;
@@ -328,7 +340,8 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                     const int lj = li + kPNT;
                     const bool has1 = lj < R;
                     float s0, s1;
-                    row_pair_f32(arp, aci, av, li, lj, has1, dir, s0, s1);
+                    if constexpr (WIN) row_pair_f32(arp, aci, av, li, lj, has1, wg, s0, s1);
+                    else row_pair_f32(arp, aci, av, li, lj, has1, dir, s0, s1);
                     own(li, s0);
                     if (has1) own(lj, s1);
                 }
@@ -358,9 +371,13 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                 const float af = (float)a;
                 auto res = [&](int c) { return fmaf(-af, ldv(P.q + c), ldv(rc + c)); };
                 double acc[3] = {0.0, 0.0, 0.0};
+                if constexpr (WIN) {
+                    for (int k = wlo + tid; k < whi; k += kPNT) win[k - wlo] = res(k);
+                    __syncthreads();
+                }
                 auto own = [&](int li, float s) {
                     const int i = r0 + li;
-                    const float rv = res(i);
+                    const float rv = WIN ? win[i - wlo] : res(i);
                     rn[i] = rv;
                     P.x[i] = fma(a, (double)ldv(pc + i), ldv(P.x + i));
                     P.z[i] = s;
@@ -372,7 +389,8 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                     const int lj = li + kPNT;
                     const bool has1 = lj < R;
                     float s0, s1;
-                    row_pair_f32(mrp, mci, mv, li, lj, has1, res, s0, s1);
+                    if constexpr (WIN) row_pair_f32(mrp, mci, mv, li, lj, has1, wg, s0, s1);
+                    else row_pair_f32(mrp, mci, mv, li, lj, has1, res, s0, s1);
                     own(li, s0);
                     if (has1) own(lj, s1);
                 }
@@ -461,7 +479,7 @@ out:
 // IR (reliable updates, cg_mixed without FSAI): x accumulated in FP64
 // (P.x), b in FP64 (P.b), the stop rule of cg_finalize_ir, and -- when due --
 // the residual replacement r = (float)(b - A x) in FP64 in the same kernel.
-template <bool IR>
+template <bool IR, bool WIN>
 __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
     extern __shared__ __align__(16) unsigned char psmem[];
     __shared__ PersistShared sh;
@@ -473,6 +491,9 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
     int* arp = reinterpret_cast<int*>(psmem);
     int* aci = arp + (R + 1);
     float* av = reinterpret_cast<float*>(aci + na);
+    const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
+    float* win = av + na;
+    auto wg = [&](int c) { return win[c - wlo]; };
     for (int i = tid; i <= R; i += kPNT) arp[i] = P.a_rp[r0 + i] - a0;
     for (int k = tid; k < na; k += kPNT) {
         aci[k] = P.a_ci[a0 + k];
@@ -568,9 +589,13 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
                 return beta != 0.f ? fmaf(beta, ldv(po + c), zc) : zc;
             };
             double acc[1] = {0.0};
+            if constexpr (WIN) {
+                for (int c = wlo + tid; c < whi; c += kPNT) win[c - wlo] = dir(c);
+                __syncthreads();
+            }
             auto own = [&](int li, float sv) {
                 const int i = r0 + li;
-                const float pv = dir(i);
+                const float pv = WIN ? win[i - wlo] : dir(i);
                 pn[i] = pv;
                 P.q[i] = sv;
                 acc[0] += (double)pv * (double)sv;
@@ -579,7 +604,8 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
                 const int lj = li + kPNT;
                 const bool has1 = lj < R;
                 float s0, s1;
-                row_pair_f32(arp, aci, av, li, lj, has1, dir, s0, s1);
+                if constexpr (WIN) row_pair_f32(arp, aci, av, li, lj, has1, wg, s0, s1);
+                else row_pair_f32(arp, aci, av, li, lj, has1, dir, s0, s1);
                 own(li, s0);
                 if (has1) own(lj, s1);
             }
@@ -630,6 +656,47 @@ out:
     }
 }
 
+// Per CTA block: the smallest column, and one past the largest, that its
+// rows of A (and M) reference, widened to the block's own rows -- the window
+// of the multiplied vector the block's row sums read.
+__global__ void persist_window_kernel(const int* __restrict__ a_rp, const int* __restrict__ a_ci,
+                                      const int* __restrict__ m_rp, const int* __restrict__ m_ci,
+                                      const int* __restrict__ row_start, int* __restrict__ win) {
+    const int b = blockIdx.x;
+    const int r0 = row_start[b], r1 = row_start[b + 1];
+    int lo = r0, hi = r1;
+    for (int k = a_rp[r0] + threadIdx.x; k < a_rp[r1]; k += blockDim.x) {
+        const int c = a_ci[k];
+        lo = min(lo, c);
+        hi = max(hi, c + 1);
+    }
+    if (m_rp) {
+        for (int k = m_rp[r0] + threadIdx.x; k < m_rp[r1]; k += blockDim.x) {
+            const int c = m_ci[k];
+            lo = min(lo, c);
+            hi = max(hi, c + 1);
+        }
+    }
+    __shared__ int s_lo[32], s_hi[32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    if (lane == 0) {
+        s_lo[w] = lo;
+        s_hi[w] = hi;
+    }
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        lo = __reduce_min_sync(0xffffffffu, lane < nw ? s_lo[lane] : INT_MAX);
+        hi = __reduce_max_sync(0xffffffffu, lane < nw ? s_hi[lane] : INT_MIN);
+        if (lane == 0) {
+            win[2 * b] = lo;
+            win[2 * b + 1] = hi;
+        }
+    }
+}
+
 }  // namespace
 
 // Row blocks of A and M for one CTA per SM, balanced by their shared-memory
@@ -638,7 +705,7 @@ out:
 // balanced by their shared-memory bytes; pp.state = -1 when a block would
 // not fit or the kernel cannot be made resident (the graph form runs then).
 static cudaError_t plan_rows(PersistPlan& pp, const std::vector<int>& arp, const std::vector<int>* mrp,
-                             int n, const void* kernel, cudaStream_t s) {
+                             int n, const void* kernel, const CsrMat& A, const CsrMat* M, cudaStream_t s) {
     pp.state = -1;
     int per_sm = 0;
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -682,14 +749,32 @@ static cudaError_t plan_rows(PersistPlan& pp, const std::vector<int>& arp, const
     if (worst > kPSmemBudget) return cudaSuccess;   // rows do not fit: not eligible
     dev_free(pp.d_row_start);
     pp.d_row_start = nullptr;
-    // grid + 1 boundaries, then the barrier words
-    e = dev_alloc(&pp.d_row_start, (size_t)(grid + 1 + kBarWords) * 4, s);
+    // grid + 1 boundaries, the barrier words, then 2 window bounds per block
+    e = dev_alloc(&pp.d_row_start, (size_t)(grid + 1 + kBarWords + 2 * grid) * 4, s);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(pp.d_row_start, start.data(), (size_t)(grid + 1) * 4, cudaMemcpyHostToDevice, s);
+    int* d_win = pp.d_row_start + grid + 1 + kBarWords;
+    std::vector<int> win(2 * (size_t)grid);
+    if (e == cudaSuccess) {
+        persist_window_kernel<<<grid, 256, 0, s>>>(A.rp, A.ci, M ? M->rp : nullptr, M ? M->ci : nullptr,
+                                                   pp.d_row_start, d_win);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(win.data(), d_win, win.size() * 4, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return e;
+    // window form when every block's rows plus its vector window fit
+    size_t worst_win = 0;
+    for (int c = 0; c < grid; ++c) {
+        const int rows = start[c + 1] - start[c];
+        size_t b = 4 * (size_t)words * ((size_t)rows + 1) + 8 * (size_t)(arp[start[c + 1]] - arp[start[c]]);
+        if (mrp) b += 8 * (size_t)((*mrp)[start[c + 1]] - (*mrp)[start[c]]);
+        b += 4 * (size_t)(win[2 * c + 1] - win[2 * c]);
+        worst_win = std::max(worst_win, b);
+    }
     pp.grid = grid;
-    pp.smem = ((worst + 15) / 16) * 16;
+    pp.win = worst_win <= kPSmemBudget ? 1 : 0;
+    pp.smem = (((pp.win ? worst_win : worst) + 15) / 16) * 16;
     pp.state = 1;
     return cudaSuccess;
 }
@@ -710,7 +795,7 @@ cudaError_t persist_plan_build(mps_csr* h, cudaStream_t s) {
     if (e == cudaSuccess) e = host_row_ptr(h->M, mrp, s);
     if (e != cudaSuccess) return e;
     return plan_rows(h->pp, arp, &mrp, (int)h->A.n_rows,
-                     reinterpret_cast<const void*>(fsai_pcg_persistent), s);
+                     reinterpret_cast<const void*>(fsai_pcg_persistent<false>), h->A, &h->M, s);
 }
 
 // Plan of the CG form (rows of A only).
@@ -721,7 +806,7 @@ cudaError_t persist_plan_build_a(mps_csr* h, cudaStream_t s) {
     const cudaError_t e = host_row_ptr(h->A, arp, s);
     if (e != cudaSuccess) return e;
     return plan_rows(h->pp_a, arp, nullptr, (int)h->A.n_rows,
-                     reinterpret_cast<const void*>(cg_persistent<false>), s);
+                     reinterpret_cast<const void*>(cg_persistent<false, false>), h->A, nullptr, s);
 }
 
 // Plain CG / Jacobi-PCG as one cooperative launch: b is H.v(vB), x lands in
@@ -756,8 +841,12 @@ cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s, const double* b64, doub
     P.x32 = H.v(vX);
     P.b = b64;
     P.x = x64;
-    const void* k = b64 ? reinterpret_cast<const void*>(cg_persistent<true>)
-                        : reinterpret_cast<const void*>(cg_persistent<false>);
+    P.win = h->pp_a.d_row_start + h->pp_a.grid + 1 + kBarWords;
+    const bool w = h->pp_a.win != 0;
+    const void* k = b64 ? (w ? reinterpret_cast<const void*>(cg_persistent<true, true>)
+                             : reinterpret_cast<const void*>(cg_persistent<true, false>))
+                        : (w ? reinterpret_cast<const void*>(cg_persistent<false, true>)
+                             : reinterpret_cast<const void*>(cg_persistent<false, false>));
     cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->pp_a.smem);
@@ -812,14 +901,15 @@ cudaError_t persist_solve(mps_csr* h, const double* b64, double* x64, cudaStream
     P.prm = H.ws.d_params;
     P.n = (int)h->A.n_rows;
     static_assert(4 * 3 * 1024 <= 4 * kMaxPartials, "partial slots");
+    P.win = h->pp.d_row_start + h->pp.grid + 1 + kBarWords;
+    const void* k = h->pp.win ? reinterpret_cast<const void*>(fsai_pcg_persistent<true>)
+                              : reinterpret_cast<const void*>(fsai_pcg_persistent<false>);
     cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(fsai_pcg_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)h->pp.smem);
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->pp.smem);
     if (e != cudaSuccess) return e;
     void* args[] = {&P};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(fsai_pcg_persistent), dim3(h->pp.grid),
-                                       dim3(kPNT), args, h->pp.smem, s);
+    return cudaLaunchCooperativeKernel(k, dim3(h->pp.grid), dim3(kPNT), args, h->pp.smem, s);
 }
 
 }  // namespace mps

@@ -200,3 +200,42 @@ def test_persistent_reliable_cg_matches_graph_form(mps, oracle, precond):
     x = torch.ones(c.n, dtype=torch.float64, device="cuda")
     info = A.cg_mixed(torch.zeros_like(b), x, precond=precond)
     assert info["persistent"] and info["converged"] and float(x.abs().max()) == 0.0
+
+
+def test_persistent_gather_form_on_random_graph(mps, oracle):
+    """A random graph Laplacian (60,000 rows, mean degree 6): every row block
+    couples to columns all over the matrix, so the blocks' vector windows do
+    not fit beside their rows and the persistent kernels gather the vector
+    entries instead.  Plain CG and learned-FSAI mixed-precision PCG both
+    agree with the graph form (first iterates) and reach their targets."""
+    c = W.graph_laplacian(60000, 6.0, 3, shift=0.05)
+    A = _cg_system(mps, c)
+    Ao = oracle.Csr(*c.to_csr(), c.n)
+    b = W.rhs(c.n, 7)
+    bt = torch.from_numpy(b).cuda()
+    for k in (1, 5, 20):
+        xs = []
+        for persistent in (True, False):
+            A.set_persistent(persistent)
+            x = torch.zeros(c.n, device="cuda")
+            info = A.cgd(bt, x, tol=1e-300, max_iter=k)
+            assert info["iters"] == k and info["persistent"] == persistent
+            xs.append(x)
+        assert float((xs[0] - xs[1]).norm() / xs[1].norm()) <= 1e-6, k
+    A.set_persistent(True)
+    x = torch.zeros(c.n, device="cuda")
+    info = A.cgd(bt, x, tol=1e-6, max_iter=20000)
+    assert info["persistent"] and info["stop_rule_met"]
+    from mpsparse_b200.fsai import LearnedFsai
+    LearnedFsai.load().attach(A)
+    A.set_fsai_apply("product")
+    b64 = bt.double()
+    sols = []
+    for persistent in (True, False):
+        A.set_persistent(persistent)
+        x = torch.zeros(c.n, dtype=torch.float64, device="cuda")
+        info = A.cg_mixed(b64, x, tol=1e-8, inner_tol=1e-3, max_inner=40000, precond="fsai")
+        assert info["converged"] and info["persistent"] == persistent, info
+        assert oracle.true_residual(Ao, b, x.cpu().numpy()) <= 1e-8 * 1.01
+        sols.append(x)
+    assert float((sols[0] - sols[1]).norm() / sols[1].norm()) <= 1e-6
