@@ -35,6 +35,7 @@ namespace {
 
 constexpr int kPNT = 1024;                       // threads per CTA
 constexpr size_t kPSmemBudget = 200 * 1024;      // matrix rows per CTA (dynamic shared memory)
+constexpr size_t kPSmemWinBudget = 220 * 1024;   // window form: rows, vector window, own x and D^-1
 constexpr unsigned kGridSpinLimit = 1u << 22;    // polls of one barrier wait (about a second)
 constexpr int kCountWord = 0;                    // barrier words: [0] arrivals (monotonic),
 constexpr int kAbortWord = 2;                    // [2] abort
@@ -112,15 +113,20 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
 //      per poll for the warp) and then sums all CTAs' partials -- lane l the
 //      partials l, l + 32, ..., then a butterfly -- so every CTA adds the same
 //      partials in the same order and gets the same bits;
-//   4. one bar.sync hands the totals to the CTA.
+//   4. thread 0 applies `fin` to the totals (the solver's scalar update), and
+//      one bar.sync hands both to the CTA.
 // Consecutive reductions must use different slots: a CTA may store its next
 // partials while a slower CTA still reads these.  The wait is bounded
 // (kGridSpinLimit polls, back-off after 64); a timeout raises the error word
 // and the abort word, and the abort word ends every other CTA's wait.
 // false: this CTA gave up (timeout or abort).
-template <int NS>
+struct NoFin {
+    __device__ void operator()(const double*) const {}
+};
+
+template <int NS, class Fin = NoFin>
 __device__ bool reduce_all(const PersistDev& P, PersistShared& sh, int slot, double (&acc)[NS],
-                           double (&tot)[NS]) {
+                           double (&tot)[NS], Fin fin = Fin{}) {
     constexpr int W = kPNT / 32;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
@@ -173,6 +179,7 @@ __device__ bool reduce_all(const PersistDev& P, PersistShared& sh, int slot, dou
             if (lane == 0) {
 #pragma unroll
                 for (int j = 0; j < NS; ++j) sh.tot[j] = s[j];
+                fin(s);   // scalar updates from the totals, before the bar.sync
             }
         }
         if (lane == 0) {
@@ -184,6 +191,21 @@ __device__ bool reduce_all(const PersistDev& P, PersistShared& sh, int slot, dou
 #pragma unroll
     for (int j = 0; j < NS; ++j) tot[j] = sh.tot[j];
     return sh.ok != 0;
+}
+
+// win[k - lo] = f(k) for k in [lo, hi): each thread loads up to four
+// entries before it stores any, so their global loads are in flight
+// together (a window is about three entries per thread).
+template <class F>
+__device__ __forceinline__ void fill_window(float* win, int lo, int hi, F f) {
+    for (int k0 = lo + (int)threadIdx.x; k0 < hi; k0 += 4 * kPNT) {
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = k0 + u * kPNT < hi ? f(k0 + u * kPNT) : 0.f;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k0 + u * kPNT < hi) win[k0 + u * kPNT - lo] = v[u];
+    }
 }
 
 // Row li of a block of a CSR held in shared memory times a gathered vector:
@@ -244,9 +266,13 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
     float* av = reinterpret_cast<float*>(mci + nm);
     float* mv = av + na;
     // WIN: the multiplied vector over the CTA's column window, staged once
-    // per step (coalesced loads) so the row sums read shared memory only
+    // per step (coalesced loads) so the row sums read shared memory only;
+    // the own rows' x (FP64, written through to global) and D^-1 stay in
+    // shared memory too:  ... mv | xs[R] | ds[R] | win[hi - lo]
     const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
-    float* win = mv + nm;
+    double* xs = reinterpret_cast<double*>(mv + nm);
+    float* ds = reinterpret_cast<float*>(xs + (WIN ? R : 0));
+    float* win = ds + (WIN ? R : 0);
     auto wg = [&](int c) { return win[c - wlo]; };
     for (int i = tid; i <= R; i += kPNT) {
         arp[i] = P.a_rp[r0 + i] - a0;
@@ -259,6 +285,12 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
     for (int k = tid; k < nm; k += kPNT) {
         mci[k] = P.m_ci[m0 + k];
         mv[k] = P.m_v[m0 + k];
+    }
+    if constexpr (WIN) {
+        for (int li = tid; li < R; li += kPNT) {
+            xs[li] = 0.0;
+            ds[li] = P.dinv[r0 + li];
+        }
     }
     if (tid == 0) {
         sh.gen = 0;
@@ -326,7 +358,7 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                 };
                 double acc[1] = {0.0};
                 if constexpr (WIN) {
-                    for (int k = wlo + tid; k < whi; k += kPNT) win[k - wlo] = dir(k);
+                    fill_window(win, wlo, whi, dir);
                     __syncthreads();
                 }
                 auto own = [&](int li, float s) {
@@ -346,20 +378,28 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                     if (has1) own(lj, s1);
                 }
                 double tot[1];
-                if (!reduce_all<1>(P, sh, 0, acc, tot)) goto out;
-                if (tid == 0) {
-                    const double pq = tot[0];
-                    S.pq = pq;
-                    if (!(pq > 0.0) || !isfinite(pq)) {
-                        S.breakdown = 1;
-                        S.done = 1;
-                        S.alpha = 0.0;
-                    } else {
-                        S.alpha = S.rz / pq;
+                if (!reduce_all<1>(P, sh, 0, acc, tot, [&](const double* t) {
+                        const double pq = t[0];
+                        S.pq = pq;
+                        if (!(pq > 0.0) || !isfinite(pq)) {
+                            S.breakdown = 1;
+                            S.done = 1;
+                            S.alpha = 0.0;
+                        } else {
+                            S.alpha = S.rz / pq;
+                        }
+                    }))
+                    goto out;
+                if (S.done) break;
+                if constexpr (WIN) {
+                    // x += alpha p (FP64) while the window still holds p
+                    const double a = S.alpha;
+                    for (int li = tid; li < R; li += kPNT) {
+                        const double xv = fma(a, (double)win[r0 + li - wlo], xs[li]);
+                        xs[li] = xv;
+                        P.x[r0 + li] = xv;
                     }
                 }
-                __syncthreads();
-                if (S.done) break;
             }
             // ---- step 2: r' = r - alpha q on the fly, z = M r', x += alpha p
             {
@@ -372,17 +412,17 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                 auto res = [&](int c) { return fmaf(-af, ldv(P.q + c), ldv(rc + c)); };
                 double acc[3] = {0.0, 0.0, 0.0};
                 if constexpr (WIN) {
-                    for (int k = wlo + tid; k < whi; k += kPNT) win[k - wlo] = res(k);
+                    fill_window(win, wlo, whi, res);
                     __syncthreads();
                 }
                 auto own = [&](int li, float s) {
                     const int i = r0 + li;
                     const float rv = WIN ? win[i - wlo] : res(i);
                     rn[i] = rv;
-                    P.x[i] = fma(a, (double)ldv(pc + i), ldv(P.x + i));
+                    if constexpr (!WIN) P.x[i] = fma(a, (double)ldv(pc + i), ldv(P.x + i));
                     P.z[i] = s;
                     acc[0] += (double)rv * rv;
-                    acc[1] += (double)rv * rv * dinv[i];
+                    acc[1] += (double)rv * rv * (WIN ? ds[li] : dinv[i]);
                     acc[2] += (double)rv * (double)s;
                 };
                 for (int li = tid; li < R; li += 2 * kPNT) {
@@ -395,12 +435,11 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                     if (has1) own(lj, s1);
                 }
                 double tot[3];
-                if (!reduce_all<3>(P, sh, 1, acc, tot)) goto out;
-                if (tid == 0) {
-                    cg_finalize_ir(&S, tot[0], tot[1]);
-                    if (!S.replace && !S.done && S.mode == 2) fsai_beta(&S, tot[2]);
-                }
-                __syncthreads();
+                if (!reduce_all<3>(P, sh, 1, acc, tot, [&](const double* t) {
+                        cg_finalize_ir(&S, t[0], t[1]);
+                        if (!S.replace && !S.done && S.mode == 2) fsai_beta(&S, t[2]);
+                    }))
+                    goto out;
             }
         } else {
             // ---- replacement: r = (float)(b - A x) in FP64 ------------------
@@ -590,7 +629,7 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
             };
             double acc[1] = {0.0};
             if constexpr (WIN) {
-                for (int c = wlo + tid; c < whi; c += kPNT) win[c - wlo] = dir(c);
+                fill_window(win, wlo, whi, dir);
                 __syncthreads();
             }
             auto own = [&](int li, float sv) {
@@ -770,10 +809,21 @@ static cudaError_t plan_rows(PersistPlan& pp, const std::vector<int>& arp, const
         size_t b = 4 * (size_t)words * ((size_t)rows + 1) + 8 * (size_t)(arp[start[c + 1]] - arp[start[c]]);
         if (mrp) b += 8 * (size_t)((*mrp)[start[c + 1]] - (*mrp)[start[c]]);
         b += 4 * (size_t)(win[2 * c + 1] - win[2 * c]);
+        if (mrp) b += 12 * (size_t)rows;   // FSAI form: the own rows' x (FP64) and D^-1
         worst_win = std::max(worst_win, b);
     }
     pp.grid = grid;
-    pp.win = worst_win <= kPSmemBudget ? 1 : 0;
+    pp.win = worst_win <= kPSmemWinBudget ? 1 : 0;
+    if (pp.win) {   // the larger footprint must still leave one CTA resident per SM
+        const int sz = (int)(((worst_win + 15) / 16) * 16);
+        int per = 0;
+        cudaError_t ew = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
+        if (ew == cudaSuccess) ew = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kPNT, sz);
+        if (ew != cudaSuccess || per < 1) {
+            cudaGetLastError();
+            pp.win = 0;
+        }
+    }
     pp.smem = (((pp.win ? worst_win : worst) + 15) / 16) * 16;
     pp.state = 1;
     return cudaSuccess;
