@@ -167,12 +167,27 @@ __device__ bool reduce_all(const PersistDev& P, PersistShared& sh, int slot, dou
         }
         ok = __all_sync(0xffffffffu, ok);
         if (ok) {
+            // all of a lane's partials are loaded before any is added (one
+            // L2 round trip, not one per partial); added in CTA order
+            constexpr int U = 5;   // 5 * 32 = 160 CTAs per round
             double s[NS];
 #pragma unroll
             for (int j = 0; j < NS; ++j) s[j] = 0.0;
-            for (int c = lane; c < G; c += 32) {
+            for (int c0 = lane; c0 < G; c0 += 32 * U) {
+                double v[U][NS];
 #pragma unroll
-                for (int j = 0; j < NS; ++j) s[j] += __ldcg(P.part + (slot * 3 + j) * G + c);
+                for (int u = 0; u < U; ++u) {
+#pragma unroll
+                    for (int j = 0; j < NS; ++j)
+                        v[u][j] = c0 + 32 * u < G ? __ldcg(P.part + (slot * 3 + j) * G + c0 + 32 * u) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    if (c0 + 32 * u < G) {
+#pragma unroll
+                        for (int j = 0; j < NS; ++j) s[j] += v[u][j];
+                    }
+                }
             }
 #pragma unroll
             for (int j = 0; j < NS; ++j) s[j] = warp_sum(s[j]);
@@ -526,12 +541,21 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
     const int r0 = P.row_start[blockIdx.x], r1 = P.row_start[blockIdx.x + 1];
     const int R = r1 - r0;
     const int a0 = P.a_rp[r0], na = P.a_rp[r1] - a0;
-    // shared layout: arp[R+1] | aci[na] | av[na]
+    // shared layout: arp[R+1] | aci[na] | av[na]; window form adds the own
+    // rows' x (FP64 under IR, written through to global), r (written
+    // through), q and D^-1, then the vector window:
+    //   ... av | pad to 8 | xs[R] | rs[R] | qs[R] | ds[R] | win[hi - lo]
+    using XT = std::conditional_t<IR, double, float>;
     int* arp = reinterpret_cast<int*>(psmem);
     int* aci = arp + (R + 1);
     float* av = reinterpret_cast<float*>(aci + na);
     const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
-    float* win = av + na;
+    const size_t tail = ((size_t)(4 * (R + 1) + 8 * na) + 7) & ~(size_t)7;
+    XT* xs = reinterpret_cast<XT*>(psmem + tail);
+    float* rs = reinterpret_cast<float*>(xs + (WIN ? R : 0));
+    float* qs = rs + (WIN ? R : 0);
+    float* ds = qs + (WIN ? R : 0);
+    float* win = WIN ? ds + R : av + na;
     auto wg = [&](int c) { return win[c - wlo]; };
     for (int i = tid; i <= R; i += kPNT) arp[i] = P.a_rp[r0 + i] - a0;
     for (int k = tid; k < na; k += kPNT) {
@@ -549,6 +573,9 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
     const int mode0 = P.prm->precond;            // 0 none, 1 Jacobi
     const float* dinv = mode0 == 1 ? P.dinv : nullptr;
     float* r = P.r0;
+    if constexpr (WIN) {
+        for (int li = tid; li < R; li += kPNT) ds[li] = dinv ? dinv[r0 + li] : 1.f;
+    }
     {
         // x = 0, r = b; b.b and b.D^-1 b
         double acc[2] = {0.0, 0.0};
@@ -559,12 +586,20 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
                 const float bf = (float)bd;
                 P.x[i] = 0.0;
                 r[i] = bf;
+                if constexpr (WIN) {
+                    xs[li] = 0.0;
+                    rs[li] = bf;
+                }
                 if (dinv) acc[1] += (double)bf * bf * dinv[i];
                 acc[0] += bd * bd;
             } else {
                 const float bf = P.b32[i];
                 P.x32[i] = 0.f;
                 r[i] = bf;
+                if constexpr (WIN) {
+                    xs[li] = 0.f;
+                    rs[li] = bf;
+                }
                 if (dinv) acc[1] += (double)bf * bf * dinv[i];
                 acc[0] += (double)bf * bf;
             }
@@ -590,6 +625,7 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
                 const double rt = __ldg(P.b + i) - sd;
                 const float rf = (float)rt;
                 r[i] = rf;
+                if constexpr (WIN) rs[li] = rf;
                 acc[0] += rt * rt;
                 acc[1] += (double)rf * rf * (dinv ? dinv[i] : 1.f);
             }
@@ -636,7 +672,8 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
                 const int i = r0 + li;
                 const float pv = WIN ? win[i - wlo] : dir(i);
                 pn[i] = pv;
-                P.q[i] = sv;
+                if constexpr (WIN) qs[li] = sv;
+                else P.q[i] = sv;
                 acc[0] += (double)pv * (double)sv;
             };
             for (int li = tid; li < R; li += 2 * kPNT) {
@@ -649,19 +686,18 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
                 if (has1) own(lj, s1);
             }
             double tot[1];
-            if (!reduce_all<1>(P, sh, 0, acc, tot)) goto out;
-            if (tid == 0) {
-                const double pq = tot[0];
-                S.pq = pq;
-                if (!(pq > 0.0) || !isfinite(pq)) {
-                    S.breakdown = 1;
-                    S.done = 1;
-                    S.alpha = 0.0;
-                } else {
-                    S.alpha = S.rz / pq;
-                }
-            }
-            __syncthreads();
+            if (!reduce_all<1>(P, sh, 0, acc, tot, [&](const double* t) {
+                    const double pq = t[0];
+                    S.pq = pq;
+                    if (!(pq > 0.0) || !isfinite(pq)) {
+                        S.breakdown = 1;
+                        S.done = 1;
+                        S.alpha = 0.0;
+                    } else {
+                        S.alpha = S.rz / pq;
+                    }
+                }))
+                goto out;
             if (S.done) break;
         }
         // ---- step 2: x += alpha p, r -= alpha q, r.r, r.D^-1 r -------------
@@ -672,20 +708,40 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
             double acc[2] = {0.0, 0.0};
             for (int li = tid; li < R; li += kPNT) {
                 const int i = r0 + li;
-                if constexpr (IR) P.x[i] = fma(a64, (double)ldv(pc + i), ldv(P.x + i));
-                else P.x32[i] = fmaf(a, ldv(pc + i), ldv(P.x32 + i));
-                const float rv = fmaf(-a, ldv(P.q + i), ldv(r + i));
-                r[i] = rv;
-                acc[0] += (double)rv * rv;
-                if (dinv) acc[1] += (double)rv * rv * dinv[i];
+                float rv;
+                if constexpr (WIN) {
+                    // p is still in the window; x, r, q, D^-1 of own rows in
+                    // shared memory (x and r written through)
+                    const float pv = win[i - wlo];
+                    if constexpr (IR) {
+                        const double xv = fma(a64, (double)pv, xs[li]);
+                        xs[li] = xv;
+                        P.x[i] = xv;
+                    } else {
+                        const float xv = fmaf(a, pv, xs[li]);
+                        xs[li] = xv;
+                        P.x32[i] = xv;
+                    }
+                    rv = fmaf(-a, qs[li], rs[li]);
+                    rs[li] = rv;
+                    r[i] = rv;
+                    acc[0] += (double)rv * rv;
+                    if (dinv) acc[1] += (double)rv * rv * ds[li];
+                } else {
+                    if constexpr (IR) P.x[i] = fma(a64, (double)ldv(pc + i), ldv(P.x + i));
+                    else P.x32[i] = fmaf(a, ldv(pc + i), ldv(P.x32 + i));
+                    rv = fmaf(-a, ldv(P.q + i), ldv(r + i));
+                    r[i] = rv;
+                    acc[0] += (double)rv * rv;
+                    if (dinv) acc[1] += (double)rv * rv * dinv[i];
+                }
             }
             double tot[2];
-            if (!reduce_all<2>(P, sh, 1, acc, tot)) goto out;
-            if (tid == 0) {
-                if constexpr (IR) cg_finalize_ir(&S, tot[0], tot[1]);
-                else cg_finalize_xr(&S, tot[0], tot[1]);
-            }
-            __syncthreads();
+            if (!reduce_all<2>(P, sh, 1, acc, tot, [&](const double* t) {
+                    if constexpr (IR) cg_finalize_ir(&S, t[0], t[1]);
+                    else cg_finalize_xr(&S, t[0], t[1]);
+                }))
+                goto out;
         }
     }
 out:
@@ -810,6 +866,7 @@ static cudaError_t plan_rows(PersistPlan& pp, const std::vector<int>& arp, const
         if (mrp) b += 8 * (size_t)((*mrp)[start[c + 1]] - (*mrp)[start[c]]);
         b += 4 * (size_t)(win[2 * c + 1] - win[2 * c]);
         if (mrp) b += 12 * (size_t)rows;   // FSAI form: the own rows' x (FP64) and D^-1
+        else b += 8 + 20 * (size_t)rows;   // CG form: x (FP64 at most), r, q, D^-1
         worst_win = std::max(worst_win, b);
     }
     pp.grid = grid;
