@@ -136,6 +136,20 @@ def evaluate(fsai: LearnedFsai | None, seeds, spec=SPEC_512, tol=1e-6, max_iter=
                          "converged": bool(info["converged"])}
             if timed:
                 row[name]["ms"] = ms
+        # Jacobi-PCG with the learned solve's precision scheme (FP64 x,
+        # residual replacement): the like-for-like FP64-checked comparison
+        b64j = b.double()
+
+        def jacobi_mp():
+            x = torch.zeros(n, dtype=torch.float64, device="cuda")
+            return A.cg_mixed(b64j, x, tol=tol, inner_tol=inner_tol, max_inner=max_iter, precond="jacobi")
+        info, ms = _timed(jacobi_mp)
+        if timed:
+            info, ms = _timed(jacobi_mp)
+        row["jacobi_mp"] = {"iters": info["inner_iters"], "true_resid": info["rel_resid"],
+                            "converged": bool(info["converged"])}
+        if timed:
+            row["jacobi_mp"]["ms"] = ms
         rows.append(row)
     return rows
 
@@ -143,7 +157,7 @@ def evaluate(fsai: LearnedFsai | None, seeds, spec=SPEC_512, tol=1e-6, max_iter=
 def summarize(rows):
     """Mean / median / 95th percentile of iterations and times per method."""
     out = {"systems": len(rows)}
-    for name in ("fsai", "jacobi", "none"):
+    for name in ("fsai", "jacobi", "none", "jacobi_mp"):
         if name not in rows[0]:
             continue
         it = np.array([r[name]["iters"] for r in rows], np.float64)
@@ -159,6 +173,9 @@ def summarize(rows):
     if "fsai" in out:
         out["fsai_fewer_iters_than_jacobi"] = int(sum(r["fsai"]["iters"] < r["jacobi"]["iters"]
                                                      for r in rows))
+        if "ms" in rows[0]["fsai"]:
+            out["fsai_faster_than_jacobi_mp"] = int(sum(r["fsai"]["ms"] < r["jacobi_mp"]["ms"]
+                                                        for r in rows))
     return out
 
 
