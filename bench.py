@@ -49,6 +49,9 @@ UNIT = "ms"
 WORKLOAD = "512x512 log-normal diffusion (2D 5-pt, sigma 1.5, corr 16), held-out seeds"
 TEST_SEED0 = 100_000        # held-out seeds start here (training uses 0..1999)
 TOL = 1e-6
+# C1 (256^2 Laplacian, n 65,536, nnz 326,656): bytes of one CG iteration in
+# the reference's schedule, SpMV 3,399,684 + 36 n
+C1_ITER_BYTES = 3_399_684 + 36 * 65_536
 MAX_ITER = 40_000
 
 
@@ -703,7 +706,9 @@ def vendor_baselines(A, keys, vals, x, n, nnz, bytes_alg, stream):
                         stream, 3)
     return {"cusparse_spmv_ms": sp_ms, "cusparse_spmv_gbs": bytes_alg / (sp_ms * 1e-3) / 1e9,
             "cub_sort_keys_ms": sort_ms, "ours_coo_to_csr_ms": ours_ms,
-            "ours_coo_to_csr_gbs_onepass_model": (20 * nnz + 4 * (n + 1)) / (ours_ms * 1e-3) / 1e9}
+            "ours_coo_to_csr_gbs_onepass_model": (20 * nnz + 4 * (n + 1)) / (ours_ms * 1e-3) / 1e9,
+            # the reference's own byte model (spmv_kernel/spmv/benchmark.py:63-68)
+            "ours_coo_to_csr_gbs_ref_model": (16 * nnz + 4 * n) / (ours_ms * 1e-3) / 1e9}
 
 
 # ------------------------------------------------- the other configurations --
@@ -784,6 +789,11 @@ def c1_leg(dev, flush):
             "solver": "cgd (plain FP32 CG), tol 1e-6, max 2000", "ms": ms, "iters": info["iters"],
             "oracle_fp64_iters": io["iters"], "true_resid": info["true_resid"],
             "converged_fp64": bool(info["converged"]),
+            "persistent": bool(info["persistent"]),
+            # algorithmic bytes of one iteration of the reference's 3-kernel
+            # schedule: SpMV (8 nnz + 4 (n+1) + 8 n) + 9 vector passes (36 n)
+            "cg_iteration_bytes_model": C1_ITER_BYTES,
+            "gbs_model": C1_ITER_BYTES * info["iters"] / (ms * 1e-3) / 1e9,
             "iterate20_rel_diff_vs_oracle": _rel(x20.cpu().numpy(), xo20),
             "mixed_precision_cg": {"ms": ms_mp, "iters": imp["inner_iters"],
                                    "replacements": imp["outer_iters"],
@@ -839,6 +849,9 @@ def c2_leg(dev, flush):
             "solver": "bicgstab (plain FP32), tol 1e-6", "ms": ms, "iters": info["iters"],
             "oracle_fp64_iters": io["iters"], "true_resid": info["true_resid"],
             "converged_fp64": bool(info["converged"]),
+            # one BiCGSTAB iteration: 2 BCSR SpMVs + 17 vector passes (68 n)
+            "bicgstab_iteration_bytes_model": 2 * bytes_alg + 68 * n,
+            "gbs_model": (2 * bytes_alg + 68 * n) * info["iters"] / (ms * 1e-3) / 1e9,
             "bcsr_spmv": {"bytes_per_launch": bytes_alg, "ms_l2_flushed": mv_cold,
                           "gbs_l2_flushed": bytes_alg / (mv_cold * 1e-3) / 1e9,
                           "ms_l2_resident": mv_warm,
@@ -1082,7 +1095,8 @@ def main():
                 "config": {"workload": WORKLOAD, "solver": res["solver"], "tol": TOL,
                            "l2": "flushed between steps (256 MB write)",
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-                "step_ms": res["step_ms"], "step_host_ms": res["step_host_ms"],
+                "step_ms": res["step_ms"], "ms_median": statistics.median(res["step_ms"]),
+                "step_host_ms": res["step_host_ms"],
                 "iters_mean": res["iters_mean"], "outer_mean": res["outer_mean"],
                 "true_resid_max": res["true_resid_max"],
                 "setup_ms_first_solve": res["setup_ms_first_solve"],
