@@ -209,6 +209,56 @@ __device__ __forceinline__ void grp_dot2(const Grp& G, const int* __restrict__ r
     }
 }
 
+// Rows lo + lt, lo + lt + GS, ... of a CSR times x, two rows (i, i + GS)
+// per trip as grp_dot2 does, with the next pair's row bounds loaded before
+// this pair's products (one dependent memory round trip less per trip);
+// emit(row, sum) in row order.
+template <class Grp, class F>
+__device__ __forceinline__ void grp_spmv_rows(const Grp& G, const int* __restrict__ rp,
+                                              const int* __restrict__ ci, const float* __restrict__ v,
+                                              const float* x, int lo, int hi, F emit) {
+    constexpr int GS = Grp::GS;
+    int i = lo + G.lt;
+    if (i >= hi) return;
+    int j = i + GS;
+    int b0 = __ldg(rp + i), e0 = __ldg(rp + i + 1);
+    int b1 = j < hi ? __ldg(rp + j) : 0, e1 = j < hi ? __ldg(rp + j + 1) : 0;
+    for (;;) {
+        const int in = i + 2 * GS, jn = in + GS;
+        const int nb0 = in < hi ? __ldg(rp + in) : 0, ne0 = in < hi ? __ldg(rp + in + 1) : 0;
+        const int nb1 = jn < hi ? __ldg(rp + jn) : 0, ne1 = jn < hi ? __ldg(rp + jn + 1) : 0;
+        float s0 = 0.f, s1 = 0.f;
+        const int len = max(e0 - b0, e1 - b1);
+        for (int k = 0; k < len; k += 4) {
+            float x0[4], x1[4], v0[4], v1[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const bool in0 = b0 + k + u < e0, in1 = b1 + k + u < e1;
+                const int c0 = in0 ? __ldg(ci + b0 + k + u) : 0;
+                const int c1 = in1 ? __ldg(ci + b1 + k + u) : 0;
+                v0[u] = in0 ? __ldg(v + b0 + k + u) : 0.f;
+                v1[u] = in1 ? __ldg(v + b1 + k + u) : 0.f;
+                x0[u] = in0 ? G.gather(x, c0) : 0.f;
+                x1[u] = in1 ? G.gather(x, c1) : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (b0 + k + u < e0) s0 = fmaf(v0[u], x0[u], s0);
+                if (b1 + k + u < e1) s1 = fmaf(v1[u], x1[u], s1);
+            }
+        }
+        emit(i, s0);
+        if (j < hi) emit(j, s1);
+        if (in >= hi) break;
+        i = in;
+        j = jn;
+        b0 = nb0;
+        e0 = ne0;
+        b1 = nb1;
+        e1 = ne1;
+    }
+}
+
 // b_i - (A x)_i in FP64 for an FP64 x (exact products of the FP32 values).
 template <class Grp>
 __device__ __forceinline__ double grp_resid64(const Grp& G, const int* __restrict__ rp,
@@ -293,29 +343,45 @@ __device__ __forceinline__ void batch_pcg_body(const BatchDev& B, const float* _
         }
         while (!conv && it < max_iter) {
             double a[1] = {0.0};
-            for (int i = lo + lt; i < hi; i += 2 * GS) {
-                const int j = i + GS;
-                float q0, q1;
-                grp_dot2(G, B.rp, B.ci, B.v, B.p, i, j, j < hi, q0, q1);
-                B.q[i] = q0;
-                a[0] += (double)B.p[i] * q0;
-                if (j < hi) {
-                    B.q[j] = q1;
-                    a[0] += (double)B.p[j] * q1;
-                }
-            }
+            grp_spmv_rows(G, B.rp, B.ci, B.v, B.p, lo, hi, [&](int i, float qi) {
+                B.q[i] = qi;
+                a[0] += (double)B.p[i] * qi;
+            });
             G.template reduce<1>(a, sh);
             if (!(a[0] > 0.0)) break;             // breakdown (not SPD)
             const double alpha64 = rz / a[0];
             const float alpha = (float)alpha64;
             double c[2] = {0.0, 0.0};
-            for (int i = lo + lt; i < hi; i += GS) {
-                if constexpr (kIR) x[i] = fma(alpha64, (double)B.p[i], x[i]);
-                else x[i] = fmaf(alpha, B.p[i], x[i]);
-                const float ri = fmaf(-alpha, B.q[i], B.r[i]);
-                B.r[i] = ri;
-                c[0] += (double)ri * ri;
-                c[1] += (double)ri * ri * B.dinv[i];
+            // four rows per thread per trip, every load issued before the
+            // first store (one memory round trip per trip, not per row);
+            // rows are visited, and summed, in the same order as one at a time
+            constexpr int UV = 4;
+            for (int i0 = lo + lt; i0 < hi; i0 += UV * GS) {
+                float pv[UV], qv[UV], rv[UV], dv[UV];
+                XT xv[UV];
+#pragma unroll
+                for (int u = 0; u < UV; ++u) {
+                    const int i = i0 + u * GS;
+                    if (i < hi) {
+                        pv[u] = B.p[i];
+                        qv[u] = B.q[i];
+                        rv[u] = B.r[i];
+                        dv[u] = B.dinv[i];
+                        xv[u] = x[i];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < UV; ++u) {
+                    const int i = i0 + u * GS;
+                    if (i < hi) {
+                        if constexpr (kIR) x[i] = fma(alpha64, (double)pv[u], xv[u]);
+                        else x[i] = fmaf(alpha, pv[u], xv[u]);
+                        const float ri = fmaf(-alpha, qv[u], rv[u]);
+                        B.r[i] = ri;
+                        c[0] += (double)ri * ri;
+                        c[1] += (double)ri * ri * dv[u];
+                    }
+                }
             }
             G.template reduce<2>(c, sh);
             ++it;
@@ -345,17 +411,10 @@ __device__ __forceinline__ void batch_pcg_body(const BatchDev& B, const float* _
             double beta;
             if (mode == 2) {
                 double d[1] = {0.0};
-                for (int i = lo + lt; i < hi; i += 2 * GS) {
-                    const int j = i + GS;
-                    float w0, w1;
-                    grp_dot2(G, B.grp, B.gci, B.gv, B.r, i, j, j < hi, w0, w1);
-                    B.w[i] = w0;
-                    d[0] += (double)w0 * w0;
-                    if (j < hi) {
-                        B.w[j] = w1;
-                        d[0] += (double)w1 * w1;
-                    }
-                }
+                grp_spmv_rows(G, B.grp, B.gci, B.gv, B.r, lo, hi, [&](int i, float wi) {
+                    B.w[i] = wi;
+                    d[0] += (double)wi * wi;
+                });
                 G.template reduce<1>(d, sh);
                 if (stall_window > 0 && !(d[0] < 0.25 * best) && it - best_it >= stall_window) {
                     mode = 1;                     // stalled: Jacobi from here, restart p
@@ -371,21 +430,29 @@ __device__ __forceinline__ void batch_pcg_body(const BatchDev& B, const float* _
                 beta = d[0] / rz;
                 rz = d[0];
                 const float bf = (float)beta;
-                for (int i = lo + lt; i < hi; i += 2 * GS) {
-                    const int j = i + GS;
-                    float z0, z1;
-                    grp_dot2(G, B.gtrp, B.gtci, B.gtv, B.w, i, j, j < hi, z0, z1);
-                    B.p[i] = fmaf(bf, B.p[i], z0);
-                    if (j < hi) B.p[j] = fmaf(bf, B.p[j], z1);
-                }
+                grp_spmv_rows(G, B.gtrp, B.gtci, B.gtv, B.w, lo, hi,
+                              [&](int i, float zi) { B.p[i] = fmaf(bf, B.p[i], zi); });
             } else {
                 const double rzn = mode == 1 ? c[1] : c[0];
                 beta = rzn / rz;
                 rz = rzn;
                 const float bf = (float)beta;
-                for (int i = lo + lt; i < hi; i += GS) {
-                    const float z = mode == 1 ? B.r[i] * B.dinv[i] : B.r[i];
-                    B.p[i] = fmaf(bf, B.p[i], z);
+                constexpr int UP = 4;
+                for (int i0 = lo + lt; i0 < hi; i0 += UP * GS) {
+                    float pv[UP], zv[UP];
+#pragma unroll
+                    for (int u = 0; u < UP; ++u) {
+                        const int i = i0 + u * GS;
+                        if (i < hi) {
+                            pv[u] = B.p[i];
+                            zv[u] = mode == 1 ? B.r[i] * B.dinv[i] : B.r[i];
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < UP; ++u) {
+                        const int i = i0 + u * GS;
+                        if (i < hi) B.p[i] = fmaf(bf, pv[u], zv[u]);
+                    }
                 }
             }
             G.sync();
