@@ -751,14 +751,48 @@ out:
     }
 }
 
+// Row blocks for `grid` CTAs balanced by their shared-memory bytes
+// (4 * words per row + 8 per nonzero of A, and of M when given): boundary c
+// is the first row whose prefix reaches c / grid of the total.  Each
+// boundary is its own binary search over the row pointers (the prefix is
+// monotone), so the result does not depend on the search order.
+__global__ void persist_split_kernel(const int* __restrict__ a_rp, const int* __restrict__ m_rp, int n,
+                                     int grid, int words, int* __restrict__ start) {
+    auto bytes_to = [&](int i) {   // rows [0, i)
+        return 4.0 * words * i + 8.0 * ((double)a_rp[i] + (m_rp ? (double)m_rp[i] : 0.0));
+    };
+    const double total = bytes_to(n);
+    for (int c = threadIdx.x; c <= grid; c += blockDim.x) {
+        int a = 0, bnd = n;
+        if (c == 0) {
+            bnd = 0;
+        } else if (c < grid) {
+            const double target = total * c / grid;
+            while (a < bnd) {   // first row whose prefix reaches the target
+                const int mid = a + (bnd - a) / 2;
+                if (bytes_to(mid) < target) a = mid + 1;
+                else bnd = mid;
+            }
+        } else {
+            a = n;
+        }
+        start[c] = c == 0 ? 0 : a;
+    }
+}
+
 // Per CTA block: the smallest column, and one past the largest, that its
 // rows of A (and M) reference, widened to the block's own rows -- the window
 // of the multiplied vector the block's row sums read.
 __global__ void persist_window_kernel(const int* __restrict__ a_rp, const int* __restrict__ a_ci,
                                       const int* __restrict__ m_rp, const int* __restrict__ m_ci,
-                                      const int* __restrict__ row_start, int* __restrict__ win) {
+                                      const int* __restrict__ row_start, int* __restrict__ win,
+                                      int* __restrict__ cnt) {
     const int b = blockIdx.x;
     const int r0 = row_start[b], r1 = row_start[b + 1];
+    if (threadIdx.x == 0) {   // the block's nonzeros of A and M
+        cnt[2 * b] = a_rp[r1] - a_rp[r0];
+        cnt[2 * b + 1] = m_rp ? m_rp[r1] - m_rp[r0] : 0;
+    }
     int lo = r0, hi = r1;
     for (int k = a_rp[r0] + threadIdx.x; k < a_rp[r1]; k += blockDim.x) {
         const int c = a_ci[k];
@@ -794,13 +828,12 @@ __global__ void persist_window_kernel(const int* __restrict__ a_rp, const int* _
 
 }  // namespace
 
-// Row blocks of A and M for one CTA per SM, balanced by their shared-memory
-// bytes; false when a block would not fit (the graph form is used then).
-// Row blocks for one CTA per SM over A's rows (and M's when mrp is given),
-// balanced by their shared-memory bytes; pp.state = -1 when a block would
-// not fit or the kernel cannot be made resident (the graph form runs then).
-static cudaError_t plan_rows(PersistPlan& pp, const std::vector<int>& arp, const std::vector<int>* mrp,
-                             int n, const void* kernel, const CsrMat& A, const CsrMat* M, cudaStream_t s) {
+// Row blocks for one CTA per SM over A's rows (and M's when given), split
+// and measured on the GPU (one small read-back), balanced by their
+// shared-memory bytes; pp.state = -1 when a block would not fit or the
+// kernel cannot be made resident (the graph form runs then).
+static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const CsrMat& A, const CsrMat* M,
+                             cudaStream_t s) {
     pp.state = -1;
     int per_sm = 0;
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -811,64 +844,43 @@ static cudaError_t plan_rows(PersistPlan& pp, const std::vector<int>& arp, const
         cudaGetLastError();
         return cudaSuccess;   // not eligible
     }
-    const int words = mrp ? 2 : 1;   // row-pointer words per row
+    const int words = M ? 2 : 1;   // row-pointer words per row
     // at least 128 rows per CTA; one CTA per SM at most
     const int grid = std::min(num_sms(), std::max(1, n / 128));
-    auto bytes_to = [&](int i) {   // rows [0, i)
-        return 4.0 * words * i + 8.0 * ((double)arp[i] + (mrp ? (double)(*mrp)[i] : 0.0));
-    };
-    const double total = bytes_to(n);
-    std::vector<int> start(grid + 1);
-    start[0] = 0;
-    start[grid] = n;
-    int lo = 0;
-    for (int c = 1; c < grid; ++c) {
-        const double target = total * c / grid;
-        int a = lo, bnd = n;
-        while (a < bnd) {   // first row whose prefix reaches the target
-            const int mid = a + (bnd - a) / 2;
-            if (bytes_to(mid) < target) a = mid + 1;
-            else bnd = mid;
-        }
-        start[c] = a;
-        lo = a;
-    }
-    size_t worst = 0;
+    dev_free(pp.d_row_start);
+    pp.d_row_start = nullptr;
+    // grid + 1 boundaries, the barrier words, 2 window bounds per block, then
+    // 2 nonzero counts per block (read back here only)
+    const size_t words_all = (size_t)grid + 1 + kBarWords + 4 * (size_t)grid;
+    e = dev_alloc(&pp.d_row_start, words_all * 4, s);
+    if (e != cudaSuccess) return e;
+    int* d_win = pp.d_row_start + grid + 1 + kBarWords;
+    int* d_cnt = d_win + 2 * grid;
+    persist_split_kernel<<<1, 256, 0, s>>>(A.rp, M ? M->rp : nullptr, n, grid, words, pp.d_row_start);
+    persist_window_kernel<<<grid, 256, 0, s>>>(A.rp, A.ci, M ? M->rp : nullptr, M ? M->ci : nullptr,
+                                               pp.d_row_start, d_win, d_cnt);
+    e = cudaGetLastError();
+    std::vector<int> h(words_all);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), pp.d_row_start, words_all * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    const int* start = h.data();
+    const int* win = start + grid + 1 + kBarWords;
+    const int* cnt = win + 2 * grid;
+    size_t worst = 0, worst_win = 0;
     for (int c = 0; c < grid; ++c) {
         const int rows = start[c + 1] - start[c];
         if (rows < 0) return cudaSuccess;
-        size_t b = 4 * (size_t)words * ((size_t)rows + 1) + 8 * (size_t)(arp[start[c + 1]] - arp[start[c]]);
-        if (mrp) b += 8 * (size_t)((*mrp)[start[c + 1]] - (*mrp)[start[c]]);
+        size_t b = 4 * (size_t)words * ((size_t)rows + 1) + 8 * (size_t)cnt[2 * c];
+        if (M) b += 8 * (size_t)cnt[2 * c + 1];
         worst = std::max(worst, b);
-    }
-    if (worst > kPSmemBudget) return cudaSuccess;   // rows do not fit: not eligible
-    dev_free(pp.d_row_start);
-    pp.d_row_start = nullptr;
-    // grid + 1 boundaries, the barrier words, then 2 window bounds per block
-    e = dev_alloc(&pp.d_row_start, (size_t)(grid + 1 + kBarWords + 2 * grid) * 4, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(pp.d_row_start, start.data(), (size_t)(grid + 1) * 4, cudaMemcpyHostToDevice, s);
-    int* d_win = pp.d_row_start + grid + 1 + kBarWords;
-    std::vector<int> win(2 * (size_t)grid);
-    if (e == cudaSuccess) {
-        persist_window_kernel<<<grid, 256, 0, s>>>(A.rp, A.ci, M ? M->rp : nullptr, M ? M->ci : nullptr,
-                                                   pp.d_row_start, d_win);
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(win.data(), d_win, win.size() * 4, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return e;
-    // window form when every block's rows plus its vector window fit
-    size_t worst_win = 0;
-    for (int c = 0; c < grid; ++c) {
-        const int rows = start[c + 1] - start[c];
-        size_t b = 4 * (size_t)words * ((size_t)rows + 1) + 8 * (size_t)(arp[start[c + 1]] - arp[start[c]]);
-        if (mrp) b += 8 * (size_t)((*mrp)[start[c + 1]] - (*mrp)[start[c]]);
+        // window form: the vector window and the own rows' vectors beside the rows
         b += 4 * (size_t)(win[2 * c + 1] - win[2 * c]);
-        if (mrp) b += 12 * (size_t)rows;   // FSAI form: the own rows' x (FP64) and D^-1
+        if (M) b += 12 * (size_t)rows;   // FSAI form: the own rows' x (FP64) and D^-1
         else b += 8 + 20 * (size_t)rows;   // CG form: x (FP64 at most), r, q, D^-1
         worst_win = std::max(worst_win, b);
     }
+    if (worst > kPSmemBudget) return cudaSuccess;   // rows do not fit: not eligible
     pp.grid = grid;
     pp.win = worst_win <= kPSmemWinBudget ? 1 : 0;
     if (pp.win) {   // the larger footprint must still leave one CTA resident per SM
@@ -886,34 +898,20 @@ static cudaError_t plan_rows(PersistPlan& pp, const std::vector<int>& arp, const
     return cudaSuccess;
 }
 
-static cudaError_t host_row_ptr(const CsrMat& m, std::vector<int>& out, cudaStream_t s) {
-    out.resize((size_t)m.n_rows + 1);
-    cudaError_t e = cudaMemcpyAsync(out.data(), m.rp, out.size() * 4, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    return e;
-}
-
 // Plan of the FSAI form (rows of A and M).
 cudaError_t persist_plan_build(mps_csr* h, cudaStream_t s) {
     h->pp.state = -1;
     if (!h->use_m || !h->M.rp || h->A.n_rows != h->M.n_rows) return cudaSuccess;
-    std::vector<int> arp, mrp;
-    cudaError_t e = host_row_ptr(h->A, arp, s);
-    if (e == cudaSuccess) e = host_row_ptr(h->M, mrp, s);
-    if (e != cudaSuccess) return e;
-    return plan_rows(h->pp, arp, &mrp, (int)h->A.n_rows,
-                     reinterpret_cast<const void*>(fsai_pcg_persistent<false>), h->A, &h->M, s);
+    return plan_rows(h->pp, (int)h->A.n_rows, reinterpret_cast<const void*>(fsai_pcg_persistent<false>),
+                     h->A, &h->M, s);
 }
 
 // Plan of the CG form (rows of A only).
 cudaError_t persist_plan_build_a(mps_csr* h, cudaStream_t s) {
     h->pp_a.state = -1;
     if (h->A.n_rows != h->A.n_cols) return cudaSuccess;
-    std::vector<int> arp;
-    const cudaError_t e = host_row_ptr(h->A, arp, s);
-    if (e != cudaSuccess) return e;
-    return plan_rows(h->pp_a, arp, nullptr, (int)h->A.n_rows,
-                     reinterpret_cast<const void*>(cg_persistent<false, false>), h->A, nullptr, s);
+    return plan_rows(h->pp_a, (int)h->A.n_rows, reinterpret_cast<const void*>(cg_persistent<false, false>),
+                     h->A, nullptr, s);
 }
 
 // Plain CG / Jacobi-PCG as one cooperative launch: b is H.v(vB), x lands in
