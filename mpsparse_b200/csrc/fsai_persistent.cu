@@ -1,6 +1,7 @@
-// fsai_persistent.cu -- reliable-update FSAI-PCG (product form: z = M r with
-// M = G^T G) as one cooperative kernel, for matrices whose rows of A and M
-// fit the shared memory of one CTA per SM.
+// fsai_persistent.cu -- whole solves as one cooperative kernel, for matrices
+// whose rows fit the shared memory of one CTA per SM: reliable-update
+// FSAI-PCG (product form: z = M r with M = G^T G; fsai_pcg_persistent) and
+// plain CG / Jacobi-PCG, FP32 or with reliable updates (cg_persistent).
 //
 // The graph form of the same solve (driver.hpp, build_graph_nested) runs two
 // grid-wide kernels per iteration; on an L2-resident system (512^2: 1.3 M
@@ -9,9 +10,13 @@
 // per SM keeps its block of rows of A and of M in shared memory for the whole
 // solve and the two dependent steps of an iteration are separated by grid
 // barriers instead of kernel boundaries:
-//   step 1  p = z + beta p_old (formed on the fly), q = A p, p.q      -> alpha
-//   step 2  r' = r - alpha q (on the fly), z = M r', x += alpha p (FP64),
+//   step 1  p = z + beta p_old, q = A p, p.q                          -> alpha
+//   step 2  x += alpha p (FP64), r' = r - alpha q, z = M r',
 //           r'.r', r'.D^-1 r', r'.z                                  -> beta
+// In the window form each step first stages its multiplied vector (p, or r')
+// over the column window the CTA's rows reach, formed while it is loaded,
+// and the row sums read shared memory only; in the gather form (windows too
+// large) the row sums gather the vector entries and form them per nonzero.
 // plus, when due, the residual replacement r = (float)(b - A x) in FP64 and
 // z = M r.  The arithmetic of every row is the graph form's (same products,
 // same order of additions, same FP32 / FP64 rounding points); only the FP64
