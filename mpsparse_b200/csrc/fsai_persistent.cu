@@ -228,14 +228,26 @@ __device__ __forceinline__ void fill_window(float* win, int lo, int hi, F f) {
     }
 }
 
+// p rounded up to a multiple of a bytes (shared-memory layout).
+template <class T>
+__device__ __forceinline__ T* align_up(void* p, size_t a) {
+    return reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(p) + (a - 1)) & ~(uintptr_t)(a - 1));
+}
+
+// Column indices in shared memory: window form 16-bit, relative to the
+// window's first column (windows of at most 65,536 columns); gather form
+// the global 32-bit index.
+template <bool WIN>
+using ColIdx = std::conditional_t<WIN, unsigned short, int>;
+
 // Row li of a block of a CSR held in shared memory times a gathered vector:
 // the products rounded to FP32 first, then added in column order (the tile
 // kernels' arithmetic).
-template <class F>
-__device__ __forceinline__ float row_f32(const int* rp, const int* ci, const float* v, int li, F gather) {
+template <class IT, class F>
+__device__ __forceinline__ float row_f32(const int* rp, const IT* ci, const float* v, int li, F gather) {
     float s = 0.f;
     const int e = rp[li + 1];
-    for (int k = rp[li]; k < e; ++k) s = __fadd_rn(s, __fmul_rn(v[k], gather(ci[k])));
+    for (int k = rp[li]; k < e; ++k) s = __fadd_rn(s, __fmul_rn(v[k], gather((int)ci[k])));
     return s;
 }
 
@@ -243,8 +255,8 @@ __device__ __forceinline__ float row_f32(const int* rp, const int* ci, const flo
 // order exactly as row_f32 does: the gathers of both rows are issued four at
 // a time before their products are added, so the two rows' gather latencies
 // overlap instead of adding up.
-template <class F>
-__device__ __forceinline__ void row_pair_f32(const int* rp, const int* ci, const float* v, int li0,
+template <class IT, class F>
+__device__ __forceinline__ void row_pair_f32(const int* rp, const IT* ci, const float* v, int li0,
                                              int li1, bool has1, F gather, float& s0, float& s1) {
     const int b0 = rp[li0], e0 = rp[li0 + 1];
     const int b1 = has1 ? rp[li1] : 0, e1 = has1 ? rp[li1 + 1] : 0;
@@ -258,8 +270,8 @@ __device__ __forceinline__ void row_pair_f32(const int* rp, const int* ci, const
             const bool in0 = b0 + k + u < e0, in1 = b1 + k + u < e1;
             w0[u] = in0 ? v[b0 + k + u] : 0.f;
             w1[u] = in1 ? v[b1 + k + u] : 0.f;
-            g0[u] = in0 ? gather(ci[b0 + k + u]) : 0.f;
-            g1[u] = in1 ? gather(ci[b1 + k + u]) : 0.f;
+            g0[u] = in0 ? gather((int)ci[b0 + k + u]) : 0.f;
+            g1[u] = in1 ? gather((int)ci[b1 + k + u]) : 0.f;
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -278,32 +290,35 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
     const int R = r1 - r0;
     const int a0 = P.a_rp[r0], na = P.a_rp[r1] - a0;
     const int m0 = P.m_rp[r0], nm = P.m_rp[r1] - m0;
-    // shared layout: arp[R+1] | mrp[R+1] | aci[na] | mci[nm] | av[na] | mv[nm]
-    int* arp = reinterpret_cast<int*>(psmem);
-    int* mrp = arp + (R + 1);
-    int* aci = mrp + (R + 1);
-    int* mci = aci + na;
-    float* av = reinterpret_cast<float*>(mci + nm);
-    float* mv = av + na;
     // WIN: the multiplied vector over the CTA's column window, staged once
     // per step (coalesced loads) so the row sums read shared memory only;
-    // the own rows' x (FP64, written through to global) and D^-1 stay in
-    // shared memory too:  ... mv | xs[R] | ds[R] | win[hi - lo]
+    // columns stored relative to the window (16-bit); the own rows' x (FP64,
+    // written through to global) and D^-1 stay in shared memory too.
+    // shared layout: arp[R+1] | mrp[R+1] | aci[na] | mci[nm] | pad | av[na] |
+    //                mv[nm] | (WIN: pad | xs[R] | ds[R] | win[hi - lo])
+    using CI = ColIdx<WIN>;
     const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
-    double* xs = reinterpret_cast<double*>(mv + nm);
+    const int coff = wlo;   // global column = coff + stored index (0 in the gather form)
+    int* arp = reinterpret_cast<int*>(psmem);
+    int* mrp = arp + (R + 1);
+    CI* aci = reinterpret_cast<CI*>(mrp + (R + 1));
+    CI* mci = aci + na;
+    float* av = align_up<float>(mci + nm, 4);
+    float* mv = av + na;
+    double* xs = align_up<double>(mv + nm, 8);
     float* ds = reinterpret_cast<float*>(xs + (WIN ? R : 0));
     float* win = ds + (WIN ? R : 0);
-    auto wg = [&](int c) { return win[c - wlo]; };
+    auto wg = [&](int c) { return win[c]; };
     for (int i = tid; i <= R; i += kPNT) {
         arp[i] = P.a_rp[r0 + i] - a0;
         mrp[i] = P.m_rp[r0 + i] - m0;
     }
     for (int k = tid; k < na; k += kPNT) {
-        aci[k] = P.a_ci[a0 + k];
+        aci[k] = (CI)(P.a_ci[a0 + k] - coff);
         av[k] = P.a_v[a0 + k];
     }
     for (int k = tid; k < nm; k += kPNT) {
-        mci[k] = P.m_ci[m0 + k];
+        mci[k] = (CI)(P.m_ci[m0 + k] - coff);
         mv[k] = P.m_v[m0 + k];
     }
     if constexpr (WIN) {
@@ -351,7 +366,7 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
         double acc[1] = {0.0};
         const float* rc = P.r0;
         for (int li = tid; li < R; li += kPNT) {
-            const float s = row_f32(mrp, mci, mv, li, [&](int c) { return ldv(rc + c); });
+            const float s = row_f32(mrp, mci, mv, li, [&](int c) { return ldv(rc + coff + c); });
             const int i = r0 + li;
             P.z[i] = s;
             acc[0] += (double)ldv(rc + i) * (double)s;
@@ -470,7 +485,7 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                     double s = 0.0;
                     const int e = arp[li + 1];
                     for (int k = arp[li]; k < e; ++k)
-                        s = __dadd_rn(s, __dmul_rn((double)av[k], ldv(P.x + aci[k])));
+                        s = __dadd_rn(s, __dmul_rn((double)av[k], ldv(P.x + coff + aci[k])));
                     const int i = r0 + li;
                     const double rt = __ldg(P.b + i) - s;
                     const float rf = (float)rt;
@@ -506,7 +521,7 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                 const float* rc = (S.iter & 1) ? P.r1 : P.r0;
                 double acc[1] = {0.0};
                 for (int li = tid; li < R; li += kPNT) {
-                    const float s = row_f32(mrp, mci, mv, li, [&](int c) { return ldv(rc + c); });
+                    const float s = row_f32(mrp, mci, mv, li, [&](int c) { return ldv(rc + coff + c); });
                     const int i = r0 + li;
                     P.z[i] = s;
                     acc[0] += (double)ldv(rc + i) * (double)s;
@@ -546,25 +561,27 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
     const int r0 = P.row_start[blockIdx.x], r1 = P.row_start[blockIdx.x + 1];
     const int R = r1 - r0;
     const int a0 = P.a_rp[r0], na = P.a_rp[r1] - a0;
-    // shared layout: arp[R+1] | aci[na] | av[na]; window form adds the own
-    // rows' x (FP64 under IR, written through to global), r (written
-    // through), q and D^-1, then the vector window:
+    // shared layout: arp[R+1] | aci[na] | pad | av[na]; the window form
+    // stores columns relative to the window (16-bit) and adds the own rows'
+    // x (FP64 under IR, written through to global), r (written through), q
+    // and D^-1, then the vector window:
     //   ... av | pad to 8 | xs[R] | rs[R] | qs[R] | ds[R] | win[hi - lo]
     using XT = std::conditional_t<IR, double, float>;
-    int* arp = reinterpret_cast<int*>(psmem);
-    int* aci = arp + (R + 1);
-    float* av = reinterpret_cast<float*>(aci + na);
+    using CI = ColIdx<WIN>;
     const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
-    const size_t tail = ((size_t)(4 * (R + 1) + 8 * na) + 7) & ~(size_t)7;
-    XT* xs = reinterpret_cast<XT*>(psmem + tail);
+    const int coff = wlo;   // global column = coff + stored index (0 in the gather form)
+    int* arp = reinterpret_cast<int*>(psmem);
+    CI* aci = reinterpret_cast<CI*>(arp + (R + 1));
+    float* av = align_up<float>(aci + na, 4);
+    XT* xs = align_up<XT>(av + na, 8);
     float* rs = reinterpret_cast<float*>(xs + (WIN ? R : 0));
     float* qs = rs + (WIN ? R : 0);
     float* ds = qs + (WIN ? R : 0);
-    float* win = WIN ? ds + R : av + na;
-    auto wg = [&](int c) { return win[c - wlo]; };
+    float* win = ds + (WIN ? R : 0);
+    auto wg = [&](int c) { return win[c]; };
     for (int i = tid; i <= R; i += kPNT) arp[i] = P.a_rp[r0 + i] - a0;
     for (int k = tid; k < na; k += kPNT) {
-        aci[k] = P.a_ci[a0 + k];
+        aci[k] = (CI)(P.a_ci[a0 + k] - coff);
         av[k] = P.a_v[a0 + k];
     }
     if (tid == 0) {
@@ -625,7 +642,7 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
                 double sd = 0.0;
                 const int e = arp[li + 1];
                 for (int k = arp[li]; k < e; ++k)
-                    sd = __dadd_rn(sd, __dmul_rn((double)av[k], ldv(P.x + aci[k])));
+                    sd = __dadd_rn(sd, __dmul_rn((double)av[k], ldv(P.x + coff + aci[k])));
                 const int i = r0 + li;
                 const double rt = __ldg(P.b + i) - sd;
                 const float rf = (float)rt;
@@ -879,13 +896,16 @@ static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const C
         size_t b = 4 * (size_t)words * ((size_t)rows + 1) + 8 * (size_t)cnt[2 * c];
         if (M) b += 8 * (size_t)cnt[2 * c + 1];
         worst = std::max(worst, b);
-        // window form: the vector window and the own rows' vectors beside the rows
-        b += 4 * (size_t)(win[2 * c + 1] - win[2 * c]);
-        if (M) b += 12 * (size_t)rows;   // FSAI form: the own rows' x (FP64) and D^-1
-        else b += 8 + 20 * (size_t)rows;   // CG form: x (FP64 at most), r, q, D^-1
-        worst_win = std::max(worst_win, b);
+        // window form: 16-bit columns (6 bytes per nonzero), the vector
+        // window and the own rows' vectors beside the rows, 12 bytes of
+        // alignment padding
+        const size_t w = (size_t)(win[2 * c + 1] - win[2 * c]);
+        size_t bw = 4 * (size_t)words * ((size_t)rows + 1) + 6 * (size_t)cnt[2 * c] + 12 + 4 * w;
+        if (M) bw += 6 * (size_t)cnt[2 * c + 1] + 12 * (size_t)rows;   // FSAI: x (FP64), D^-1
+        else bw += 20 * (size_t)rows;                                  // CG: x (FP64 at most), r, q, D^-1
+        if (w > 65536) bw = ~(size_t)0;   // relative columns must fit 16 bits
+        worst_win = std::max(worst_win, bw);
     }
-    if (worst > kPSmemBudget) return cudaSuccess;   // rows do not fit: not eligible
     pp.grid = grid;
     pp.win = worst_win <= kPSmemWinBudget ? 1 : 0;
     if (pp.win) {   // the larger footprint must still leave one CTA resident per SM
@@ -898,6 +918,8 @@ static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const C
             pp.win = 0;
         }
     }
+    // the window form (16-bit columns) can fit where the gather form does not
+    if (!pp.win && worst > kPSmemBudget) return cudaSuccess;   // rows do not fit: not eligible
     pp.smem = (((pp.win ? worst_win : worst) + 15) / 16) * 16;
     pp.state = 1;
     return cudaSuccess;
