@@ -280,12 +280,9 @@ __device__ __forceinline__ void row_pair_f32(const int* rp, const IT* ci, const 
     }
 }
 
-// WF: 0 gather form, 1 window form (32-bit columns), 2 window form with
-// 16-bit window-relative columns (for blocks that fit only that way: the
-// narrow loads cost about 3 % per iteration on a 512^2 system).
-template <int WF>
+// WIN: window form (16-bit window-relative columns); else gather form.
+template <bool WIN>
 __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
-    constexpr bool WIN = WF > 0;
     extern __shared__ __align__(16) unsigned char psmem[];
     __shared__ PersistShared sh;
     const int tid = threadIdx.x;
@@ -295,14 +292,13 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
     const int m0 = P.m_rp[r0], nm = P.m_rp[r1] - m0;
     // WIN: the multiplied vector over the CTA's column window, staged once
     // per step (coalesced loads) so the row sums read shared memory only
-    // (WF 2: columns stored 16-bit, relative to the window); the own rows' x
-    // (FP64, written through to global) and D^-1 stay in shared memory too.
+    // (columns stored 16-bit, relative to the window); the own rows' x (FP64,
+    // written through to global) and D^-1 stay in shared memory too.
     // shared layout: arp[R+1] | mrp[R+1] | aci[na] | mci[nm] | pad | av[na] |
     //                mv[nm] | (WIN: pad | xs[R] | ds[R] | win[hi - lo])
-    using CI = ColIdx<WF == 2>;
+    using CI = ColIdx<WIN>;
     const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
-    const int coff = WF == 2 ? wlo : 0;    // global column = coff + stored index
-    const int wbase = WF == 1 ? wlo : 0;   // window slot = stored index - wbase
+    const int coff = wlo;   // global column = coff + stored index (wlo = 0 in the gather form)
     int* arp = reinterpret_cast<int*>(psmem);
     int* mrp = arp + (R + 1);
     CI* aci = reinterpret_cast<CI*>(mrp + (R + 1));
@@ -313,7 +309,7 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
     double* xs = reinterpret_cast<double*>(psmem + round_up(off_v + 4 * (size_t)(na + nm), 8));
     float* ds = reinterpret_cast<float*>(xs + (WIN ? R : 0));
     float* win = ds + (WIN ? R : 0);
-    auto wg = [&](int c) { return win[c - wbase]; };
+    auto wg = [&](int c) { return win[c]; };
     for (int i = tid; i <= R; i += kPNT) {
         arp[i] = P.a_rp[r0 + i] - a0;
         mrp[i] = P.m_rp[r0 + i] - m0;
@@ -558,25 +554,23 @@ out:
 // IR (reliable updates, cg_mixed without FSAI): x accumulated in FP64
 // (P.x), b in FP64 (P.b), the stop rule of cg_finalize_ir, and -- when due --
 // the residual replacement r = (float)(b - A x) in FP64 in the same kernel.
-template <bool IR, int WF>
+template <bool IR, bool WIN>
 __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
-    constexpr bool WIN = WF > 0;
     extern __shared__ __align__(16) unsigned char psmem[];
     __shared__ PersistShared sh;
     const int tid = threadIdx.x;
     const int r0 = P.row_start[blockIdx.x], r1 = P.row_start[blockIdx.x + 1];
     const int R = r1 - r0;
     const int a0 = P.a_rp[r0], na = P.a_rp[r1] - a0;
-    // shared layout: arp[R+1] | aci[na] | pad | av[na]; the window forms
-    // (WF 2: columns 16-bit, relative to the window) add the own rows' x
+    // shared layout: arp[R+1] | aci[na] | pad | av[na]; the window form
+    // (columns 16-bit, relative to the window) adds the own rows' x
     // (FP64 under IR, written through to global), r (written through), q
     // and D^-1, then the vector window:
     //   ... av | pad to 8 | xs[R] | rs[R] | qs[R] | ds[R] | win[hi - lo]
     using XT = std::conditional_t<IR, double, float>;
-    using CI = ColIdx<WF == 2>;
+    using CI = ColIdx<WIN>;
     const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
-    const int coff = WF == 2 ? wlo : 0;    // global column = coff + stored index
-    const int wbase = WF == 1 ? wlo : 0;   // window slot = stored index - wbase
+    const int coff = wlo;   // global column = coff + stored index (wlo = 0 in the gather form)
     int* arp = reinterpret_cast<int*>(psmem);
     CI* aci = reinterpret_cast<CI*>(arp + (R + 1));
     const size_t off_v = round_up(4 * (size_t)(R + 1) + sizeof(CI) * (size_t)na, 4);
@@ -586,7 +580,7 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
     float* qs = rs + (WIN ? R : 0);
     float* ds = qs + (WIN ? R : 0);
     float* win = ds + (WIN ? R : 0);
-    auto wg = [&](int c) { return win[c - wbase]; };
+    auto wg = [&](int c) { return win[c]; };
     for (int i = tid; i <= R; i += kPNT) arp[i] = P.a_rp[r0 + i] - a0;
     for (int k = tid; k < na; k += kPNT) {
         aci[k] = (CI)(P.a_ci[a0 + k] - coff);
@@ -897,26 +891,25 @@ static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const C
     const int* start = h.data();
     const int* win = start + grid + 1 + kBarWords;
     const int* cnt = win + 2 * grid;
-    size_t worst = 0, worst_win = 0, worst_win16 = 0;
+    size_t worst = 0, worst_win = 0;
     for (int c = 0; c < grid; ++c) {
         const int rows = start[c + 1] - start[c];
         if (rows < 0) return cudaSuccess;
         size_t b = 4 * (size_t)words * ((size_t)rows + 1) + 8 * (size_t)cnt[2 * c];
         if (M) b += 8 * (size_t)cnt[2 * c + 1];
         worst = std::max(worst, b);
-        // window forms: the vector window and the own rows' vectors beside
-        // the rows (12 bytes of alignment padding); 8 or, with 16-bit
-        // window-relative columns, 6 bytes per nonzero
+        // window form: 16-bit window-relative columns (6 bytes per
+        // nonzero), the vector window and the own rows' vectors beside the
+        // rows, 12 bytes of alignment padding
         const size_t w = (size_t)(win[2 * c + 1] - win[2 * c]);
-        size_t extra = 12 + 4 * w + (M ? 12 : 20) * (size_t)rows;   // FSAI: x, D^-1; CG: x, r, q, D^-1
         const size_t nz = (size_t)cnt[2 * c] + (M ? (size_t)cnt[2 * c + 1] : 0);
-        const size_t head = 4 * (size_t)words * ((size_t)rows + 1);
-        worst_win = std::max(worst_win, head + 8 * nz + extra);
-        worst_win16 = std::max(worst_win16, w > 65536 ? ~(size_t)0 : head + 6 * nz + extra);
+        const size_t bw = 4 * (size_t)words * ((size_t)rows + 1) + 6 * nz + 12 + 4 * w +
+                          (M ? 12 : 20) * (size_t)rows;   // FSAI: x, D^-1; CG: x, r, q, D^-1
+        worst_win = std::max(worst_win, w > 65536 ? ~(size_t)0 : bw);
     }
     pp.grid = grid;
-    pp.win = worst_win <= kPSmemWinBudget ? 1 : worst_win16 <= kPSmemWinBudget ? 2 : 0;
-    const size_t need = pp.win == 1 ? worst_win : pp.win == 2 ? worst_win16 : worst;
+    pp.win = worst_win <= kPSmemWinBudget ? 1 : 0;
+    const size_t need = pp.win ? worst_win : worst;
     if (pp.win) {   // the larger footprint must still leave one CTA resident per SM
         const int sz = (int)(((need + 15) / 16) * 16);
         int per = 0;
@@ -938,7 +931,7 @@ static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const C
 cudaError_t persist_plan_build(mps_csr* h, cudaStream_t s) {
     h->pp.state = -1;
     if (!h->use_m || !h->M.rp || h->A.n_rows != h->M.n_rows) return cudaSuccess;
-    return plan_rows(h->pp, (int)h->A.n_rows, reinterpret_cast<const void*>(fsai_pcg_persistent<0>),
+    return plan_rows(h->pp, (int)h->A.n_rows, reinterpret_cast<const void*>(fsai_pcg_persistent<false>),
                      h->A, &h->M, s);
 }
 
@@ -946,7 +939,7 @@ cudaError_t persist_plan_build(mps_csr* h, cudaStream_t s) {
 cudaError_t persist_plan_build_a(mps_csr* h, cudaStream_t s) {
     h->pp_a.state = -1;
     if (h->A.n_rows != h->A.n_cols) return cudaSuccess;
-    return plan_rows(h->pp_a, (int)h->A.n_rows, reinterpret_cast<const void*>(cg_persistent<false, 0>),
+    return plan_rows(h->pp_a, (int)h->A.n_rows, reinterpret_cast<const void*>(cg_persistent<false, false>),
                      h->A, nullptr, s);
 }
 
@@ -983,14 +976,11 @@ cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s, const double* b64, doub
     P.b = b64;
     P.x = x64;
     P.win = h->pp_a.d_row_start + h->pp_a.grid + 1 + kBarWords;
-    const int w = h->pp_a.win;
-    const void* k =
-        b64 ? (w == 2   ? reinterpret_cast<const void*>(cg_persistent<true, 2>)
-               : w == 1 ? reinterpret_cast<const void*>(cg_persistent<true, 1>)
-                        : reinterpret_cast<const void*>(cg_persistent<true, 0>))
-            : (w == 2   ? reinterpret_cast<const void*>(cg_persistent<false, 2>)
-               : w == 1 ? reinterpret_cast<const void*>(cg_persistent<false, 1>)
-                        : reinterpret_cast<const void*>(cg_persistent<false, 0>));
+    const bool w = h->pp_a.win != 0;
+    const void* k = b64 ? (w ? reinterpret_cast<const void*>(cg_persistent<true, true>)
+                             : reinterpret_cast<const void*>(cg_persistent<true, false>))
+                        : (w ? reinterpret_cast<const void*>(cg_persistent<false, true>)
+                             : reinterpret_cast<const void*>(cg_persistent<false, false>));
     cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->pp_a.smem);
@@ -1046,9 +1036,8 @@ cudaError_t persist_solve(mps_csr* h, const double* b64, double* x64, cudaStream
     P.n = (int)h->A.n_rows;
     static_assert(4 * 3 * 1024 <= 4 * kMaxPartials, "partial slots");
     P.win = h->pp.d_row_start + h->pp.grid + 1 + kBarWords;
-    const void* k = h->pp.win == 2   ? reinterpret_cast<const void*>(fsai_pcg_persistent<2>)
-                    : h->pp.win == 1 ? reinterpret_cast<const void*>(fsai_pcg_persistent<1>)
-                                     : reinterpret_cast<const void*>(fsai_pcg_persistent<0>);
+    const void* k = h->pp.win ? reinterpret_cast<const void*>(fsai_pcg_persistent<true>)
+                              : reinterpret_cast<const void*>(fsai_pcg_persistent<false>);
     cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->pp.smem);
