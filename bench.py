@@ -345,8 +345,8 @@ def run_ours(args, rank, world, dev):
         total_ms = float(t.item())
     iters = [i["iters"] for i in infos]
     if args.solver == "learned":
-        # per solve: attach (network forward, value map, G^T gather, and
-        # G^T G values in product form) + ||b||^2 + init + per iteration 2
+        # per solve: attach (network forward, value map, G^T gather, G^T G
+        # values in product form, the error-word fold) + ||b||^2 + init + per iteration 2
         # kernels (product form: direction + A p, update + M r) or 3 (split:
         # A p, update + G r, G^T w) + 2 per residual replacement + the FP64
         # true residual at the end; the product form's graph runs 16
@@ -354,13 +354,14 @@ def run_ours(args, rank, world, dev):
         # stop) about 7.5 iterations' kernels return at once: 15 launches
         def per_solve(i):
             if i.get("persistent"):
-                # attach (forward, value map, G^T gather, G^T G values),
-                # ||b||^2, the persistent solve, the FP64 true residual
-                return 4 + 1 + 1 + 1
+                # attach (forward, value map, G^T gather, G^T G values, the
+                # network's error word folded into the handle's), ||b||^2,
+                # the persistent solve, the FP64 true residual
+                return 5 + 1 + 1 + 1
             if i.get("form") == "product":
                 rounds = max(i["outer"], 1)
-                return 4 + 1 + 2 + 2 * i["iters"] + 2 * rounds + 15 * rounds + 1
-            return 3 + 1 + 3 + 3 * i["iters"] + 2 * i["outer"] + 1
+                return 5 + 1 + 2 + 2 * i["iters"] + 2 * rounds + 15 * rounds + 1
+            return 4 + 1 + 3 + 3 * i["iters"] + 2 * i["outer"] + 1
         launches = sum(per_solve(i) for i in infos)
     else:
         launches = sum(2 + 3 * i["iters"] for i in infos)   # init + 3 kernels/iteration + copy
