@@ -476,12 +476,12 @@ static mps_status solve_errors(mps_csr* h, const unsigned* e2, mps_status st, cu
     return MPS_OK;
 }
 
-// Plain CG / Jacobi-PCG as one persistent cooperative kernel when A's rows
-// fit one CTA per SM (fsai_persistent.cu); *ran = false: not eligible, the
-// graph form runs instead.  Same parameters, result places and report as
+// Plain CG / Jacobi-PCG, or BiCGSTAB, as one persistent cooperative kernel
+// when A's rows fit one CTA per SM (fsai_persistent.cu; BiCGSTAB in the
+// window form only); *ran = false: not eligible, the graph form runs instead.  Same parameters, result places and report as
 // run_solve.
-static mps_status csr_cg_persistent(mps_csr* h, const float* b, float* x, const mps_solve_opts& o,
-                                    mps_solve_info* info, cudaStream_t s, bool* ran) {
+static mps_status csr_persistent(SolverKind kind, mps_csr* h, const float* b, float* x,
+                                 const mps_solve_opts& o, mps_solve_info* info, cudaStream_t s, bool* ran) {
     *ran = false;
     SolverHost& H = h->H;
     const size_t n = h->A.n_rows;
@@ -491,20 +491,20 @@ static mps_status csr_cg_persistent(mps_csr* h, const float* b, float* x, const 
     P.omega = o.omega != 0 ? o.omega : 0.01;
     P.max_iter = o.max_iter > 0 ? o.max_iter : 2000;
     P.compat = 0;
-    P.precond = o.precond;
+    P.precond = kind == kCG ? o.precond : 0;
     P.stall_window = o.stall_window > 0 ? o.stall_window : 400;
     MPS_CUDA(cudaMemcpyAsync(H.ws.d_params, H.h_params, sizeof(SolveParams), cudaMemcpyHostToDevice, s));
     MPS_CUDA(cudaMemcpyAsync(H.v(vB), b, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
-    const cudaError_t pe = persist_cg_solve(h, s);
+    const cudaError_t pe = kind == kCG ? persist_cg_solve(h, s) : persist_bicg_solve(h, s);
     if (pe == cudaErrorNotSupported) return MPS_OK;
-    if (pe != cudaSuccess) return cuda_fail(pe, "persistent CG");
+    if (pe != cudaSuccess) return cuda_fail(pe, kind == kCG ? "persistent CG" : "persistent BiCGSTAB");
     *ran = true;
     MPS_CUDA(cudaMemcpyAsync(x, H.v(vX), n * sizeof(float), cudaMemcpyDeviceToDevice, s));
     const CsrOp op{&h->A, nullptr};
     MPS_CUDA(op.true_resid(x, H.v(vB), &H.ws.sc->true_rr, H.ws.counters + 11, H.ws.partials, s));
     MPS_CUDA(cudaMemcpyAsync(H.ws.h_sc, H.ws.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
     MPS_CUDA(cudaStreamSynchronize(s));
-    const mps_status st = solve_report(kCG, H, info, nullptr, true);
+    const mps_status st = solve_report(kind, H, info, nullptr, true);
     if (info) info->persistent = 1;
     return st;
 }
@@ -524,9 +524,10 @@ static mps_status csr_solve(SolverKind kind, mps_csr* h, const float* b, float* 
     mps_solve_opts_default(&oo);
     if (o) oo = *o;
     bool ran = false;
-    if (kind == kCG && h->persistent && !oo.reference_compat && !oo.host_loop &&
-        (oo.precond == MPS_PRECOND_NONE || oo.precond == MPS_PRECOND_JACOBI))
-        st = csr_cg_persistent(h, b, x, oo, info, s, &ran);
+    if (h->persistent && !oo.reference_compat && !oo.host_loop &&
+        ((kind == kCG && (oo.precond == MPS_PRECOND_NONE || oo.precond == MPS_PRECOND_JACOBI)) ||
+         kind == kBiCG))
+        st = csr_persistent(kind, h, b, x, oo, info, s, &ran);
     if (st != MPS_OK) return st;
     if (!ran) st = run_solve(kind, op, pc, h->H, b, x, o, info, s);
     unsigned err[2] = {0, 0};

@@ -1,7 +1,8 @@
 // fsai_persistent.cu -- whole solves as one cooperative kernel, for matrices
 // whose rows fit the shared memory of one CTA per SM: reliable-update
-// FSAI-PCG (product form: z = M r with M = G^T G; fsai_pcg_persistent) and
-// plain CG / Jacobi-PCG, FP32 or with reliable updates (cg_persistent).
+// FSAI-PCG (product form: z = M r with M = G^T G; fsai_pcg_persistent),
+// plain CG / Jacobi-PCG, FP32 or with reliable updates (cg_persistent), and
+// BiCGSTAB (bicg_persistent).
 //
 // The graph form of the same solve (driver.hpp, build_graph_nested) runs two
 // grid-wide kernels per iteration; on an L2-resident system (512^2: 1.3 M
@@ -13,12 +14,12 @@
 //   step 1  p = z + beta p_old, q = A p, p.q                          -> alpha
 //   step 2  x += alpha p (FP64), r' = r - alpha q, z = M r',
 //           r'.r', r'.D^-1 r', r'.z                                  -> beta
-// In the window form each step first stages its multiplied vector (p, or r')
-// over the column window the CTA's rows reach, formed while it is loaded,
-// and the row sums read shared memory only; in the gather form (windows too
-// large) the row sums gather the vector entries and form them per nonzero.
 // plus, when due, the residual replacement r = (float)(b - A x) in FP64 and
-// z = M r.  The arithmetic of every row is the graph form's (same products,
+// z = M r.  In the window form each step first stages its multiplied vector
+// (p, or r') over the column window the CTA's rows reach, formed while it is
+// loaded, and the row sums read shared memory only; in the gather form
+// (windows too large) the row sums gather the vector entries and form them
+// per nonzero.  The arithmetic of every row is the graph form's (same products,
 // same order of additions, same FP32 / FP64 rounding points); only the FP64
 // sums of the per-CTA partials group differently.  Every CTA sums all
 // partials itself in one fixed order, so all CTAs take the same decisions
@@ -775,6 +776,183 @@ out:
     }
 }
 
+// BiCGSTAB (the drop-in bicgstab, outside reference_compat) as one
+// cooperative kernel over A's rows held in shared memory.  Per iteration,
+// each step separated from the next by a grid-wide sum:
+//   A  p = r + beta (p_old - omega v_old) (first iteration: p = r), formed
+//      while staging it; v = A p; sigma = r0.v                -> alpha
+//   B  s = r - alpha v, formed while staging it; t = A s;
+//      t.s, t.t                                               -> omega
+//   C  x += alpha p + omega s; r = s - omega t; r0.r, r.r     -> beta, stop
+// with the graph form's per-element arithmetic (bicg_update_p, EpiBicgV,
+// bicg_update_s, EpiBicgT, bicg_update_xr) and its stop rule
+// (bicg_stop_beta).  p and v are double-buffered by iteration parity: a CTA
+// writes its rows of the new ones while slower CTAs still gather the old.
+// s and t are never written to global memory: every CTA forms s over its
+// own window, and keeps its rows of t in shared memory.
+// Window form only (the plan's window-form budget covers the own rows' x
+// and t kept here).  Buffers: P.r0 = r, P.r1 = r0 (the shadow residual),
+// P.p0 / P.p1 = p, P.q / P.z = v, P.b32 = b, P.x32 = x.
+__global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
+    extern __shared__ __align__(16) unsigned char psmem[];
+    __shared__ PersistShared sh;
+    const int tid = threadIdx.x;
+    const int r0 = P.row_start[blockIdx.x], r1 = P.row_start[blockIdx.x + 1];
+    const int R = r1 - r0;
+    const int a0 = P.a_rp[r0], na = P.a_rp[r1] - a0;
+    // shared layout: arp[R+1] | aci[na] | pad | av[na] | pad | xs[R] | ts[R] |
+    //                win[hi - lo]; columns 16-bit, window-relative
+    using CI = ColIdx<true>;
+    const int wlo = P.win[2 * blockIdx.x], whi = P.win[2 * blockIdx.x + 1];
+    const int coff = wlo;   // global column = coff + stored index
+    int* arp = reinterpret_cast<int*>(psmem);
+    CI* aci = reinterpret_cast<CI*>(arp + (R + 1));
+    const size_t off_v = round_up(4 * (size_t)(R + 1) + sizeof(CI) * (size_t)na, 4);
+    float* av = reinterpret_cast<float*>(psmem + off_v);
+    float* xs = reinterpret_cast<float*>(psmem + round_up(off_v + 4 * (size_t)na, 8));
+    float* ts = xs + R;
+    float* win = ts + R;
+    auto wg = [&](int c) { return win[c]; };
+    for (int i = tid; i <= R; i += kPNT) arp[i] = P.a_rp[r0 + i] - a0;
+    for (int k = tid; k < na; k += kPNT) {
+        aci[k] = (CI)(P.a_ci[a0 + k] - coff);
+        av[k] = P.a_v[a0 + k];
+    }
+    if (tid == 0) {
+        sh.gen = 0;
+        sh.ok = 1;
+        sh.S = DevScalars{};
+    }
+    __syncthreads();
+    DevScalars& S = sh.S;
+    const Ctx cx{&sh.S, nullptr, nullptr, {}, 0, {}};
+    float* r = P.r0;
+    float* rh = P.r1;
+    {
+        // x = 0, r = r0 = b; b.b (bicg_init)
+        double acc[1] = {0.0};
+        for (int li = tid; li < R; li += kPNT) {
+            const int i = r0 + li;
+            const float bf = P.b32[i];
+            xs[li] = 0.f;
+            P.x32[i] = 0.f;
+            r[i] = bf;
+            rh[i] = bf;
+            acc[0] += (double)bf * bf;
+        }
+        double tot[1];
+        if (!reduce_all<1>(P, sh, 3, acc, tot, [&](const double* t) { bicg_init_scalars(cx, P.prm, P.n, t[0]); }))
+            goto out;
+    }
+    while (!S.done) {
+        const bool odd = S.iter & 1;
+        float* pn = odd ? P.p1 : P.p0;
+        const float* po = odd ? P.p0 : P.p1;
+        float* vn = odd ? P.z : P.q;
+        const float* vo = odd ? P.q : P.z;
+        // ---- A: p (staged), v = A p, sigma = r0.v -----------------------
+        {
+            const bool first = S.iter == 0;
+            const float beta = (float)S.beta, omega = (float)S.omega;
+            auto dirp = [&](int c) {
+                return first ? ldv(r + c) : fmaf(beta, fmaf(-omega, ldv(vo + c), ldv(po + c)), ldv(r + c));
+            };
+            fill_window(win, wlo, whi, dirp);
+            __syncthreads();
+            double acc[1] = {0.0};
+            auto own = [&](int li, float s) {
+                const int i = r0 + li;
+                pn[i] = win[i - wlo];
+                vn[i] = s;
+                acc[0] += (double)rh[i] * (double)s;
+            };
+            for (int li = tid; li < R; li += 2 * kPNT) {
+                const int lj = li + kPNT;
+                const bool has1 = lj < R;
+                float s0, s1;
+                row_pair_f32(arp, aci, av, li, lj, has1, wg, s0, s1);
+                own(li, s0);
+                if (has1) own(lj, s1);
+            }
+            double tot[1];
+            if (!reduce_all<1>(P, sh, 0, acc, tot, [&](const double* t) {
+                    const double sigma = t[0];
+                    S.sigma = sigma;
+                    if (sigma == 0.0 || !isfinite(sigma)) {   // EpiBicgV outside reference_compat
+                        S.breakdown = 1;
+                        S.done = 1;
+                        S.alpha = 0.0;
+                    } else {
+                        S.alpha = S.rho / sigma;
+                    }
+                }))
+                goto out;
+            if (S.done) break;
+        }
+        // ---- B: s = r - alpha v (staged), t = A s, t.s, t.t ---------------
+        const float af = (float)S.alpha;
+        auto dirs = [&](int c) { return fmaf(-af, ldv(vn + c), ldv(r + c)); };
+        {
+            fill_window(win, wlo, whi, dirs);
+            __syncthreads();
+            double acc[2] = {0.0, 0.0};
+            auto own = [&](int li, float t) {
+                const int i = r0 + li;
+                const float sv = win[i - wlo];
+                ts[li] = t;
+                acc[0] += (double)t * (double)sv;
+                acc[1] += (double)t * (double)t;
+            };
+            for (int li = tid; li < R; li += 2 * kPNT) {
+                const int lj = li + kPNT;
+                const bool has1 = lj < R;
+                float s0, s1;
+                row_pair_f32(arp, aci, av, li, lj, has1, wg, s0, s1);
+                own(li, s0);
+                if (has1) own(lj, s1);
+            }
+            double tot[2];
+            if (!reduce_all<2>(P, sh, 1, acc, tot, [&](const double* t) {
+                    S.phi1 = t[0];
+                    S.phi2 = t[1];
+                    S.omega = fabs(t[1]) < 1e-20 ? 0.0 : t[0] / t[1];   // EpiBicgT
+                }))
+                goto out;
+        }
+        // ---- C: x += alpha p + omega s, r = s - omega t, r0.r, r.r ---------
+        {
+            const float w = (float)S.omega;
+            double acc[2] = {0.0, 0.0};
+            for (int li = tid; li < R; li += kPNT) {
+                const int i = r0 + li;
+                const float sv = win[i - wlo];
+                float xv = fmaf(af, ldv(pn + i), xs[li]);
+                xv = fmaf(w, sv, xv);
+                xs[li] = xv;
+                P.x32[i] = xv;
+                const float rv = fmaf(-w, ts[li], sv);
+                r[i] = rv;
+                acc[0] += (double)rh[i] * (double)rv;
+                acc[1] += (double)rv * (double)rv;
+            }
+            double tot[2];
+            if (!reduce_all<2>(P, sh, 2, acc, tot, [&](const double* t) {
+                    S.iter = S.iter + 1;
+                    S.rho_old = S.rho;
+                    S.rho = t[0];
+                    S.rnorm2 = t[1];
+                    bicg_stop_beta(&S);
+                }))
+                goto out;
+        }
+    }
+out:
+    if (tid == 0 && blockIdx.x == 0) {
+        if (!sh.ok) S.err |= kErrTimeout;
+        *P.sc_out = S;
+    }
+}
+
 // Row blocks for `grid` CTAs balanced by their shared-memory bytes
 // (4 * words per row + 8 per nonzero of A, and of M when given): boundary c
 // is the first row whose prefix reaches c / grid of the total.  Each
@@ -981,6 +1159,45 @@ cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s, const double* b64, doub
                              : reinterpret_cast<const void*>(cg_persistent<true, false>))
                         : (w ? reinterpret_cast<const void*>(cg_persistent<false, true>)
                              : reinterpret_cast<const void*>(cg_persistent<false, false>));
+    cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->pp_a.smem);
+    if (e != cudaSuccess) return e;
+    void* args[] = {&P};
+    return cudaLaunchCooperativeKernel(k, dim3(h->pp_a.grid), dim3(kPNT), args, h->pp_a.smem, s);
+}
+
+// BiCGSTAB as one cooperative launch (window form only): b is H.v(vB), x
+// lands in H.v(vX) and the final scalars in H.ws.sc; the parameters must be
+// in H.ws.d_params.  cudaErrorNotSupported: not eligible (the graph form runs).
+cudaError_t persist_bicg_solve(mps_csr* h, cudaStream_t s) {
+    if (h->pp_a.state == 0) {
+        const cudaError_t e = persist_plan_build_a(h, s);
+        if (e != cudaSuccess) return e;
+    }
+    if (h->pp_a.state != 1 || !h->pp_a.win) return cudaErrorNotSupported;
+    SolverHost& H = h->H;
+    PersistDev P{};
+    P.a_rp = h->A.rp;
+    P.a_ci = h->A.ci;
+    P.a_v = h->A.v;
+    P.row_start = h->pp_a.d_row_start;
+    P.win = h->pp_a.d_row_start + h->pp_a.grid + 1 + kBarWords;
+    P.r0 = H.v(vR);
+    P.r1 = H.v(vR0);
+    P.p0 = H.v(vP);
+    P.p1 = H.v(vS);
+    P.q = H.v(vQ);
+    P.z = H.v(vT);
+    P.part = H.ws.partials;
+    P.bar = reinterpret_cast<unsigned*>(h->pp_a.d_row_start + h->pp_a.grid + 1);
+    P.err = h->d_err;
+    P.sc_out = H.ws.sc;
+    P.prm = H.ws.d_params;
+    P.n = (int)h->A.n_rows;
+    P.b32 = H.v(vB);
+    P.x32 = H.v(vX);
+    const void* k = reinterpret_cast<const void*>(bicg_persistent);
     cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->pp_a.smem);

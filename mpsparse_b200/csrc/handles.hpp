@@ -86,4 +86,5 @@ void persist_plan_free_all(mps_csr* h);
 cudaError_t persist_solve(mps_csr* h, const double* b64, double* x64, cudaStream_t s);
 cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s, const double* b64 = nullptr,
                              double* x64 = nullptr);
+cudaError_t persist_bicg_solve(mps_csr* h, cudaStream_t s);
 }  // namespace mps

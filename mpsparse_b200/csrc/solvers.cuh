@@ -755,6 +755,9 @@ struct EpiFsaiM {
 
 // ============================ BiCGSTAB =====================================
 
+static __device__ void bicg_init_scalars(const Ctx& c, const SolveParams* __restrict__ prm, int n,
+                                         double bb);
+
 static __global__ void __launch_bounds__(kNT)
 bicg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restrict__ r,
           float4* __restrict__ r0, float4* __restrict__ p, float4* __restrict__ v, int n4, int n,
@@ -773,8 +776,13 @@ bicg_init(const float4* __restrict__ b, float4* __restrict__ x, float4* __restri
     double tot[1];
     if (!reduce_partials<1>(c, 4, acc, tot)) return;
     if (threadIdx.x != 0) return;
+    bicg_init_scalars(c, prm, n, tot[0]);
+}
+
+// Scalars of a BiCGSTAB start from bb = ||b||^2 (one thread).
+static __device__ void bicg_init_scalars(const Ctx& c, const SolveParams* __restrict__ prm, int n,
+                                         double bb) {
     DevScalars* s = c.sc;
-    const double bb = tot[0];
     s->n = n;
     s->compat = prm->compat;
     s->max_iter = prm->compat ? (n < 5000 ? n : 5000) : prm->max_iter;
@@ -895,6 +903,24 @@ struct EpiBicgT {
     }
 };
 
+// Stop rule and next beta of a BiCGSTAB iteration (outside reference_compat),
+// once iter, rho_old, rho and rnorm2 hold the new values.
+static __device__ void bicg_stop_beta(DevScalars* s) {
+    if (!isfinite(s->rnorm2)) {
+        s->breakdown = 1;
+        s->done = 1;
+    } else if (s->rnorm2 <= s->tol2) {
+        s->converged = 1;
+        s->done = 1;
+    } else if (s->omega == 0.0 || s->rho == 0.0) {
+        s->breakdown = 1;
+        s->done = 1;
+    } else if (s->iter >= s->max_iter) {
+        s->done = 1;
+    }
+    s->beta = (s->rho / s->rho_old) * (s->alpha / s->omega);
+}
+
 // x += alpha p + omega s ; r = s - omega t ; rho = r0.r ; ||r||^2
 // (f_upomega_upxr_laa, bicgstab.metal:245-326).  Last kernel of an iteration.
 static __global__ void __launch_bounds__(kNT)
@@ -955,19 +981,7 @@ bicg_update_xr(float4* __restrict__ x, float4* __restrict__ r, const float4* __r
         if (check) s->staged = tot[1];
         if (s->iter >= s->max_iter) s->done = 1;
     } else {
-        if (!isfinite(tot[1])) {
-            s->breakdown = 1;
-            s->done = 1;
-        } else if (tot[1] <= s->tol2) {
-            s->converged = 1;
-            s->done = 1;
-        } else if (s->omega == 0.0 || s->rho == 0.0) {
-            s->breakdown = 1;
-            s->done = 1;
-        } else if (s->iter >= s->max_iter) {
-            s->done = 1;
-        }
-        s->beta = (s->rho / s->rho_old) * (s->alpha / s->omega);
+        bicg_stop_beta(s);
     }
     set_cond(c, !s->done);
 }

@@ -262,3 +262,70 @@ def test_persistent_560_window_form(mps, oracle):
     assert ip["persistent"] and ip["converged"]
     Ao = oracle.Csr(*c.to_csr(), c.n)
     assert oracle.true_residual(Ao, b.cpu().numpy(), xp.cpu().numpy()) <= 1e-9 * 1.01
+
+
+def _convection_diffusion(nx):
+    """Nonsymmetric 5-point system: the 2D Laplacian with each east coupling
+    halved (diagonally dominant, nonsingular)."""
+    c = W.laplacian_2d(nx)
+    vals = c.vals.copy()
+    vals[c.cols == c.rows + 1] *= 0.5
+    return W.Coo(c.rows, c.cols, vals.astype(np.float32), c.n)
+
+
+@pytest.mark.parametrize("nx", [32, 128])
+def test_persistent_bicgstab_matches_graph_form_and_oracle(mps, oracle, nx):
+    """BiCGSTAB (the drop-in bicgstab) as one persistent kernel: the first
+    iterates agree with the graph form's (1e-5 relative) and with the FP64
+    oracle's (1e-5 relative up to 5 iterations, and up to 20 on the 32^2
+    system; on 128^2 both FP32 forms drift from the FP64 recurrence by
+    6e-5 after 20 iterations); converged solves need the same iterations
+    within 2 and reach the FP64 true residual bar."""
+    from tests.helpers import assert_solved_fp32
+    c = _convection_diffusion(nx)
+    A = _cg_system(mps, c)
+    Ao = oracle.Csr(*c.to_csr(), c.n)
+    b = W.rhs(c.n, 9)
+    bt = torch.from_numpy(b).cuda()
+    for k in (1, 2, 5, 20):
+        xs = []
+        for persistent in (True, False):
+            A.set_persistent(persistent)
+            x = torch.zeros(c.n, device="cuda")
+            info = A.bicgstab(bt, x, tol=1e-300, max_iter=k)
+            assert info["iters"] == k and info["persistent"] == persistent, (k, info)
+            xs.append(x.cpu().numpy().astype(np.float64))
+        assert np.linalg.norm(xs[0] - xs[1]) / np.linalg.norm(xs[1]) <= 1e-5, k
+        if k <= 5 or nx == 32:
+            xo, _ = oracle.bicgstab(Ao, b, tol=0.0, max_iter=k)
+            for xk in xs:
+                assert np.linalg.norm(xk - xo) / np.linalg.norm(xo) <= 1e-5, k
+    infos = []
+    for persistent in (True, False):
+        A.set_persistent(persistent)
+        x = torch.zeros(c.n, device="cuda")
+        info = A.bicgstab(bt, x, tol=1e-6, max_iter=20000)
+        assert info["stop_rule_met"] and info["persistent"] == persistent
+        assert_solved_fp32(oracle, Ao, b, x.cpu().numpy(), 1e-6, info)
+        infos.append(info)
+    assert abs(infos[0]["iters"] - infos[1]["iters"]) <= 2, infos
+
+
+def test_persistent_bicgstab_edge_cases(mps):
+    """b = 0 returns x = 0 at once; a non-finite b is rejected; the handle
+    stays usable; reference_compat keeps the graph form."""
+    c = _convection_diffusion(64)
+    A = _cg_system(mps, c)
+    A.set_persistent(True)
+    x = torch.ones(c.n, device="cuda")
+    info = A.bicgstab(torch.zeros(c.n, device="cuda"), x)
+    assert info["persistent"] and info["converged"] and info["iters"] == 0
+    assert float(x.abs().max()) == 0.0
+    bad = torch.ones(c.n, device="cuda")
+    bad[5] = float("nan")
+    with pytest.raises(RuntimeError, match="non-finite"):
+        A.bicgstab(bad, x)
+    info = A.bicgstab(torch.ones(c.n, device="cuda"), x, max_iter=4, tol=1e-300)
+    assert info["iters"] == 4 and info["persistent"]
+    info = A.bicgstab(torch.ones(c.n, device="cuda"), x, reference_compat=True)
+    assert not info["persistent"]
