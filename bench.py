@@ -924,11 +924,60 @@ def c3_leg(args, dev, ctx):
                                "solves": errs}}
 
 
+def reference_sizes_leg(dev):
+    """The reference's own CSR solver benchmarks, re-run here on B200: CG on
+    2D 5-point Laplacians with n = 1,024 ... 20,449 (iterative/cgd/
+    comp_bench.py) and BiCGSTAB with n = 1,024 ... 16,384
+    (iterative/BiCGSTAB/benchmark.py), each from x = 0 to a relative
+    residual of 1e-6, device time per solve (median of 5 after a warm-up),
+    the persistent form (the default) beside the graph form.  The
+    reference's published times are Metal timings on an Apple GPU, so no
+    ratio is formed."""
+    import torch
+    import mpsparse_b200 as mps
+    W = _workloads()
+    stream = torch.cuda.current_stream()
+    e = torch.empty(0)
+
+    def time_solve(fn, n):
+        times, info = [], None
+        for rep in range(6):
+            x = torch.zeros(n, device=dev)
+            a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            info = fn(x)
+            z.record(stream)
+            torch.cuda.synchronize()
+            if rep:
+                times.append(a.elapsed_time(z))
+        return {"ms": statistics.median(times), "iters": info["iters"], "true_resid": info["true_resid"],
+                "persistent": bool(info["persistent"])}
+
+    out = {}
+    for name, grids in (("cg", (32, 71, 84, 101, 123, 143)), ("bicgstab", (32, 64, 100, 128))):
+        rows = []
+        for g in grids:
+            c = W.laplacian_2d(g)
+            A = mps.spmv.csr_tensor(torch.from_numpy(c.keys()), torch.from_numpy(c.vals), e, e, e,
+                                    c.n, c.n, fill_outputs=False)
+            b = torch.from_numpy(W.rhs(c.n, 1)).to(dev)
+            solve = (lambda x: A.cgd(b, x, tol=1e-6, max_iter=20000)) if name == "cg" else \
+                (lambda x: A.bicgstab(b, x, tol=1e-6, max_iter=20000))
+            row = {"n": c.n}
+            for pers in (True, False):
+                A.set_persistent(pers)
+                row["persistent_form" if pers else "graph_form"] = time_solve(solve, c.n)
+            rows.append(row)
+        out[name] = rows
+    return out
+
+
 def configs_legs(args, dev, c3):
     import torch
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2
     out = {"C1": c1_leg(dev, flush), "C2": c2_leg(dev, flush)}
     del flush
+    out["reference_benchmark_sizes"] = reference_sizes_leg(dev)
     if c3 is not None:
         c3.drop_coo()
         out["C3"] = c3_leg(args, dev, c3)
