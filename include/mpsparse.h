@@ -77,9 +77,9 @@ typedef struct {
     double true_resid;        /* ||b - A x|| / ||b|| of the returned x, recomputed on the
                                  GPU after the solve in FP64 (FP64 products and sums
                                  over the stored FP32 matrix and x) */
-    int32_t persistent;       /* 1: the solve ran as one persistent kernel
-                                 (CG / Jacobi-PCG on a CSR whose rows fit one CTA
-                                 per SM; see mps_csr_set_persistent) */
+    int32_t persistent;       /* nonzero: the solve ran as one persistent kernel
+                                 (see mps_csr_set_persistent) in its gather (1),
+                                 window (2) or stream (3) form; 0: graph form */
     int32_t reserved;
 } mps_solve_info;
 
@@ -87,7 +87,8 @@ typedef struct {
 void mps_solve_opts_default(mps_solve_opts* opts);
 const char* mps_last_error_string(void);
 const char* mps_status_string(mps_status s);
-/* 3: mps_solve_info carries stop_rule_met, true_resid and persistent. */
+/* 3: mps_solve_info carries stop_rule_met, true_resid and persistent;
+ * 4: persistent (also in mps_ir_info) names the persistent form. */
 int32_t mps_abi_version(void);
 
 /* ---- COO -> CSR ------------------------------------------------------- */
@@ -221,20 +222,23 @@ typedef struct {
     int32_t outer_iters;      /* refinement sweeps (restart) or residual replacements */
     int32_t inner_iters;      /* total inner CG iterations */
     int32_t converged;
-    int32_t persistent;       /* 1: the solve ran as one persistent kernel
-                                 (see mps_csr_set_persistent) */
+    int32_t persistent;       /* nonzero: the solve ran as one persistent kernel,
+                                 1 gather, 2 window, 3 stream form (see
+                                 mps_csr_set_persistent) */
     double rel_resid;         /* FP64 true residual at exit */
 } mps_ir_info;
 
-/* Reliable-update FSAI-PCG in product form (M = G^T G), and plain CG /
- * Jacobi-PCG (mps_csr_cg without reference_compat or host_loop), run as ONE
- * cooperative kernel -- one CTA per SM holding its rows of A (and M) in
- * shared memory, grid barriers between the steps of an iteration --
- * whenever those rows fit (about 200 KB per SM; e.g. 2D 5-point systems up
- * to ~300k rows with M, ~1M rows without); otherwise, or with enable = 0, as
- * the CUDA graph of two or three kernels per iteration.  Default 1.  Both
- * forms compute the same iterates up to the grouping of the FP64 partial
- * sums.  No reference counterpart. */
+/* Reliable-update FSAI-PCG in product form (M = G^T G), plain CG /
+ * Jacobi-PCG and BiCGSTAB (mps_csr_cg / mps_csr_bicgstab without
+ * reference_compat or host_loop), run as ONE cooperative kernel -- one CTA
+ * per SM, grid barriers between the steps of an iteration -- whenever the
+ * CTA's share fits its shared memory (about 220 KB): its rows of A (and M)
+ * with the vector window they reach (window form), its rows alone (gather
+ * form), or -- rows read from L2 in every step -- the window alone (stream
+ * form; 2D 5-point systems up to about a million rows).  Otherwise, or with enable = 0, as the CUDA graph of two or
+ * three kernels per iteration.  Default 1.  The forms compute the same
+ * iterates up to the grouping of the FP64 partial sums.  No reference
+ * counterpart. */
 mps_status mps_csr_set_persistent(mps_csr* A, int32_t enable);
 
 mps_status mps_csr_cg_mixed(mps_csr* A, const double* d_b, double* d_x, const mps_ir_opts* opts,

@@ -179,7 +179,7 @@ mps_status build_from_keys(CsrMat& m, const uint64_t* keys, const uint32_t* payl
 
 extern "C" {
 
-int32_t mps_abi_version(void) { return 3; }
+int32_t mps_abi_version(void) { return 4; }
 
 void mps_solve_opts_default(mps_solve_opts* o) {
     if (!o) return;
@@ -477,9 +477,10 @@ static mps_status solve_errors(mps_csr* h, const unsigned* e2, mps_status st, cu
 }
 
 // Plain CG / Jacobi-PCG, or BiCGSTAB, as one persistent cooperative kernel
-// when A's rows fit one CTA per SM (fsai_persistent.cu; BiCGSTAB in the
-// window form only); *ran = false: not eligible, the graph form runs instead.  Same parameters, result places and report as
-// run_solve.
+// when A's rows (or, in the stream form, their vector windows) fit one CTA
+// per SM (fsai_persistent.cu; BiCGSTAB in the window and stream forms only);
+// *ran = false: not eligible, the graph form runs instead.  Same parameters,
+// result places and report as run_solve.
 static mps_status csr_persistent(SolverKind kind, mps_csr* h, const float* b, float* x,
                                  const mps_solve_opts& o, mps_solve_info* info, cudaStream_t s, bool* ran) {
     *ran = false;
@@ -505,7 +506,7 @@ static mps_status csr_persistent(SolverKind kind, mps_csr* h, const float* b, fl
     MPS_CUDA(cudaMemcpyAsync(H.ws.h_sc, H.ws.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
     MPS_CUDA(cudaStreamSynchronize(s));
     const mps_status st = solve_report(kind, H, info, nullptr, true);
-    if (info) info->persistent = 1;
+    if (info) info->persistent = 1 + h->pp_a.form;
     return st;
 }
 
@@ -736,7 +737,7 @@ extern "C" mps_status mps_csr_cg_mixed(mps_csr* h, const double* d_b, double* d_
             info->outer_iters = rep;
             info->inner_iters = ii.iters;
             info->converged = ii.converged && rel <= tol;
-            info->persistent = persisted ? 1 : 0;
+            info->persistent = persisted ? 1 + (fsai_pc ? h->pp.form : h->pp_a.form) : 0;
             info->rel_resid = rel;
         }
         return st;

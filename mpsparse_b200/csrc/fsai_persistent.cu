@@ -19,11 +19,16 @@
 // (p, or r') over the column window the CTA's rows reach, formed while it is
 // loaded, and the row sums read shared memory only; in the gather form
 // (windows too large) the row sums gather the vector entries and form them
-// per nonzero.  The arithmetic of every row is the graph form's (same products,
+// per nonzero; in the stream form (rows too large for shared memory, the
+// window not) the vector is staged as in the window form and the rows are
+// read from global memory (L2) in every step.  The arithmetic of every row is the graph form's (same products,
 // same order of additions, same FP32 / FP64 rounding points); only the FP64
 // sums of the per-CTA partials group differently.  Every CTA sums all
 // partials itself in one fixed order, so all CTAs take the same decisions
 // from the same bits and reach the same barriers.
+//
+// The host picks the window form when its footprint fits, else the gather
+// form, else the stream form (plan_rows).
 //
 // Safety: the launch is cooperative (the runtime refuses a grid that cannot
 // be co-resident); rows are assigned by blockIdx (no SM ids); every barrier
@@ -46,6 +51,10 @@ constexpr unsigned kGridSpinLimit = 1u << 22;    // polls of one barrier wait (a
 constexpr int kCountWord = 0;                    // barrier words: [0] arrivals (monotonic),
 constexpr int kAbortWord = 2;                    // [2] abort
 constexpr int kBarWords = 3;
+// Persistent forms: rows in shared memory with the vector gathered per
+// nonzero (gather), rows in shared memory with the vector's window staged
+// (window), rows read from global memory with the window staged (stream).
+constexpr int kGatherForm = 0, kWindowForm = 1, kStreamForm = 2;
 
 struct PersistDev {
     const int* a_rp;
@@ -240,14 +249,22 @@ __device__ __forceinline__ size_t round_up(size_t off, size_t a) { return (off +
 template <bool NARROW>
 using ColIdx = std::conditional_t<NARROW, unsigned short, int>;
 
-// Row li of a block of a CSR held in shared memory times a gathered vector:
-// the products rounded to FP32 first, then added in column order (the tile
-// kernels' arithmetic).
-template <class IT, class F>
+// A matrix entry: from shared memory, or (G) a read-only load from global
+// memory (the stream form's rows, unchanged for the kernel's lifetime).
+template <bool G, class T>
+__device__ __forceinline__ T ldm(const T* p) {
+    if constexpr (G) return __ldg(p);
+    else return *p;
+}
+
+// Row li of a block of a CSR (in shared memory, or G: in global memory)
+// times a gathered vector: the products rounded to FP32 first, then added in
+// column order (the tile kernels' arithmetic).
+template <bool G = false, class IT, class F>
 __device__ __forceinline__ float row_f32(const int* rp, const IT* ci, const float* v, int li, F gather) {
     float s = 0.f;
-    const int e = rp[li + 1];
-    for (int k = rp[li]; k < e; ++k) s = __fadd_rn(s, __fmul_rn(v[k], gather((int)ci[k])));
+    const int e = ldm<G>(rp + li + 1);
+    for (int k = ldm<G>(rp + li); k < e; ++k) s = __fadd_rn(s, __fmul_rn(ldm<G>(v + k), gather((int)ldm<G>(ci + k))));
     return s;
 }
 
@@ -255,11 +272,11 @@ __device__ __forceinline__ float row_f32(const int* rp, const IT* ci, const floa
 // order exactly as row_f32 does: the gathers of both rows are issued four at
 // a time before their products are added, so the two rows' gather latencies
 // overlap instead of adding up.
-template <class IT, class F>
+template <bool G = false, class IT, class F>
 __device__ __forceinline__ void row_pair_f32(const int* rp, const IT* ci, const float* v, int li0,
                                              int li1, bool has1, F gather, float& s0, float& s1) {
-    const int b0 = rp[li0], e0 = rp[li0 + 1];
-    const int b1 = has1 ? rp[li1] : 0, e1 = has1 ? rp[li1 + 1] : 0;
+    const int b0 = ldm<G>(rp + li0), e0 = ldm<G>(rp + li0 + 1);
+    const int b1 = has1 ? ldm<G>(rp + li1) : 0, e1 = has1 ? ldm<G>(rp + li1 + 1) : 0;
     s0 = 0.f;
     s1 = 0.f;
     const int len = max(e0 - b0, e1 - b1);
@@ -268,10 +285,10 @@ __device__ __forceinline__ void row_pair_f32(const int* rp, const IT* ci, const 
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const bool in0 = b0 + k + u < e0, in1 = b1 + k + u < e1;
-            w0[u] = in0 ? v[b0 + k + u] : 0.f;
-            w1[u] = in1 ? v[b1 + k + u] : 0.f;
-            g0[u] = in0 ? gather((int)ci[b0 + k + u]) : 0.f;
-            g1[u] = in1 ? gather((int)ci[b1 + k + u]) : 0.f;
+            w0[u] = in0 ? ldm<G>(v + b0 + k + u) : 0.f;
+            w1[u] = in1 ? ldm<G>(v + b1 + k + u) : 0.f;
+            g0[u] = in0 ? gather((int)ldm<G>(ci + b0 + k + u)) : 0.f;
+            g1[u] = in1 ? gather((int)ldm<G>(ci + b1 + k + u)) : 0.f;
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -281,9 +298,11 @@ __device__ __forceinline__ void row_pair_f32(const int* rp, const IT* ci, const 
     }
 }
 
-// WIN: window form (16-bit window-relative columns); else gather form.
-template <bool WIN>
+// FORM: kGatherForm, kWindowForm or kStreamForm (see their definition).
+template <int FORM>
 __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
+    constexpr bool WIN = FORM != kGatherForm;
+    constexpr bool STREAM = FORM == kStreamForm;
     extern __shared__ __align__(16) unsigned char psmem[];
     __shared__ PersistShared sh;
     const int tid = threadIdx.x;
@@ -293,36 +312,62 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
     const int m0 = P.m_rp[r0], nm = P.m_rp[r1] - m0;
     // WIN: the multiplied vector over the CTA's column window, staged once
     // per step (coalesced loads) so the row sums read shared memory only
-    // (columns stored 16-bit, relative to the window); the own rows' x (FP64,
-    // written through to global) and D^-1 stay in shared memory too.
-    // shared layout: arp[R+1] | mrp[R+1] | aci[na] | mci[nm] | pad | av[na] |
-    //                mv[nm] | (WIN: pad | xs[R] | ds[R] | win[hi - lo])
-    using CI = ColIdx<WIN>;
+    // for the vector; the own rows' x (FP64, written through to global) and
+    // D^-1 stay in shared memory too.  Rows of A and M: in shared memory
+    // (window form: columns 16-bit, relative to the window), or (stream form)
+    // read from global memory in every step.
+    // shared layout: [arp[R+1] | mrp[R+1] | aci[na] | mci[nm] | pad | av[na] |
+    //                mv[nm] | pad] | (WIN: xs[R] | ds[R] | win[hi - lo])
+    using CI = ColIdx<FORM == kWindowForm>;
     const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
-    const int coff = wlo;   // global column = coff + stored index (wlo = 0 in the gather form)
-    int* arp = reinterpret_cast<int*>(psmem);
-    int* mrp = arp + (R + 1);
-    CI* aci = reinterpret_cast<CI*>(mrp + (R + 1));
-    CI* mci = aci + na;
-    const size_t off_v = round_up(8 * (size_t)(R + 1) + sizeof(CI) * (size_t)(na + nm), 4);
-    float* av = reinterpret_cast<float*>(psmem + off_v);
-    float* mv = av + na;
-    double* xs = reinterpret_cast<double*>(psmem + round_up(off_v + 4 * (size_t)(na + nm), 8));
+    const int coff = FORM == kWindowForm ? wlo : 0;   // global column = coff + stored index
+    const int wbase = STREAM ? wlo : 0;                // window slot = stored index - wbase
+    const int* arp;
+    const int* mrp;
+    const CI* aci;
+    const CI* mci;
+    const float* av;
+    const float* mv;
+    size_t off_own = 0;
+    if constexpr (STREAM) {   // absolute row offsets into the global arrays
+        arp = P.a_rp + r0;
+        mrp = P.m_rp + r0;
+        aci = P.a_ci;
+        mci = P.m_ci;
+        av = P.a_v;
+        mv = P.m_v;
+    } else {
+        int* arp_s = reinterpret_cast<int*>(psmem);
+        int* mrp_s = arp_s + (R + 1);
+        CI* aci_s = reinterpret_cast<CI*>(mrp_s + (R + 1));
+        CI* mci_s = aci_s + na;
+        const size_t off_v = round_up(8 * (size_t)(R + 1) + sizeof(CI) * (size_t)(na + nm), 4);
+        float* av_s = reinterpret_cast<float*>(psmem + off_v);
+        float* mv_s = av_s + na;
+        off_own = round_up(off_v + 4 * (size_t)(na + nm), 8);
+        for (int i = tid; i <= R; i += kPNT) {
+            arp_s[i] = P.a_rp[r0 + i] - a0;
+            mrp_s[i] = P.m_rp[r0 + i] - m0;
+        }
+        for (int k = tid; k < na; k += kPNT) {
+            aci_s[k] = (CI)(P.a_ci[a0 + k] - coff);
+            av_s[k] = P.a_v[a0 + k];
+        }
+        for (int k = tid; k < nm; k += kPNT) {
+            mci_s[k] = (CI)(P.m_ci[m0 + k] - coff);
+            mv_s[k] = P.m_v[m0 + k];
+        }
+        arp = arp_s;
+        mrp = mrp_s;
+        aci = aci_s;
+        mci = mci_s;
+        av = av_s;
+        mv = mv_s;
+    }
+    double* xs = reinterpret_cast<double*>(psmem + off_own);
     float* ds = reinterpret_cast<float*>(xs + (WIN ? R : 0));
     float* win = ds + (WIN ? R : 0);
-    auto wg = [&](int c) { return win[c]; };
-    for (int i = tid; i <= R; i += kPNT) {
-        arp[i] = P.a_rp[r0 + i] - a0;
-        mrp[i] = P.m_rp[r0 + i] - m0;
-    }
-    for (int k = tid; k < na; k += kPNT) {
-        aci[k] = (CI)(P.a_ci[a0 + k] - coff);
-        av[k] = P.a_v[a0 + k];
-    }
-    for (int k = tid; k < nm; k += kPNT) {
-        mci[k] = (CI)(P.m_ci[m0 + k] - coff);
-        mv[k] = P.m_v[m0 + k];
-    }
+    auto wg = [&](int c) { return win[c - wbase]; };
     if constexpr (WIN) {
         for (int li = tid; li < R; li += kPNT) {
             xs[li] = 0.0;
@@ -368,7 +413,7 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
         double acc[1] = {0.0};
         const float* rc = P.r0;
         for (int li = tid; li < R; li += kPNT) {
-            const float s = row_f32(mrp, mci, mv, li, [&](int c) { return ldv(rc + coff + c); });
+            const float s = row_f32<STREAM>(mrp, mci, mv, li, [&](int c) { return ldv(rc + coff + c); });
             const int i = r0 + li;
             P.z[i] = s;
             acc[0] += (double)ldv(rc + i) * (double)s;
@@ -409,7 +454,7 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                     const int lj = li + kPNT;
                     const bool has1 = lj < R;
                     float s0, s1;
-                    if constexpr (WIN) row_pair_f32(arp, aci, av, li, lj, has1, wg, s0, s1);
+                    if constexpr (WIN) row_pair_f32<STREAM>(arp, aci, av, li, lj, has1, wg, s0, s1);
                     else row_pair_f32(arp, aci, av, li, lj, has1, dir, s0, s1);
                     own(li, s0);
                     if (has1) own(lj, s1);
@@ -436,6 +481,9 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                         xs[li] = xv;
                         P.x[r0 + li] = xv;
                     }
+                    // step 2 restages the window (r' over p): every thread's
+                    // reads of p above come first
+                    __syncthreads();
                 }
             }
             // ---- step 2: r' = r - alpha q on the fly, z = M r', x += alpha p
@@ -466,7 +514,7 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                     const int lj = li + kPNT;
                     const bool has1 = lj < R;
                     float s0, s1;
-                    if constexpr (WIN) row_pair_f32(mrp, mci, mv, li, lj, has1, wg, s0, s1);
+                    if constexpr (WIN) row_pair_f32<STREAM>(mrp, mci, mv, li, lj, has1, wg, s0, s1);
                     else row_pair_f32(mrp, mci, mv, li, lj, has1, res, s0, s1);
                     own(li, s0);
                     if (has1) own(lj, s1);
@@ -523,7 +571,7 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
                 const float* rc = (S.iter & 1) ? P.r1 : P.r0;
                 double acc[1] = {0.0};
                 for (int li = tid; li < R; li += kPNT) {
-                    const float s = row_f32(mrp, mci, mv, li, [&](int c) { return ldv(rc + coff + c); });
+                    const float s = row_f32<STREAM>(mrp, mci, mv, li, [&](int c) { return ldv(rc + coff + c); });
                     const int i = r0 + li;
                     P.z[i] = s;
                     acc[0] += (double)ldv(rc + i) * (double)s;
@@ -555,38 +603,56 @@ out:
 // IR (reliable updates, cg_mixed without FSAI): x accumulated in FP64
 // (P.x), b in FP64 (P.b), the stop rule of cg_finalize_ir, and -- when due --
 // the residual replacement r = (float)(b - A x) in FP64 in the same kernel.
-template <bool IR, bool WIN>
+template <bool IR, int FORM>
 __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
+    constexpr bool WIN = FORM != kGatherForm;
+    constexpr bool STREAM = FORM == kStreamForm;
     extern __shared__ __align__(16) unsigned char psmem[];
     __shared__ PersistShared sh;
     const int tid = threadIdx.x;
     const int r0 = P.row_start[blockIdx.x], r1 = P.row_start[blockIdx.x + 1];
     const int R = r1 - r0;
     const int a0 = P.a_rp[r0], na = P.a_rp[r1] - a0;
-    // shared layout: arp[R+1] | aci[na] | pad | av[na]; the window form
-    // (columns 16-bit, relative to the window) adds the own rows' x
-    // (FP64 under IR, written through to global), r (written through), q
-    // and D^-1, then the vector window:
-    //   ... av | pad to 8 | xs[R] | rs[R] | qs[R] | ds[R] | win[hi - lo]
+    // shared layout: [arp[R+1] | aci[na] | pad | av[na] | pad to 8] (not in
+    // the stream form, whose rows are read from global memory); the window
+    // and stream forms add the own rows' x (FP64 under IR, written through
+    // to global), r (written through), q and D^-1, then the vector window
+    // (window form: columns 16-bit, relative to the window):
+    //   ... | xs[R] | rs[R] | qs[R] | ds[R] | win[hi - lo]
     using XT = std::conditional_t<IR, double, float>;
-    using CI = ColIdx<WIN>;
+    using CI = ColIdx<FORM == kWindowForm>;
     const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
-    const int coff = wlo;   // global column = coff + stored index (wlo = 0 in the gather form)
-    int* arp = reinterpret_cast<int*>(psmem);
-    CI* aci = reinterpret_cast<CI*>(arp + (R + 1));
-    const size_t off_v = round_up(4 * (size_t)(R + 1) + sizeof(CI) * (size_t)na, 4);
-    float* av = reinterpret_cast<float*>(psmem + off_v);
-    XT* xs = reinterpret_cast<XT*>(psmem + round_up(off_v + 4 * (size_t)na, 8));
+    const int coff = FORM == kWindowForm ? wlo : 0;   // global column = coff + stored index
+    const int wbase = STREAM ? wlo : 0;                // window slot = stored index - wbase
+    const int* arp;
+    const CI* aci;
+    const float* av;
+    size_t off_own = 0;
+    if constexpr (STREAM) {   // absolute row offsets into the global arrays
+        arp = P.a_rp + r0;
+        aci = P.a_ci;
+        av = P.a_v;
+    } else {
+        int* arp_s = reinterpret_cast<int*>(psmem);
+        CI* aci_s = reinterpret_cast<CI*>(arp_s + (R + 1));
+        const size_t off_v = round_up(4 * (size_t)(R + 1) + sizeof(CI) * (size_t)na, 4);
+        float* av_s = reinterpret_cast<float*>(psmem + off_v);
+        off_own = round_up(off_v + 4 * (size_t)na, 8);
+        for (int i = tid; i <= R; i += kPNT) arp_s[i] = P.a_rp[r0 + i] - a0;
+        for (int k = tid; k < na; k += kPNT) {
+            aci_s[k] = (CI)(P.a_ci[a0 + k] - coff);
+            av_s[k] = P.a_v[a0 + k];
+        }
+        arp = arp_s;
+        aci = aci_s;
+        av = av_s;
+    }
+    XT* xs = reinterpret_cast<XT*>(psmem + off_own);
     float* rs = reinterpret_cast<float*>(xs + (WIN ? R : 0));
     float* qs = rs + (WIN ? R : 0);
     float* ds = qs + (WIN ? R : 0);
     float* win = ds + (WIN ? R : 0);
-    auto wg = [&](int c) { return win[c]; };
-    for (int i = tid; i <= R; i += kPNT) arp[i] = P.a_rp[r0 + i] - a0;
-    for (int k = tid; k < na; k += kPNT) {
-        aci[k] = (CI)(P.a_ci[a0 + k] - coff);
-        av[k] = P.a_v[a0 + k];
-    }
+    auto wg = [&](int c) { return win[c - wbase]; };
     if (tid == 0) {
         sh.gen = 0;
         sh.ok = 1;
@@ -705,7 +771,7 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
                 const int lj = li + kPNT;
                 const bool has1 = lj < R;
                 float s0, s1;
-                if constexpr (WIN) row_pair_f32(arp, aci, av, li, lj, has1, wg, s0, s1);
+                if constexpr (WIN) row_pair_f32<STREAM>(arp, aci, av, li, lj, has1, wg, s0, s1);
                 else row_pair_f32(arp, aci, av, li, lj, has1, dir, s0, s1);
                 own(li, s0);
                 if (has1) own(lj, s1);
@@ -790,9 +856,10 @@ out:
 // writes its rows of the new ones while slower CTAs still gather the old.
 // s and t are never written to global memory: every CTA forms s over its
 // own window, and keeps its rows of t in shared memory.
-// Window form only (the plan's window-form budget covers the own rows' x
+// Window or stream form (the plan's budget for them covers the own rows' x
 // and t kept here).  Buffers: P.r0 = r, P.r1 = r0 (the shadow residual),
 // P.p0 / P.p1 = p, P.q / P.z = v, P.b32 = b, P.x32 = x.
+template <int FORM>
 __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
     extern __shared__ __align__(16) unsigned char psmem[];
     __shared__ PersistShared sh;
@@ -800,24 +867,42 @@ __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
     const int r0 = P.row_start[blockIdx.x], r1 = P.row_start[blockIdx.x + 1];
     const int R = r1 - r0;
     const int a0 = P.a_rp[r0], na = P.a_rp[r1] - a0;
-    // shared layout: arp[R+1] | aci[na] | pad | av[na] | pad | xs[R] | ts[R] |
-    //                win[hi - lo]; columns 16-bit, window-relative
-    using CI = ColIdx<true>;
+    // shared layout: [arp[R+1] | aci[na] | pad | av[na] | pad to 8] (window
+    // form: columns 16-bit, window-relative; the stream form reads its rows
+    // from global memory) | xs[R] | ts[R] | win[hi - lo]
+    static_assert(FORM == kWindowForm || FORM == kStreamForm, "BiCGSTAB: window or stream form");
+    constexpr bool STREAM = FORM == kStreamForm;
+    using CI = ColIdx<!STREAM>;
     const int wlo = P.win[2 * blockIdx.x], whi = P.win[2 * blockIdx.x + 1];
-    const int coff = wlo;   // global column = coff + stored index
-    int* arp = reinterpret_cast<int*>(psmem);
-    CI* aci = reinterpret_cast<CI*>(arp + (R + 1));
-    const size_t off_v = round_up(4 * (size_t)(R + 1) + sizeof(CI) * (size_t)na, 4);
-    float* av = reinterpret_cast<float*>(psmem + off_v);
-    float* xs = reinterpret_cast<float*>(psmem + round_up(off_v + 4 * (size_t)na, 8));
+    const int coff = STREAM ? 0 : wlo;   // global column = coff + stored index
+    const int wbase = STREAM ? wlo : 0;  // window slot = stored index - wbase
+    const int* arp;
+    const CI* aci;
+    const float* av;
+    size_t off_own = 0;
+    if constexpr (STREAM) {   // absolute row offsets into the global arrays
+        arp = P.a_rp + r0;
+        aci = P.a_ci;
+        av = P.a_v;
+    } else {
+        int* arp_s = reinterpret_cast<int*>(psmem);
+        CI* aci_s = reinterpret_cast<CI*>(arp_s + (R + 1));
+        const size_t off_v = round_up(4 * (size_t)(R + 1) + sizeof(CI) * (size_t)na, 4);
+        float* av_s = reinterpret_cast<float*>(psmem + off_v);
+        off_own = round_up(off_v + 4 * (size_t)na, 8);
+        for (int i = tid; i <= R; i += kPNT) arp_s[i] = P.a_rp[r0 + i] - a0;
+        for (int k = tid; k < na; k += kPNT) {
+            aci_s[k] = (CI)(P.a_ci[a0 + k] - coff);
+            av_s[k] = P.a_v[a0 + k];
+        }
+        arp = arp_s;
+        aci = aci_s;
+        av = av_s;
+    }
+    float* xs = reinterpret_cast<float*>(psmem + off_own);
     float* ts = xs + R;
     float* win = ts + R;
-    auto wg = [&](int c) { return win[c]; };
-    for (int i = tid; i <= R; i += kPNT) arp[i] = P.a_rp[r0 + i] - a0;
-    for (int k = tid; k < na; k += kPNT) {
-        aci[k] = (CI)(P.a_ci[a0 + k] - coff);
-        av[k] = P.a_v[a0 + k];
-    }
+    auto wg = [&](int c) { return win[c - wbase]; };
     if (tid == 0) {
         sh.gen = 0;
         sh.ok = 1;
@@ -870,7 +955,7 @@ __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
                 const int lj = li + kPNT;
                 const bool has1 = lj < R;
                 float s0, s1;
-                row_pair_f32(arp, aci, av, li, lj, has1, wg, s0, s1);
+                row_pair_f32<STREAM>(arp, aci, av, li, lj, has1, wg, s0, s1);
                 own(li, s0);
                 if (has1) own(lj, s1);
             }
@@ -907,7 +992,7 @@ __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
                 const int lj = li + kPNT;
                 const bool has1 = lj < R;
                 float s0, s1;
-                row_pair_f32(arp, aci, av, li, lj, has1, wg, s0, s1);
+                row_pair_f32<STREAM>(arp, aci, av, li, lj, has1, wg, s0, s1);
                 own(li, s0);
                 if (has1) own(lj, s1);
             }
@@ -1069,7 +1154,7 @@ static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const C
     const int* start = h.data();
     const int* win = start + grid + 1 + kBarWords;
     const int* cnt = win + 2 * grid;
-    size_t worst = 0, worst_win = 0;
+    size_t worst = 0, worst_win = 0, worst_stream = 0;
     for (int c = 0; c < grid; ++c) {
         const int rows = start[c + 1] - start[c];
         if (rows < 0) return cudaSuccess;
@@ -1084,23 +1169,38 @@ static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const C
         const size_t bw = 4 * (size_t)words * ((size_t)rows + 1) + 6 * nz + 12 + 4 * w +
                           (M ? 12 : 20) * (size_t)rows;   // FSAI: x, D^-1; CG: x, r, q, D^-1
         worst_win = std::max(worst_win, w > 65536 ? ~(size_t)0 : bw);
+        // stream form: the vector window and the own rows' vectors only
+        worst_stream = std::max(worst_stream, 4 * w + (M ? 12 : 20) * (size_t)rows);
     }
     pp.grid = grid;
-    pp.win = worst_win <= kPSmemWinBudget ? 1 : 0;
-    const size_t need = pp.win ? worst_win : worst;
-    if (pp.win) {   // the larger footprint must still leave one CTA resident per SM
+    // a footprint above the gather budget must still leave one CTA
+    // resident per SM
+    auto resident = [&](size_t need) {
+        if (need > kPSmemWinBudget) return false;
         const int sz = (int)(((need + 15) / 16) * 16);
         int per = 0;
         cudaError_t ew = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sz);
         if (ew == cudaSuccess) ew = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kPNT, sz);
         if (ew != cudaSuccess || per < 1) {
             cudaGetLastError();
-            pp.win = 0;
+            return false;
         }
+        return true;
+    };
+    size_t need;
+    if (resident(worst_win)) {
+        pp.form = kWindowForm;
+        need = worst_win;
+    } else if (worst <= kPSmemBudget) {
+        pp.form = kGatherForm;
+        need = worst;
+    } else if (resident(worst_stream)) {
+        pp.form = kStreamForm;
+        need = worst_stream;
+    } else {
+        return cudaSuccess;   // not eligible: the graph form runs
     }
-    // a window form can fit where the gather form does not
-    if (!pp.win && worst > kPSmemBudget) return cudaSuccess;   // rows do not fit: not eligible
-    pp.smem = (((pp.win ? need : worst) + 15) / 16) * 16;
+    pp.smem = ((need + 15) / 16) * 16;
     pp.state = 1;
     return cudaSuccess;
 }
@@ -1109,7 +1209,7 @@ static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const C
 cudaError_t persist_plan_build(mps_csr* h, cudaStream_t s) {
     h->pp.state = -1;
     if (!h->use_m || !h->M.rp || h->A.n_rows != h->M.n_rows) return cudaSuccess;
-    return plan_rows(h->pp, (int)h->A.n_rows, reinterpret_cast<const void*>(fsai_pcg_persistent<false>),
+    return plan_rows(h->pp, (int)h->A.n_rows, reinterpret_cast<const void*>(fsai_pcg_persistent<kGatherForm>),
                      h->A, &h->M, s);
 }
 
@@ -1117,7 +1217,7 @@ cudaError_t persist_plan_build(mps_csr* h, cudaStream_t s) {
 cudaError_t persist_plan_build_a(mps_csr* h, cudaStream_t s) {
     h->pp_a.state = -1;
     if (h->A.n_rows != h->A.n_cols) return cudaSuccess;
-    return plan_rows(h->pp_a, (int)h->A.n_rows, reinterpret_cast<const void*>(cg_persistent<false, false>),
+    return plan_rows(h->pp_a, (int)h->A.n_rows, reinterpret_cast<const void*>(cg_persistent<false, kGatherForm>),
                      h->A, nullptr, s);
 }
 
@@ -1154,11 +1254,16 @@ cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s, const double* b64, doub
     P.b = b64;
     P.x = x64;
     P.win = h->pp_a.d_row_start + h->pp_a.grid + 1 + kBarWords;
-    const bool w = h->pp_a.win != 0;
-    const void* k = b64 ? (w ? reinterpret_cast<const void*>(cg_persistent<true, true>)
-                             : reinterpret_cast<const void*>(cg_persistent<true, false>))
-                        : (w ? reinterpret_cast<const void*>(cg_persistent<false, true>)
-                             : reinterpret_cast<const void*>(cg_persistent<false, false>));
+    const int f = h->pp_a.form;
+    const void* k;
+    if (b64)
+        k = f == kWindowForm ? reinterpret_cast<const void*>(cg_persistent<true, kWindowForm>)
+            : f == kStreamForm ? reinterpret_cast<const void*>(cg_persistent<true, kStreamForm>)
+                               : reinterpret_cast<const void*>(cg_persistent<true, kGatherForm>);
+    else
+        k = f == kWindowForm ? reinterpret_cast<const void*>(cg_persistent<false, kWindowForm>)
+            : f == kStreamForm ? reinterpret_cast<const void*>(cg_persistent<false, kStreamForm>)
+                               : reinterpret_cast<const void*>(cg_persistent<false, kGatherForm>);
     cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->pp_a.smem);
@@ -1167,7 +1272,7 @@ cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s, const double* b64, doub
     return cudaLaunchCooperativeKernel(k, dim3(h->pp_a.grid), dim3(kPNT), args, h->pp_a.smem, s);
 }
 
-// BiCGSTAB as one cooperative launch (window form only): b is H.v(vB), x
+// BiCGSTAB as one cooperative launch (window or stream form): b is H.v(vB), x
 // lands in H.v(vX) and the final scalars in H.ws.sc; the parameters must be
 // in H.ws.d_params.  cudaErrorNotSupported: not eligible (the graph form runs).
 cudaError_t persist_bicg_solve(mps_csr* h, cudaStream_t s) {
@@ -1175,7 +1280,7 @@ cudaError_t persist_bicg_solve(mps_csr* h, cudaStream_t s) {
         const cudaError_t e = persist_plan_build_a(h, s);
         if (e != cudaSuccess) return e;
     }
-    if (h->pp_a.state != 1 || !h->pp_a.win) return cudaErrorNotSupported;
+    if (h->pp_a.state != 1 || h->pp_a.form == kGatherForm) return cudaErrorNotSupported;
     SolverHost& H = h->H;
     PersistDev P{};
     P.a_rp = h->A.rp;
@@ -1197,7 +1302,8 @@ cudaError_t persist_bicg_solve(mps_csr* h, cudaStream_t s) {
     P.n = (int)h->A.n_rows;
     P.b32 = H.v(vB);
     P.x32 = H.v(vX);
-    const void* k = reinterpret_cast<const void*>(bicg_persistent);
+    const void* k = h->pp_a.form == kStreamForm ? reinterpret_cast<const void*>(bicg_persistent<kStreamForm>)
+                                                : reinterpret_cast<const void*>(bicg_persistent<kWindowForm>);
     cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->pp_a.smem);
@@ -1253,8 +1359,10 @@ cudaError_t persist_solve(mps_csr* h, const double* b64, double* x64, cudaStream
     P.n = (int)h->A.n_rows;
     static_assert(4 * 3 * 1024 <= 4 * kMaxPartials, "partial slots");
     P.win = h->pp.d_row_start + h->pp.grid + 1 + kBarWords;
-    const void* k = h->pp.win ? reinterpret_cast<const void*>(fsai_pcg_persistent<true>)
-                              : reinterpret_cast<const void*>(fsai_pcg_persistent<false>);
+    const int f = h->pp.form;
+    const void* k = f == kWindowForm   ? reinterpret_cast<const void*>(fsai_pcg_persistent<kWindowForm>)
+                    : f == kStreamForm ? reinterpret_cast<const void*>(fsai_pcg_persistent<kStreamForm>)
+                                       : reinterpret_cast<const void*>(fsai_pcg_persistent<kGatherForm>);
     cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->pp.smem);

@@ -41,6 +41,13 @@ void write_back(torch::Tensor& dst, const torch::Tensor& src, int64_t n) {
     dst.narrow(0, 0, n).copy_(s);
 }
 
+// The persistent form a solve ran in (None: the graph form).
+py::object persistent_form(int32_t p) {
+    static const char* names[] = {"gather", "window", "stream"};
+    if (p < 1 || p > 3) return py::none();
+    return py::str(names[p - 1]);
+}
+
 py::dict info_dict(const mps_solve_info& i) {
     py::dict d;
     d["iters"] = i.iters;
@@ -52,6 +59,7 @@ py::dict info_dict(const mps_solve_info& i) {
     d["stop_rule_met"] = (bool)i.stop_rule_met;
     d["true_resid"] = i.true_resid;
     d["persistent"] = (bool)i.persistent;
+    d["persistent_form"] = persistent_form(i.persistent);
     return d;
 }
 
@@ -316,6 +324,7 @@ public:
         d["converged"] = (bool)info.converged;
         d["rel_resid"] = info.rel_resid;
         d["persistent"] = (bool)info.persistent;
+        d["persistent_form"] = persistent_form(info.persistent);
         return d;
     }
     void set_persistent(bool enable) { check(mps_csr_set_persistent(h_, enable ? 1 : 0), "set_persistent"); }

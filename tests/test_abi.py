@@ -41,7 +41,7 @@ def test_argument_checks_without_gpu():
 def test_torch_extension_imports():
     import mpsparse_b200
     from mpsparse_b200 import spmv, bcsr, coo_csr
-    assert mpsparse_b200._C.abi_version() == 3
+    assert mpsparse_b200._C.abi_version() == 4
     assert hasattr(spmv.csr_tensor, "cgd") and hasattr(spmv.csr_tensor, "bicgstab")
     assert hasattr(spmv.csr_tensor, "richardson") and hasattr(spmv.csr_tensor, "iter_solve")
     assert hasattr(bcsr.bcsr_tensor, "bicgstab") and callable(coo_csr.coo_csr)

@@ -86,12 +86,33 @@ def test_persistent_stall_fallback(mps):
     assert info["persistent"] and info["converged"] and info["rel_resid"] <= 1e-8
 
 
-def test_rows_too_large_fall_back_to_graph_form(mps):
-    """Rows of A and M beyond the per-SM shared memory: the graph form runs."""
+def test_persistent_stream_form_fsai(mps, oracle):
+    """700^2 (3,311 rows per CTA): A's and M's rows no longer fit shared
+    memory beside their vector window, nor alone, so the CTAs read them from
+    L2 in every step (stream form) with the window staged as in the window
+    form.  Without residual replacements the iterates agree with the graph
+    form's to rounding of the FP64 partial sums through 2,000 iterations;
+    the full solve reaches its FP64-checked target."""
     c, A = _learned(mps, 700, 700, 33)
     b = torch.from_numpy(W.rhs(c.n, 2).astype(np.float64)).cuda()
+    xg, ig = _solve(A, b, False, tol=1e-30, inner_tol=1e-30, max_inner=2000, max_outer=1)
+    xp, ip = _solve(A, b, True, tol=1e-30, inner_tol=1e-30, max_inner=2000, max_outer=1)
+    assert ip["persistent_form"] == "stream" and ig["persistent_form"] is None
+    assert ip["inner_iters"] == ig["inner_iters"] == 2000
+    assert float((xp - xg).norm() / xg.norm()) <= 1e-12
+    xp, ip = _solve(A, b, True, tol=1e-9, inner_tol=1e-3, max_inner=40000)
+    assert ip["persistent_form"] == "stream" and ip["converged"]
+    Ao = oracle.Csr(*c.to_csr(), c.n)
+    assert oracle.true_residual(Ao, b.cpu().numpy(), xp.cpu().numpy()) <= 1e-9 * 1.01
+
+
+def test_rows_too_large_fall_back_to_graph_form(mps):
+    """1600^2 (17,297 rows per CTA): not even the vector window and the own
+    rows' vectors fit one CTA per SM, so the graph form runs."""
+    c, A = _learned(mps, 1600, 1600, 33)
+    b = torch.from_numpy(W.rhs(c.n, 2).astype(np.float64)).cuda()
     x, info = _solve(A, b, True, tol=1e-6, inner_tol=1e-4, max_inner=40000)
-    assert not info["persistent"] and info["converged"]
+    assert not info["persistent"] and info["persistent_form"] is None and info["converged"]
 
 
 def _cg_system(mps, c):
@@ -151,15 +172,58 @@ def test_persistent_cg_edge_cases(mps):
     assert info["iters"] == 3 and info["persistent"]
 
 
-def test_persistent_cg_falls_back_for_large_rows(mps):
-    """A's rows beyond the per-SM shared memory (1024^2 Laplacian, 5.2 M
-    nonzeros): the graph form runs."""
+def test_persistent_cg_stream_form(mps, oracle):
+    """1024^2 Laplacian (5.2 M nonzeros, 7,085 rows per CTA): A's rows do
+    not fit shared memory, the vector windows do -- plain CG and Jacobi-PCG
+    in the stream form agree with the graph form's first iterates (1e-5
+    relative) and with the FP64 oracle's, and a converged solve needs the
+    graph form's iterations within 1 % and meets the FP32 bar."""
+    from tests.helpers import assert_solved_fp32
     c = W.laplacian_2d(1024)
+    A = _cg_system(mps, c)
+    Ao = oracle.Csr(*c.to_csr(), c.n)
+    b = W.rhs(c.n, 1)
+    bt = torch.from_numpy(b).cuda()
+    for precond in ("none", "jacobi"):
+        for k in (1, 5, 20):
+            xs = []
+            for persistent in (True, False):
+                A.set_persistent(persistent)
+                x = torch.zeros(c.n, device="cuda")
+                info = A.cgd(bt, x, tol=1e-300, max_iter=k, precond=precond)
+                assert info["iters"] == k
+                assert info["persistent_form"] == ("stream" if persistent else None), info
+                xs.append(x.cpu().numpy().astype(np.float64))
+            assert np.linalg.norm(xs[0] - xs[1]) / np.linalg.norm(xs[1]) <= 1e-5, (precond, k)
+            xo, _ = oracle.cg(Ao, b, tol=0.0, max_iter=k, precond=None if precond == "none" else "jacobi")
+            for xk in xs:
+                assert np.linalg.norm(xk - xo) / np.linalg.norm(xo) <= 1e-5, (precond, k)
+    infos = []
+    for persistent in (True, False):
+        A.set_persistent(persistent)
+        x = torch.zeros(c.n, device="cuda")
+        info = A.cgd(bt, x, tol=1e-6, max_iter=40000)
+        assert info["stop_rule_met"] and info["persistent"] == persistent
+        assert_solved_fp32(oracle, Ao, b, x.cpu().numpy(), 1e-6, info)
+        infos.append(info)
+    assert abs(infos[0]["iters"] - infos[1]["iters"]) <= 0.01 * infos[1]["iters"] + 2, infos
+    # reliable updates (cg_mixed) in the stream form reach the FP64 target
+    A.set_persistent(True)
+    x = torch.zeros(c.n, dtype=torch.float64, device="cuda")
+    info = A.cg_mixed(bt.double(), x, tol=1e-9, inner_tol=1e-3, max_inner=40000)
+    assert info["persistent_form"] == "stream" and info["converged"], info
+    assert oracle.true_residual(Ao, b.astype(np.float64), x.cpu().numpy()) <= 1e-9 * 1.01
+
+
+def test_persistent_cg_falls_back_for_large_rows(mps):
+    """1600^2 Laplacian (12.8 M nonzeros, 17,297 rows per CTA): not even the
+    vector window fits one CTA per SM, so the graph form runs."""
+    c = W.laplacian_2d(1600)
     A = _cg_system(mps, c)
     b = torch.from_numpy(W.rhs(c.n, 1)).cuda()
     x = torch.zeros(c.n, device="cuda")
     info = A.cgd(b, x, tol=1e-3, max_iter=200)
-    assert not info["persistent"] and info["iters"] > 0
+    assert not info["persistent"] and info["persistent_form"] is None and info["iters"] > 0
 
 
 @pytest.mark.parametrize("precond", ["none", "jacobi"])
@@ -225,7 +289,7 @@ def test_persistent_gather_form_on_random_graph(mps, oracle):
     A.set_persistent(True)
     x = torch.zeros(c.n, device="cuda")
     info = A.cgd(bt, x, tol=1e-6, max_iter=20000)
-    assert info["persistent"] and info["stop_rule_met"]
+    assert info["persistent_form"] == "gather" and info["stop_rule_met"]
     from mpsparse_b200.fsai import LearnedFsai
     LearnedFsai.load().attach(A)
     A.set_fsai_apply("product")
@@ -255,7 +319,7 @@ def test_persistent_560_window_form(mps, oracle):
     b = torch.from_numpy(W.rhs(c.n, 8).astype(np.float64)).cuda()
     xg, ig = _solve(A, b, False, tol=1e-30, inner_tol=1e-30, max_inner=2000, max_outer=1)
     xp, ip = _solve(A, b, True, tol=1e-30, inner_tol=1e-30, max_inner=2000, max_outer=1)
-    assert ip["persistent"] and not ig["persistent"]
+    assert ip["persistent_form"] == "window" and not ig["persistent"]
     assert ip["inner_iters"] == ig["inner_iters"] == 2000
     assert float((xp - xg).norm() / xg.norm()) <= 1e-12
     xp, ip = _solve(A, b, True, tol=1e-9, inner_tol=1e-3, max_inner=40000)
@@ -329,3 +393,40 @@ def test_persistent_bicgstab_edge_cases(mps):
     assert info["iters"] == 4 and info["persistent"]
     info = A.bicgstab(torch.ones(c.n, device="cuda"), x, reference_compat=True)
     assert not info["persistent"]
+
+
+def test_persistent_bicgstab_stream_form(mps, oracle):
+    """BiCGSTAB on a 1024^2 nonsymmetric 5-point system in the stream form
+    (rows from L2, the staged p and s windows in shared memory): the first
+    iterates agree with the graph form's (1e-5 relative) and with the FP64
+    oracle's up to 5 iterations; a converged solve needs the graph form's
+    iterations within 2 % and meets the FP32 bar."""
+    from tests.helpers import assert_solved_fp32
+    c = _convection_diffusion(1024)
+    A = _cg_system(mps, c)
+    Ao = oracle.Csr(*c.to_csr(), c.n)
+    b = W.rhs(c.n, 4)
+    bt = torch.from_numpy(b).cuda()
+    for k in (1, 5, 20):
+        xs = []
+        for persistent in (True, False):
+            A.set_persistent(persistent)
+            x = torch.zeros(c.n, device="cuda")
+            info = A.bicgstab(bt, x, tol=1e-300, max_iter=k)
+            assert info["iters"] == k
+            assert info["persistent_form"] == ("stream" if persistent else None), info
+            xs.append(x.cpu().numpy().astype(np.float64))
+        assert np.linalg.norm(xs[0] - xs[1]) / np.linalg.norm(xs[1]) <= 1e-5, k
+        if k <= 5:
+            xo, _ = oracle.bicgstab(Ao, b, tol=0.0, max_iter=k)
+            for xk in xs:
+                assert np.linalg.norm(xk - xo) / np.linalg.norm(xo) <= 1e-5, k
+    infos = []
+    for persistent in (True, False):
+        A.set_persistent(persistent)
+        x = torch.zeros(c.n, device="cuda")
+        info = A.bicgstab(bt, x, tol=1e-6, max_iter=40000)
+        assert info["stop_rule_met"] and info["persistent"] == persistent
+        assert_solved_fp32(oracle, Ao, b, x.cpu().numpy(), 1e-6, info)
+        infos.append(info)
+    assert abs(infos[0]["iters"] - infos[1]["iters"]) <= 0.02 * infos[1]["iters"] + 2, infos
