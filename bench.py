@@ -972,6 +972,74 @@ def reference_sizes_leg(dev):
     return out
 
 
+def persistent_forms_leg(dev):
+    """The persistent forms against the graph form of the same solve, device
+    time per solve (median of 5 after a warm-up) on 2D 5-point systems from
+    512^2 to 1024^2: learned-FSAI mixed-precision PCG to an FP64 1e-6 on
+    log-normal diffusion systems (sigma 1.5, correlation 16, seed 5), plain
+    CG on the Laplacian and BiCGSTAB on the Laplacian with each east
+    coupling halved, both to the 1e-6 recurrence target.  512^2 runs in the
+    window form; 700^2 and up, whose rows of A and GᵀG no longer fit shared
+    memory, in the stream form (rows read from L2 in every step)."""
+    import torch
+    import mpsparse_b200 as mps
+    from mpsparse_b200.fsai import LearnedFsai
+    W = _workloads()
+    stream = torch.cuda.current_stream()
+    e = torch.empty(0)
+
+    def time_solve(fn, x):
+        times, info = [], None
+        for rep in range(6):
+            x.zero_()
+            a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            info = fn(x)
+            z.record(stream)
+            torch.cuda.synchronize()
+            if rep:
+                times.append(a.elapsed_time(z))
+        it = info.get("inner_iters", info.get("iters"))
+        ms = statistics.median(times)
+        return {"ms": ms, "iters": it, "us_per_iter": 1e3 * ms / max(1, it),
+                "form": info["persistent_form"],
+                "resid": info.get("true_resid", info.get("rel_resid"))}
+
+    def both(A, fn, x):
+        row = {}
+        for pers in (True, False):
+            A.set_persistent(pers)
+            row["persistent" if pers else "graph"] = time_solve(fn, x)
+        row["speedup"] = row["graph"]["ms"] / row["persistent"]["ms"]
+        return row
+
+    out = []
+    for nx in (512, 700, 800, 1024):
+        c = W.lognormal_diffusion_2d(nx, nx, 1.5, 16.0, 5)
+        A = mps.spmv.csr_tensor(torch.from_numpy(c.keys()), torch.from_numpy(c.vals), e, e, e,
+                                c.n, c.n, fill_outputs=False)
+        LearnedFsai.load().attach(A)
+        A.set_fsai_apply("product")
+        b = torch.from_numpy(W.rhs(c.n, 8).astype(np.float64)).to(dev)
+        x = torch.zeros(c.n, dtype=torch.float64, device=dev)
+        out.append({"solve": "learned FSAI MP-PCG", "grid": nx,
+                    **both(A, lambda x: A.cg_mixed(b, x, tol=1e-6, precond="fsai"), x)})
+        del A
+    c = W.laplacian_2d(1024)
+    x = torch.zeros(c.n, device=dev)
+    b = torch.from_numpy(W.rhs(c.n, 1)).to(dev)
+    A = mps.spmv.csr_tensor(torch.from_numpy(c.keys()), torch.from_numpy(c.vals), e, e, e,
+                            c.n, c.n, fill_outputs=False)
+    out.append({"solve": "cgd", "grid": 1024, **both(A, lambda x: A.cgd(b, x, tol=1e-6, max_iter=40000), x)})
+    vals = c.vals.copy()
+    vals[c.cols == c.rows + 1] *= 0.5
+    A = mps.spmv.csr_tensor(torch.from_numpy(c.keys()), torch.from_numpy(vals.astype(np.float32)), e, e, e,
+                            c.n, c.n, fill_outputs=False)
+    out.append({"solve": "bicgstab", "grid": 1024,
+                **both(A, lambda x: A.bicgstab(b, x, tol=1e-6, max_iter=40000), x)})
+    return out
+
+
 def configs_legs(args, dev, c3):
     import torch
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2
@@ -1069,6 +1137,8 @@ def main():
                     help="only the 256^3 (or --c3-grid) SpMV measurement; for ncu captures")
     ap.add_argument("--only-learned", action="store_true",
                     help="only the learned solve on warmup + steps systems (for profilers)")
+    ap.add_argument("--only-persistent-forms", action="store_true",
+                    help="only the persistent forms against the graph form, 512^2 to 1024^2")
     ap.add_argument("--only-mlp", action="store_true",
                     help="only the network forward/backward timing on one 512^2 system's factor")
     ap.add_argument("--solver", default="learned", choices=["learned", "plain"],
@@ -1102,6 +1172,9 @@ def main():
         return
     if args.only_learned:
         print(json.dumps({"learned": learned_only(args, local)}))
+        return
+    if args.only_persistent_forms:
+        print(json.dumps({"persistent_forms": persistent_forms_leg(local)}))
         return
     if args.only_mlp:
         import mpsparse_b200 as mps
