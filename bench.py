@@ -979,8 +979,9 @@ def persistent_forms_leg(dev):
     log-normal diffusion systems (sigma 1.5, correlation 16, seed 5), plain
     CG on the Laplacian and BiCGSTAB on the Laplacian with each east
     coupling halved, both to the 1e-6 recurrence target.  512^2 runs in the
-    window form; 700^2 and up, whose rows of A and GᵀG no longer fit shared
-    memory, in the stream form (rows read from L2 in every step)."""
+    window form (and, for comparison, in each form: all three fit there);
+    700^2 and up, whose rows of A and GᵀG no longer fit shared memory, in the
+    stream form (rows read from L2 in every step)."""
     import torch
     import mpsparse_b200 as mps
     from mpsparse_b200.fsai import LearnedFsai
@@ -1022,8 +1023,15 @@ def persistent_forms_leg(dev):
         A.set_fsai_apply("product")
         b = torch.from_numpy(W.rhs(c.n, 8).astype(np.float64)).to(dev)
         x = torch.zeros(c.n, dtype=torch.float64, device=dev)
-        out.append({"solve": "learned FSAI MP-PCG", "grid": nx,
-                    **both(A, lambda x: A.cg_mixed(b, x, tol=1e-6, precond="fsai"), x)})
+        row = {"solve": "learned FSAI MP-PCG", "grid": nx,
+               **both(A, lambda x: A.cg_mixed(b, x, tol=1e-6, precond="fsai"), x)}
+        if nx == 512:   # every form fits here: the same solve in each
+            row["by_form"] = {}
+            for form in ("window", "gather", "stream"):
+                A.set_persistent(True, form=form)
+                row["by_form"][form] = time_solve(lambda x: A.cg_mixed(b, x, tol=1e-6, precond="fsai"), x)
+            A.set_persistent(True)
+        out.append(row)
         del A
     c = W.laplacian_2d(1024)
     x = torch.zeros(c.n, device=dev)

@@ -241,6 +241,14 @@ typedef struct {
  * counterpart. */
 mps_status mps_csr_set_persistent(mps_csr* A, int32_t enable);
 
+/* Which persistent form the solves above may use: 0 (default) the first
+ * that fits -- window, then gather, then stream; 1 gather, 2 window or
+ * 3 stream: only that one (the graph form runs when it does not fit).  The
+ * forms share the row partition and the per-row arithmetic, so where
+ * several fit they return bit-identical results; a choice other than 0 is
+ * for comparing them.  No reference counterpart. */
+mps_status mps_csr_set_persistent_form(mps_csr* A, int32_t form);
+
 mps_status mps_csr_cg_mixed(mps_csr* A, const double* d_b, double* d_x, const mps_ir_opts* opts,
                             mps_ir_info* info, cudaStream_t stream);
 

@@ -290,6 +290,16 @@ mps_status mps_csr_set_persistent(mps_csr* h, int32_t enable) {
     return MPS_OK;
 }
 
+mps_status mps_csr_set_persistent_form(mps_csr* h, int32_t form) {
+    if (!h) return fail(MPS_ERR_ARG, "null handle");
+    if (form < 0 || form > 3) return fail(MPS_ERR_ARG, "form must be 0 (auto), 1 (gather), 2 (window) or 3 (stream)");
+    if (form != h->persist_form) {
+        persist_plan_free_all(h);   // planned again, for the new choice, by the next solve
+        h->persist_form = form;
+    }
+    return MPS_OK;
+}
+
 mps_status mps_csr_destroy(mps_csr* h) {
     if (!h) return MPS_OK;
     csr_free(h->A);

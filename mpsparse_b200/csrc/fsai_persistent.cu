@@ -1120,7 +1120,7 @@ __global__ void persist_window_kernel(const int* __restrict__ a_rp, const int* _
 // shared-memory bytes; pp.state = -1 when a block would not fit or the
 // kernel cannot be made resident (the graph form runs then).
 static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const CsrMat& A, const CsrMat* M,
-                             cudaStream_t s) {
+                             int pick, cudaStream_t s) {
     pp.state = -1;
     int per_sm = 0;
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1187,14 +1187,17 @@ static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const C
         }
         return true;
     };
+    // pick: 0 the first form that fits (window, gather, stream); 1 + form:
+    // that form only
+    auto may = [&](int f) { return pick == 0 || pick == 1 + f; };
     size_t need;
-    if (resident(worst_win)) {
+    if (may(kWindowForm) && resident(worst_win)) {
         pp.form = kWindowForm;
         need = worst_win;
-    } else if (worst <= kPSmemBudget) {
+    } else if (may(kGatherForm) && worst <= kPSmemBudget) {
         pp.form = kGatherForm;
         need = worst;
-    } else if (resident(worst_stream)) {
+    } else if (may(kStreamForm) && resident(worst_stream)) {
         pp.form = kStreamForm;
         need = worst_stream;
     } else {
@@ -1210,7 +1213,7 @@ cudaError_t persist_plan_build(mps_csr* h, cudaStream_t s) {
     h->pp.state = -1;
     if (!h->use_m || !h->M.rp || h->A.n_rows != h->M.n_rows) return cudaSuccess;
     return plan_rows(h->pp, (int)h->A.n_rows, reinterpret_cast<const void*>(fsai_pcg_persistent<kGatherForm>),
-                     h->A, &h->M, s);
+                     h->A, &h->M, h->persist_form, s);
 }
 
 // Plan of the CG form (rows of A only).
@@ -1218,7 +1221,7 @@ cudaError_t persist_plan_build_a(mps_csr* h, cudaStream_t s) {
     h->pp_a.state = -1;
     if (h->A.n_rows != h->A.n_cols) return cudaSuccess;
     return plan_rows(h->pp_a, (int)h->A.n_rows, reinterpret_cast<const void*>(cg_persistent<false, kGatherForm>),
-                     h->A, nullptr, s);
+                     h->A, nullptr, h->persist_form, s);
 }
 
 // Plain CG / Jacobi-PCG as one cooperative launch: b is H.v(vB), x lands in

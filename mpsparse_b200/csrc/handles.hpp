@@ -59,6 +59,7 @@ struct mps_csr {
     mps::PersistPlan pp;       // persistent form of reliable-update FSAI-PCG (rows of A and M)
     mps::PersistPlan pp_a;     // persistent form of plain CG / Jacobi-PCG (rows of A)
     int32_t persistent = 1;    // 1: use the persistent form when the rows fit
+    int32_t persist_form = 0;  // 0: the first form that fits; 1 gather, 2 window, 3 stream: only that one
 };
 
 namespace mps {

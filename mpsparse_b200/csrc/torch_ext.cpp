@@ -327,7 +327,16 @@ public:
         d["persistent_form"] = persistent_form(info.persistent);
         return d;
     }
-    void set_persistent(bool enable) { check(mps_csr_set_persistent(h_, enable ? 1 : 0), "set_persistent"); }
+    void set_persistent(bool enable, const std::string& form) {
+        int f = -1;
+        if (form == "auto") f = 0;
+        else if (form == "gather") f = 1;
+        else if (form == "window") f = 2;
+        else if (form == "stream") f = 3;
+        if (f < 0) throw std::invalid_argument("form must be auto, gather, window or stream");
+        check(mps_csr_set_persistent(h_, enable ? 1 : 0), "set_persistent");
+        check(mps_csr_set_persistent_form(h_, f), "set_persistent");
+    }
 
     void set_fsai(torch::Tensor rp, torch::Tensor ci, torch::Tensor v) {
         c10::cuda::CUDAGuard g(device_);
@@ -750,8 +759,9 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         .def("attach_fsai", &CsrTensor::attach_fsai, py::arg("model"))
         .def("set_fsai_apply", &CsrTensor::set_fsai_apply, py::arg("mode"))
         .def("fsai_apply", &CsrTensor::fsai_apply)
-        .def("set_persistent", &CsrTensor::set_persistent, py::arg("enable"),
-             "reliable-update FSAI-PCG as one persistent kernel when the rows fit (default on)")
+        .def("set_persistent", &CsrTensor::set_persistent, py::arg("enable"), py::arg("form") = "auto",
+             "cgd / bicgstab / cg_mixed as one persistent kernel when a CTA per SM can hold its share "
+             "(default on); form: auto (window, else gather, else stream), or only gather / window / stream")
         .def("fsai_product", &CsrTensor::fsai_product)
         .def("fsai_train_step", &CsrTensor::fsai_train_step, py::arg("model"), py::arg("n_probes") = 4,
              py::arg("extra") = py::none(), py::arg("lr") = 1e-3, py::arg("seed") = 0)

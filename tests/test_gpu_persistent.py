@@ -106,6 +106,47 @@ def test_persistent_stream_form_fsai(mps, oracle):
     assert oracle.true_residual(Ao, b.cpu().numpy(), xp.cpu().numpy()) <= 1e-9 * 1.01
 
 
+def test_persistent_forms_bit_identical(mps):
+    """512^2 fits one CTA per SM in all three forms (window, gather,
+    stream).  They share the row partition, each row's arithmetic and the
+    order of every sum, so learned-FSAI MP-PCG, plain CG and BiCGSTAB return
+    bit-identical solutions and iteration counts in every form they run in;
+    BiCGSTAB has no gather form (the graph form runs), and an unknown form
+    is rejected."""
+    c, A = _learned(mps, 512, 512, 31)
+    b = torch.from_numpy(W.rhs(c.n, 8).astype(np.float64)).cuda()
+    forms = ("window", "gather", "stream")
+    out = {}
+    for form in forms:
+        A.set_persistent(True, form=form)
+        x = torch.zeros(c.n, dtype=torch.float64, device="cuda")
+        info = A.cg_mixed(b, x, tol=1e-9, inner_tol=1e-3, max_inner=40000, precond="fsai")
+        assert info["persistent_form"] == form and info["converged"], (form, info)
+        out[form] = (x, info["inner_iters"], info["outer_iters"])
+    for form in forms[1:]:
+        assert torch.equal(out[form][0], out["window"][0]), form
+        assert out[form][1:] == out["window"][1:], (form, out[form][1:], out["window"][1:])
+    # plain CG needs ~19,000 iterations on this system: 500 of each solver
+    b32 = b.float()
+    for solve, fs in (("cgd", forms), ("bicgstab", ("window", "stream"))):
+        xs = {}
+        for form in fs:
+            A.set_persistent(True, form=form)
+            x = torch.zeros(c.n, device="cuda")
+            info = getattr(A, solve)(b32, x, tol=1e-300, max_iter=500)
+            assert info["persistent_form"] == form and info["iters"] == 500, (solve, form, info)
+            xs[form] = x
+        for form in fs[1:]:
+            assert torch.equal(xs[form], xs["window"]), (solve, form)
+    A.set_persistent(True, form="gather")
+    x = torch.zeros(c.n, device="cuda")
+    info = A.bicgstab(b32, x, tol=1e-300, max_iter=20)
+    assert not info["persistent"] and info["iters"] == 20
+    with pytest.raises(ValueError):
+        A.set_persistent(True, form="tiled")
+    A.set_persistent(True)
+
+
 def test_rows_too_large_fall_back_to_graph_form(mps):
     """1600^2 (17,297 rows per CTA): not even the vector window and the own
     rows' vectors fit one CTA per SM, so the graph form runs."""
