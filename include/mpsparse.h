@@ -249,6 +249,16 @@ mps_status mps_csr_set_persistent(mps_csr* A, int32_t enable);
  * for comparing them.  No reference counterpart. */
 mps_status mps_csr_set_persistent_form(mps_csr* A, int32_t form);
 
+/* Test hook for the persistent kernels' bounded grid-barrier waits (no
+ * reference counterpart): runs at most 50 iterations of persistent CG on
+ * A with every barrier wait bounded by `spin_limit` polls and CTA
+ * `silent_cta` withholding its first arrival (-1: none), so that every
+ * CTA's first wait gives up.  Returns MPS_ERR_TIMEOUT (x is then
+ * meaningless); the device and the handle stay usable.  MPS_ERR_ARG when
+ * the persistent form does not fit A. */
+mps_status mps_test_persistent_barrier_timeout(mps_csr* A, const float* d_b, float* d_x, uint32_t spin_limit,
+                                               int32_t silent_cta, cudaStream_t stream);
+
 mps_status mps_csr_cg_mixed(mps_csr* A, const double* d_b, double* d_x, const mps_ir_opts* opts,
                             mps_ir_info* info, cudaStream_t stream);
 

@@ -551,6 +551,25 @@ mps_status mps_csr_cg(mps_csr* h, const float* b, float* x, const mps_solve_opts
     return csr_solve(kCG, h, b, x, o, info, s);
 }
 
+mps_status mps_test_persistent_barrier_timeout(mps_csr* h, const float* d_b, float* d_x, uint32_t spin_limit,
+                                               int32_t silent_cta, cudaStream_t s) {
+    if (!h || !d_b || !d_x || spin_limit == 0) return fail(MPS_ERR_ARG, "null argument or zero spin limit");
+    const int32_t keep = h->persistent;
+    h->persistent = 1;
+    h->test_spin_limit = spin_limit;
+    h->test_silent_cta = silent_cta;
+    mps_solve_opts o;
+    mps_solve_opts_default(&o);
+    o.max_iter = 50;
+    mps_solve_info info{};
+    mps_status st = csr_solve(kCG, h, d_b, d_x, &o, &info, s);
+    h->test_spin_limit = 0;
+    h->test_silent_cta = -1;
+    h->persistent = keep;
+    if (st == MPS_OK && !info.persistent) return fail(MPS_ERR_ARG, "the persistent form does not fit this matrix");
+    return st;
+}
+
 mps_status mps_csr_bicgstab(mps_csr* h, const float* b, float* x, const mps_solve_opts* o,
                             mps_solve_info* info, cudaStream_t s) {
     return csr_solve(kBiCG, h, b, x, o, info, s);

@@ -82,6 +82,8 @@ struct PersistDev {
     int n;
     const float* b32;       // CG form: FP32 right-hand side
     float* x32;             // CG form: FP32 solution
+    unsigned spin_limit;    // polls of one barrier wait before it gives up
+    int silent_cta;         // test hook: this CTA skips its first arrival (-1: none)
 };
 
 struct PersistShared {
@@ -132,8 +134,10 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
 //      one bar.sync hands both to the CTA.
 // Consecutive reductions must use different slots: a CTA may store its next
 // partials while a slower CTA still reads these.  The wait is bounded
-// (kGridSpinLimit polls, back-off after 64); a timeout raises the error word
-// and the abort word, and the abort word ends every other CTA's wait.
+// (P.spin_limit polls, back-off after 64); a timeout raises the error word
+// and the abort word, and the abort word ends every other CTA's wait.  (The
+// test hook P.silent_cta withholds one CTA's first arrival, so every wait of
+// that reduction runs out this way.)
 // false: this CTA gave up (timeout or abort).
 struct NoFin {
     __device__ void operator()(const double*) const {}
@@ -160,7 +164,7 @@ __device__ bool reduce_all(const PersistDev& P, PersistShared& sh, int slot, dou
         if (lane == 0) {
 #pragma unroll
             for (int j = 0; j < NS; ++j) P.part[(slot * 3 + j) * G + blockIdx.x] = bt[j];
-            red_release_add(P.bar + kCountWord, 1u);
+            if (P.silent_cta != (int)blockIdx.x || sh.gen != 0) red_release_add(P.bar + kCountWord, 1u);
         }
         __syncwarp();
         int ok = 1;
@@ -170,7 +174,7 @@ __device__ bool reduce_all(const PersistDev& P, PersistShared& sh, int slot, dou
                 ok = 0;
                 break;
             }
-            if (++spins > kGridSpinLimit) {
+            if (++spins > P.spin_limit) {
                 if (lane == 0) {
                     atomicOr(P.err, kErrTimeout);
                     atomicExch(P.bar + kAbortWord, 1u);
@@ -1252,6 +1256,8 @@ cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s, const double* b64, doub
     P.sc_out = H.ws.sc;
     P.prm = H.ws.d_params;
     P.n = (int)h->A.n_rows;
+    P.spin_limit = h->test_spin_limit ? h->test_spin_limit : kGridSpinLimit;
+    P.silent_cta = h->test_silent_cta;
     P.b32 = H.v(vB);
     P.x32 = H.v(vX);
     P.b = b64;
@@ -1303,6 +1309,8 @@ cudaError_t persist_bicg_solve(mps_csr* h, cudaStream_t s) {
     P.sc_out = H.ws.sc;
     P.prm = H.ws.d_params;
     P.n = (int)h->A.n_rows;
+    P.spin_limit = h->test_spin_limit ? h->test_spin_limit : kGridSpinLimit;
+    P.silent_cta = h->test_silent_cta;
     P.b32 = H.v(vB);
     P.x32 = H.v(vX);
     const void* k = h->pp_a.form == kStreamForm ? reinterpret_cast<const void*>(bicg_persistent<kStreamForm>)
@@ -1360,6 +1368,8 @@ cudaError_t persist_solve(mps_csr* h, const double* b64, double* x64, cudaStream
     P.sc_out = H.ws.sc;
     P.prm = H.ws.d_params;
     P.n = (int)h->A.n_rows;
+    P.spin_limit = h->test_spin_limit ? h->test_spin_limit : kGridSpinLimit;
+    P.silent_cta = h->test_silent_cta;
     static_assert(4 * 3 * 1024 <= 4 * kMaxPartials, "partial slots");
     P.win = h->pp.d_row_start + h->pp.grid + 1 + kBarWords;
     const int f = h->pp.form;

@@ -60,6 +60,9 @@ struct mps_csr {
     mps::PersistPlan pp_a;     // persistent form of plain CG / Jacobi-PCG (rows of A)
     int32_t persistent = 1;    // 1: use the persistent form when the rows fit
     int32_t persist_form = 0;  // 0: the first form that fits; 1 gather, 2 window, 3 stream: only that one
+    // test hook of the persistent kernels' grid barrier (mps_test_persistent_barrier_timeout)
+    uint32_t test_spin_limit = 0;   // 0: the default bound on one barrier wait
+    int32_t test_silent_cta = -1;   // >= 0: that CTA skips its first arrival
 };
 
 namespace mps {

@@ -471,3 +471,45 @@ def test_persistent_bicgstab_stream_form(mps, oracle):
         assert_solved_fp32(oracle, Ao, b, x.cpu().numpy(), 1e-6, info)
         infos.append(info)
     assert abs(infos[0]["iters"] - infos[1]["iters"]) <= 0.02 * infos[1]["iters"] + 2, infos
+
+
+def test_persistent_barrier_timeout_returns_error_and_handle_stays_usable(mps, oracle):
+    """A bounded grid-barrier wait that runs out: the test hook makes CTA 3
+    withhold its first arrival, so every CTA's first wait (bounded at
+    20,000 polls, milliseconds) gives up and raises the abort word, and the
+    kernel ends.  The call returns MPS_ERR_TIMEOUT; afterwards the same
+    handle solves to the oracle's iterates, and the hook with no silent CTA
+    is an ordinary 50-iteration solve."""
+    import ctypes as C
+    from tests import cabi
+    L = cabi.lib()
+    f = L.mps_test_persistent_barrier_timeout
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p]
+    f.restype = C.c_int
+    c = W.laplacian_2d(128)
+    keys = torch.from_numpy(c.keys()).cuda()
+    vals = torch.from_numpy(c.vals).cuda()
+    h = C.c_void_p()
+    cabi.check(L.mps_csr_create_from_keys(cabi.ptr(keys), cabi.ptr(vals), c.nnz, c.n, c.n, C.byref(h), None))
+    b = torch.from_numpy(W.rhs(c.n, 3)).cuda()
+    x = torch.zeros(c.n, device="cuda")
+    try:
+        for _ in range(2):
+            st = f(h, cabi.ptr(b), cabi.ptr(x), 20000, 3, None)
+            assert st == 4, (st, L.mps_last_error_string())           # MPS_ERR_TIMEOUT
+            msg = L.mps_last_error_string()
+            assert b"watchdog" in msg or b"bounded device wait" in msg, msg
+        torch.cuda.synchronize()
+        assert f(h, cabi.ptr(b), cabi.ptr(x), 20000, -1, None) == 0
+        o = cabi.SolveOpts()
+        L.mps_solve_opts_default(C.byref(o))
+        o.tol, o.max_iter = 1e-300, 20
+        info = cabi.SolveInfo()
+        x.zero_()
+        cabi.check(L.mps_csr_cg(h, cabi.ptr(b), cabi.ptr(x), C.byref(o), C.byref(info), None))
+        assert info.persistent and info.iters == 20
+        Ao = oracle.Csr(*c.to_csr(), c.n)
+        xo, _ = oracle.cg(Ao, b.cpu().numpy(), tol=0.0, max_iter=20)
+        assert np.linalg.norm(x.cpu().numpy() - xo) / np.linalg.norm(xo) <= 1e-5
+    finally:
+        L.mps_csr_destroy(h)
