@@ -15,7 +15,7 @@ Also measured in the same run (reported, not the headline):
   * cpu_baseline: the CPU oracle's CG on the box's host cores (bounded sample)
     and scipy.sparse.linalg.cg beside it.
 
-  * configs: the other configurations at full size, every answer judged by
+  * configs: the other configurations at full size, every answer checked by
     its FP64 true residual -- C1 CG on the 256^2 Laplacian (iterations
     against the FP64 oracle, scipy cg on the host), C2 BiCGSTAB on the BCSR
     4x4 system with 65,536 block rows (BCSR SpMV GB/s, scipy bicgstab), C3
@@ -872,7 +872,7 @@ def c2_leg(dev, flush):
 def c3_leg(args, dev, ctx):
     """C3: mixed-precision CG with FP64 refinement to 1e-10 (FP32 values,
     reliable updates; BF16 values, restarted refinement) and plain FP32 CG to
-    1e-6 on the 256^3 operator, each judged by its FP64 true residual; the
+    1e-6 on the 256^3 operator, each checked by its FP64 true residual; the
     error against the FP64 oracle's solution on the 64^3 member of the same
     family (sigma 1, correlation 8), where the oracle runs in seconds."""
     import torch

@@ -13,7 +13,7 @@ def fp32_floor(oracle, A, b, x, factor=16.0):
 
 
 def assert_solved_fp32(oracle, A, b, x, tol, info=None, floor_factor=16.0):
-    """Final FP32 answer judged by the FP64 true residual: below 2*tol, or at
+    """Final FP32 answer checked by the FP64 true residual: below 2*tol, or at
     the FP32 rounding floor when that floor is above it.  With the solver's
     info dict: its true_resid (recomputed on the GPU in FP64) equals the
     oracle's FP64 true residual of the same x, and `converged` says exactly

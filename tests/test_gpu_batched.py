@@ -3,7 +3,7 @@ the FP64 oracle, system by system.
 
 Tolerances: iterates after k steps within 1e-5 relative (2-norm) of the
 oracle's FP64 PCG (FP32 arithmetic, FP64 reductions); converged answers
-judged by each system's FP64 true residual (below 2*tol, or at the FP32
+checked by each system's FP64 true residual (below 2*tol, or at the FP32
 rounding floor when that is higher); iteration counts within 10% + 3 of the
 oracle's FP64 count (FP32 Krylov vectors lose orthogonality sooner than FP64
 ones on the ill-conditioned log-normal systems, so counts drift apart after

@@ -1,4 +1,4 @@
-"""The named configurations at full size, every answer judged by its FP64
+"""The named configurations at full size, every answer checked by its FP64
 true residual (computed by the FP64 oracle on the stored FP32 values).
 
 * C2: BiCGSTAB on the BCSR 4x4 system with 65,536 block rows (n 262,144),

@@ -2,7 +2,7 @@
 
 Tolerance (from the solver contract): each of the first 20 FP32 iterates is
 within 1e-5 relative (2-norm) of the FP64 transcription; final answers are
-judged by the FP64 true residual ||b - A x|| / ||b||."""
+checked by the FP64 true residual ||b - A x|| / ||b||."""
 import numpy as np
 import pytest
 import torch
