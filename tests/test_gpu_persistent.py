@@ -147,6 +147,43 @@ def test_persistent_forms_bit_identical(mps):
     A.set_persistent(True)
 
 
+@pytest.mark.parametrize("case", ["one_cta", "isolated_nodes"])
+def test_persistent_forms_bit_identical_edge_cases(mps, case):
+    """Forced forms on a one-CTA system (10x10 Laplacian: 100 rows, a grid of
+    one CTA) and on a random graph with isolated nodes (5,000 rows, mean
+    degree 1.5: rows of 1 to about 10 nonzeros, windows spanning the
+    matrix): plain CG and BiCGSTAB over 30 iterations, and learned-FSAI
+    MP-PCG to 1e-8, return bit-identical results in every form."""
+    c = W.laplacian_2d(10) if case == "one_cta" else W.graph_laplacian(5000, 1.5, 4, shift=0.05)
+    A = _cg_system(mps, c)
+    b = torch.from_numpy(W.rhs(c.n, 2)).cuda()
+    forms = ("window", "gather", "stream")
+    for solve, fs in (("cgd", forms), ("bicgstab", ("window", "stream"))):
+        xs = {}
+        for form in fs:
+            A.set_persistent(True, form=form)
+            x = torch.zeros(c.n, device="cuda")
+            info = getattr(A, solve)(b, x, tol=1e-300, max_iter=30)
+            assert info["persistent_form"] == form, (solve, form, info)
+            xs[form] = (x, info["iters"])
+        for form in fs[1:]:
+            assert torch.equal(xs[form][0], xs["window"][0]) and xs[form][1] == xs["window"][1], (solve, form)
+    from mpsparse_b200.fsai import LearnedFsai
+    LearnedFsai.load().attach(A)
+    A.set_fsai_apply("product")
+    b64 = b.double()
+    out = {}
+    for form in forms:
+        A.set_persistent(True, form=form)
+        x = torch.zeros(c.n, dtype=torch.float64, device="cuda")
+        info = A.cg_mixed(b64, x, tol=1e-8, inner_tol=1e-3, max_inner=20000, precond="fsai")
+        assert info["persistent_form"] == form and info["converged"], (form, info)
+        out[form] = (x, info["inner_iters"])
+    for form in forms[1:]:
+        assert torch.equal(out[form][0], out["window"][0]) and out[form][1] == out["window"][1], form
+    A.set_persistent(True)
+
+
 def test_rows_too_large_fall_back_to_graph_form(mps):
     """1600^2 (17,297 rows per CTA): not even the vector window and the own
     rows' vectors fit one CTA per SM, so the graph form runs."""
