@@ -82,6 +82,8 @@ struct PersistDev {
     int n;
     const float* b32;       // CG form: FP32 right-hand side
     float* x32;             // CG form: FP32 solution
+    const unsigned short* a_c16;   // stream form: A's / M's columns, 16-bit, relative to
+    const unsigned short* m_c16;   // the column window of the CTA that owns the row
     unsigned spin_limit;    // polls of one barrier wait before it gives up
     int silent_cta;         // test hook: this CTA skips its first arrival (-1: none)
 };
@@ -317,15 +319,14 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
     // WIN: the multiplied vector over the CTA's column window, staged once
     // per step (coalesced loads) so the row sums read shared memory only
     // for the vector; the own rows' x (FP64, written through to global) and
-    // D^-1 stay in shared memory too.  Rows of A and M: in shared memory
-    // (window form: columns 16-bit, relative to the window), or (stream form)
-    // read from global memory in every step.
+    // D^-1 stay in shared memory too.  Rows of A and M: in shared memory, or
+    // (stream form) read from global memory in every step; in both WIN forms
+    // columns are 16-bit, relative to the window.
     // shared layout: [arp[R+1] | mrp[R+1] | aci[na] | mci[nm] | pad | av[na] |
     //                mv[nm] | pad] | (WIN: xs[R] | ds[R] | win[hi - lo])
-    using CI = ColIdx<FORM == kWindowForm>;
+    using CI = ColIdx<WIN>;
     const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
-    const int coff = FORM == kWindowForm ? wlo : 0;   // global column = coff + stored index
-    const int wbase = STREAM ? wlo : 0;                // window slot = stored index - wbase
+    const int coff = wlo;   // global column = coff + stored index (wlo = 0 in the gather form)
     const int* arp;
     const int* mrp;
     const CI* aci;
@@ -336,8 +337,8 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
     if constexpr (STREAM) {   // absolute row offsets into the global arrays
         arp = P.a_rp + r0;
         mrp = P.m_rp + r0;
-        aci = P.a_ci;
-        mci = P.m_ci;
+        aci = P.a_c16;
+        mci = P.m_c16;
         av = P.a_v;
         mv = P.m_v;
     } else {
@@ -371,7 +372,7 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
     double* xs = reinterpret_cast<double*>(psmem + off_own);
     float* ds = reinterpret_cast<float*>(xs + (WIN ? R : 0));
     float* win = ds + (WIN ? R : 0);
-    auto wg = [&](int c) { return win[c - wbase]; };
+    auto wg = [&](int c) { return win[c]; };
     if constexpr (WIN) {
         for (int li = tid; li < R; li += kPNT) {
             xs[li] = 0.0;
@@ -621,20 +622,19 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
     // the stream form, whose rows are read from global memory); the window
     // and stream forms add the own rows' x (FP64 under IR, written through
     // to global), r (written through), q and D^-1, then the vector window
-    // (window form: columns 16-bit, relative to the window):
+    // (columns 16-bit, relative to the window, in both forms):
     //   ... | xs[R] | rs[R] | qs[R] | ds[R] | win[hi - lo]
     using XT = std::conditional_t<IR, double, float>;
-    using CI = ColIdx<FORM == kWindowForm>;
+    using CI = ColIdx<WIN>;   // WIN forms: 16-bit columns relative to the window
     const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
-    const int coff = FORM == kWindowForm ? wlo : 0;   // global column = coff + stored index
-    const int wbase = STREAM ? wlo : 0;                // window slot = stored index - wbase
+    const int coff = wlo;   // global column = coff + stored index (wlo = 0 in the gather form)
     const int* arp;
     const CI* aci;
     const float* av;
     size_t off_own = 0;
     if constexpr (STREAM) {   // absolute row offsets into the global arrays
         arp = P.a_rp + r0;
-        aci = P.a_ci;
+        aci = P.a_c16;
         av = P.a_v;
     } else {
         int* arp_s = reinterpret_cast<int*>(psmem);
@@ -656,7 +656,7 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
     float* qs = rs + (WIN ? R : 0);
     float* ds = qs + (WIN ? R : 0);
     float* win = ds + (WIN ? R : 0);
-    auto wg = [&](int c) { return win[c - wbase]; };
+    auto wg = [&](int c) { return win[c]; };
     if (tid == 0) {
         sh.gen = 0;
         sh.ok = 1;
@@ -871,22 +871,21 @@ __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
     const int r0 = P.row_start[blockIdx.x], r1 = P.row_start[blockIdx.x + 1];
     const int R = r1 - r0;
     const int a0 = P.a_rp[r0], na = P.a_rp[r1] - a0;
-    // shared layout: [arp[R+1] | aci[na] | pad | av[na] | pad to 8] (window
-    // form: columns 16-bit, window-relative; the stream form reads its rows
-    // from global memory) | xs[R] | ts[R] | win[hi - lo]
+    // shared layout: [arp[R+1] | aci[na] | pad | av[na] | pad to 8] (the
+    // stream form reads its rows from global memory; columns 16-bit,
+    // window-relative in both forms) | xs[R] | ts[R] | win[hi - lo]
     static_assert(FORM == kWindowForm || FORM == kStreamForm, "BiCGSTAB: window or stream form");
     constexpr bool STREAM = FORM == kStreamForm;
-    using CI = ColIdx<!STREAM>;
+    using CI = ColIdx<true>;
     const int wlo = P.win[2 * blockIdx.x], whi = P.win[2 * blockIdx.x + 1];
-    const int coff = STREAM ? 0 : wlo;   // global column = coff + stored index
-    const int wbase = STREAM ? wlo : 0;  // window slot = stored index - wbase
+    const int coff = wlo;   // global column = coff + stored index
     const int* arp;
     const CI* aci;
     const float* av;
     size_t off_own = 0;
     if constexpr (STREAM) {   // absolute row offsets into the global arrays
         arp = P.a_rp + r0;
-        aci = P.a_ci;
+        aci = P.a_c16;
         av = P.a_v;
     } else {
         int* arp_s = reinterpret_cast<int*>(psmem);
@@ -906,7 +905,7 @@ __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
     float* xs = reinterpret_cast<float*>(psmem + off_own);
     float* ts = xs + R;
     float* win = ts + R;
-    auto wg = [&](int c) { return win[c - wbase]; };
+    auto wg = [&](int c) { return win[c]; };
     if (tid == 0) {
         sh.gen = 0;
         sh.ok = 1;
@@ -1117,6 +1116,17 @@ __global__ void persist_window_kernel(const int* __restrict__ a_rp, const int* _
     }
 }
 
+// Stream form: every nonzero's column relative to the column window of the
+// CTA that owns its row (CTA b = block b; windows of at most 65,536 columns).
+__global__ void persist_c16_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
+                                   const int* __restrict__ row_start, const int* __restrict__ win,
+                                   unsigned short* __restrict__ out) {
+    const int b = blockIdx.x;
+    const int lo = win[2 * b];
+    const int e = rp[row_start[b + 1]];
+    for (int k = rp[row_start[b]] + (int)threadIdx.x; k < e; k += blockDim.x) out[k] = (unsigned short)(ci[k] - lo);
+}
+
 }  // namespace
 
 // Row blocks for one CTA per SM over A's rows (and M's when given), split
@@ -1140,6 +1150,8 @@ static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const C
     const int grid = std::min(num_sms(), std::max(1, n / 128));
     dev_free(pp.d_row_start);
     pp.d_row_start = nullptr;
+    dev_free(pp.d_c16);
+    pp.d_c16 = nullptr;
     // grid + 1 boundaries, the barrier words, 2 window bounds per block, then
     // 2 nonzero counts per block (read back here only)
     const size_t words_all = (size_t)grid + 1 + kBarWords + 4 * (size_t)grid;
@@ -1174,7 +1186,8 @@ static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const C
                           (M ? 12 : 20) * (size_t)rows;   // FSAI: x, D^-1; CG: x, r, q, D^-1
         worst_win = std::max(worst_win, w > 65536 ? ~(size_t)0 : bw);
         // stream form: the vector window and the own rows' vectors only
-        worst_stream = std::max(worst_stream, 4 * w + (M ? 12 : 20) * (size_t)rows);
+        // (columns stored 16-bit relative to the window)
+        worst_stream = std::max(worst_stream, w > 65536 ? ~(size_t)0 : 4 * w + (M ? 12 : 20) * (size_t)rows);
     }
     pp.grid = grid;
     // a footprint above the gather budget must still leave one CTA
@@ -1204,6 +1217,21 @@ static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const C
     } else if (may(kStreamForm) && resident(worst_stream)) {
         pp.form = kStreamForm;
         need = worst_stream;
+        // the rows' columns relative to their CTA's window, 16-bit, in
+        // global memory (built once per pattern; values are read from the
+        // matrix itself)
+        const size_t nz = (size_t)A.nnz + (M ? (size_t)M->nnz : 0);
+        e = dev_alloc(&pp.d_c16, 2 * nz, s);
+        if (e != cudaSuccess) {   // no room: the graph form runs
+            cudaGetLastError();
+            pp.d_c16 = nullptr;
+            return cudaSuccess;
+        }
+        const int* d_win = pp.d_row_start + grid + 1 + kBarWords;
+        persist_c16_kernel<<<grid, 256, 0, s>>>(A.rp, A.ci, pp.d_row_start, d_win, pp.d_c16);
+        if (M) persist_c16_kernel<<<grid, 256, 0, s>>>(M->rp, M->ci, pp.d_row_start, d_win, pp.d_c16 + A.nnz);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
     } else {
         return cudaSuccess;   // not eligible: the graph form runs
     }
@@ -1263,6 +1291,7 @@ cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s, const double* b64, doub
     P.b = b64;
     P.x = x64;
     P.win = h->pp_a.d_row_start + h->pp_a.grid + 1 + kBarWords;
+    P.a_c16 = h->pp_a.d_c16;
     const int f = h->pp_a.form;
     const void* k;
     if (b64)
@@ -1313,6 +1342,7 @@ cudaError_t persist_bicg_solve(mps_csr* h, cudaStream_t s) {
     P.silent_cta = h->test_silent_cta;
     P.b32 = H.v(vB);
     P.x32 = H.v(vX);
+    P.a_c16 = h->pp_a.d_c16;
     const void* k = h->pp_a.form == kStreamForm ? reinterpret_cast<const void*>(bicg_persistent<kStreamForm>)
                                                 : reinterpret_cast<const void*>(bicg_persistent<kWindowForm>);
     cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
@@ -1325,12 +1355,14 @@ cudaError_t persist_bicg_solve(mps_csr* h, cudaStream_t s) {
 
 void persist_plan_free(mps_csr* h) {
     dev_free(h->pp.d_row_start);
+    dev_free(h->pp.d_c16);
     h->pp = PersistPlan{};
 }
 
 void persist_plan_free_all(mps_csr* h) {
     persist_plan_free(h);
     dev_free(h->pp_a.d_row_start);
+    dev_free(h->pp_a.d_c16);
     h->pp_a = PersistPlan{};
 }
 
@@ -1372,6 +1404,8 @@ cudaError_t persist_solve(mps_csr* h, const double* b64, double* x64, cudaStream
     P.silent_cta = h->test_silent_cta;
     static_assert(4 * 3 * 1024 <= 4 * kMaxPartials, "partial slots");
     P.win = h->pp.d_row_start + h->pp.grid + 1 + kBarWords;
+    P.a_c16 = h->pp.d_c16;
+    P.m_c16 = h->pp.d_c16 ? h->pp.d_c16 + h->A.nnz : nullptr;
     const int f = h->pp.form;
     const void* k = f == kWindowForm   ? reinterpret_cast<const void*>(fsai_pcg_persistent<kWindowForm>)
                     : f == kStreamForm ? reinterpret_cast<const void*>(fsai_pcg_persistent<kStreamForm>)

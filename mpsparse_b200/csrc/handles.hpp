@@ -40,6 +40,7 @@ struct PersistPlan {
     size_t smem = 0;               // dynamic shared memory per CTA
     int form = 0;                  // 0 gather, 1 window (16-bit window-relative columns), 2 stream
     int* d_row_start = nullptr;    // grid + 1 row boundaries, the barrier's words, the windows
+    unsigned short* d_c16 = nullptr;  // stream form: A's then M's columns relative to their CTA's window
 };
 
 }  // namespace mps
