@@ -263,14 +263,15 @@ __device__ __forceinline__ T ldm(const T* p) {
     else return *p;
 }
 
-// Row li of a block of a CSR (in shared memory, or G: in global memory)
-// times a gathered vector: the products rounded to FP32 first, then added in
-// column order (the tile kernels' arithmetic).
+// Row li of a block of a CSR (row pointers in shared memory; columns and
+// values in shared memory, or G: in global memory) times a gathered vector:
+// the products rounded to FP32 first, then added in column order (the tile
+// kernels' arithmetic).
 template <bool G = false, class IT, class F>
 __device__ __forceinline__ float row_f32(const int* rp, const IT* ci, const float* v, int li, F gather) {
     float s = 0.f;
-    const int e = ldm<G>(rp + li + 1);
-    for (int k = ldm<G>(rp + li); k < e; ++k) s = __fadd_rn(s, __fmul_rn(ldm<G>(v + k), gather((int)ldm<G>(ci + k))));
+    const int e = rp[li + 1];
+    for (int k = rp[li]; k < e; ++k) s = __fadd_rn(s, __fmul_rn(ldm<G>(v + k), gather((int)ldm<G>(ci + k))));
     return s;
 }
 
@@ -281,8 +282,8 @@ __device__ __forceinline__ float row_f32(const int* rp, const IT* ci, const floa
 template <bool G = false, class IT, class F>
 __device__ __forceinline__ void row_pair_f32(const int* rp, const IT* ci, const float* v, int li0,
                                              int li1, bool has1, F gather, float& s0, float& s1) {
-    const int b0 = ldm<G>(rp + li0), e0 = ldm<G>(rp + li0 + 1);
-    const int b1 = has1 ? ldm<G>(rp + li1) : 0, e1 = has1 ? ldm<G>(rp + li1 + 1) : 0;
+    const int b0 = rp[li0], e0 = rp[li0 + 1];
+    const int b1 = has1 ? rp[li1] : 0, e1 = has1 ? rp[li1 + 1] : 0;
     s0 = 0.f;
     s1 = 0.f;
     const int len = max(e0 - b0, e1 - b1);
@@ -320,9 +321,10 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
     // per step (coalesced loads) so the row sums read shared memory only
     // for the vector; the own rows' x (FP64, written through to global) and
     // D^-1 stay in shared memory too.  Rows of A and M: in shared memory, or
-    // (stream form) read from global memory in every step; in both WIN forms
-    // columns are 16-bit, relative to the window.
-    // shared layout: [arp[R+1] | mrp[R+1] | aci[na] | mci[nm] | pad | av[na] |
+    // (stream form) only their row pointers, the columns and values read from
+    // global memory in every step; in both WIN forms columns are 16-bit,
+    // relative to the window.
+    // shared layout: arp[R+1] | mrp[R+1] | [aci[na] | mci[nm] | pad | av[na] |
     //                mv[nm] | pad] | (WIN: xs[R] | ds[R] | win[hi - lo])
     using CI = ColIdx<WIN>;
     const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
@@ -334,9 +336,18 @@ __global__ void __launch_bounds__(kPNT, 1) fsai_pcg_persistent(PersistDev P) {
     const float* av;
     const float* mv;
     size_t off_own = 0;
-    if constexpr (STREAM) {   // absolute row offsets into the global arrays
-        arp = P.a_rp + r0;
-        mrp = P.m_rp + r0;
+    if constexpr (STREAM) {
+        // row pointers in shared memory (absolute offsets into the global
+        // columns and values, so a row's loads need no dependent global load)
+        int* arp_s = reinterpret_cast<int*>(psmem);
+        int* mrp_s = arp_s + (R + 1);
+        for (int i = tid; i <= R; i += kPNT) {
+            arp_s[i] = P.a_rp[r0 + i];
+            mrp_s[i] = P.m_rp[r0 + i];
+        }
+        off_own = round_up(8 * (size_t)(R + 1), 8);
+        arp = arp_s;
+        mrp = mrp_s;
         aci = P.a_c16;
         mci = P.m_c16;
         av = P.a_v;
@@ -618,9 +629,9 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
     const int r0 = P.row_start[blockIdx.x], r1 = P.row_start[blockIdx.x + 1];
     const int R = r1 - r0;
     const int a0 = P.a_rp[r0], na = P.a_rp[r1] - a0;
-    // shared layout: [arp[R+1] | aci[na] | pad | av[na] | pad to 8] (not in
-    // the stream form, whose rows are read from global memory); the window
-    // and stream forms add the own rows' x (FP64 under IR, written through
+    // shared layout: arp[R+1] | [aci[na] | pad | av[na]] | pad to 8 (the
+    // bracket not in the stream form, whose columns and values are read from
+    // global memory); the window and stream forms add the own rows' x (FP64 under IR, written through
     // to global), r (written through), q and D^-1, then the vector window
     // (columns 16-bit, relative to the window, in both forms):
     //   ... | xs[R] | rs[R] | qs[R] | ds[R] | win[hi - lo]
@@ -632,8 +643,13 @@ __global__ void __launch_bounds__(kPNT, 1) cg_persistent(PersistDev P) {
     const CI* aci;
     const float* av;
     size_t off_own = 0;
-    if constexpr (STREAM) {   // absolute row offsets into the global arrays
-        arp = P.a_rp + r0;
+    if constexpr (STREAM) {
+        // row pointers in shared memory (absolute offsets into the global
+        // columns and values)
+        int* arp_s = reinterpret_cast<int*>(psmem);
+        for (int i = tid; i <= R; i += kPNT) arp_s[i] = P.a_rp[r0 + i];
+        off_own = round_up(4 * (size_t)(R + 1), 8);
+        arp = arp_s;
         aci = P.a_c16;
         av = P.a_v;
     } else {
@@ -871,9 +887,9 @@ __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
     const int r0 = P.row_start[blockIdx.x], r1 = P.row_start[blockIdx.x + 1];
     const int R = r1 - r0;
     const int a0 = P.a_rp[r0], na = P.a_rp[r1] - a0;
-    // shared layout: [arp[R+1] | aci[na] | pad | av[na] | pad to 8] (the
-    // stream form reads its rows from global memory; columns 16-bit,
-    // window-relative in both forms) | xs[R] | ts[R] | win[hi - lo]
+    // shared layout: arp[R+1] | [aci[na] | pad | av[na]] | pad to 8 (the
+    // stream form reads its columns and values from global memory; columns
+    // 16-bit, window-relative in both forms) | xs[R] | ts[R] | win[hi - lo]
     static_assert(FORM == kWindowForm || FORM == kStreamForm, "BiCGSTAB: window or stream form");
     constexpr bool STREAM = FORM == kStreamForm;
     using CI = ColIdx<true>;
@@ -883,8 +899,13 @@ __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
     const CI* aci;
     const float* av;
     size_t off_own = 0;
-    if constexpr (STREAM) {   // absolute row offsets into the global arrays
-        arp = P.a_rp + r0;
+    if constexpr (STREAM) {
+        // row pointers in shared memory (absolute offsets into the global
+        // columns and values)
+        int* arp_s = reinterpret_cast<int*>(psmem);
+        for (int i = tid; i <= R; i += kPNT) arp_s[i] = P.a_rp[r0 + i];
+        off_own = round_up(4 * (size_t)(R + 1), 8);
+        arp = arp_s;
         aci = P.a_c16;
         av = P.a_v;
     } else {
@@ -1185,9 +1206,11 @@ static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const C
         const size_t bw = 4 * (size_t)words * ((size_t)rows + 1) + 6 * nz + 12 + 4 * w +
                           (M ? 12 : 20) * (size_t)rows;   // FSAI: x, D^-1; CG: x, r, q, D^-1
         worst_win = std::max(worst_win, w > 65536 ? ~(size_t)0 : bw);
-        // stream form: the vector window and the own rows' vectors only
-        // (columns stored 16-bit relative to the window)
-        worst_stream = std::max(worst_stream, w > 65536 ? ~(size_t)0 : 4 * w + (M ? 12 : 20) * (size_t)rows);
+        // stream form: the row pointers, the vector window and the own rows'
+        // vectors (columns stored 16-bit relative to the window, in global
+        // memory with the values); 4 bytes of alignment padding
+        const size_t bs = 4 * (size_t)words * ((size_t)rows + 1) + 4 + 4 * w + (M ? 12 : 20) * (size_t)rows;
+        worst_stream = std::max(worst_stream, w > 65536 ? ~(size_t)0 : bs);
     }
     pp.grid = grid;
     // a footprint above the gather budget must still leave one CTA
