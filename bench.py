@@ -981,7 +981,9 @@ def persistent_forms_leg(dev):
     coupling halved, both to the 1e-6 recurrence target.  512^2 runs in the
     window form (and, for comparison, in each form: all three fit there);
     700^2 and up, whose rows of A and GᵀG no longer fit shared memory, in the
-    stream form (rows read from L2 in every step)."""
+    stream form (rows read from L2 in every step); plain CG and BiCGSTAB on a
+    random graph Laplacian (60,000 rows, mean degree 6, + 0.05 I) in the
+    gather form."""
     import torch
     import mpsparse_b200 as mps
     from mpsparse_b200.fsai import LearnedFsai
@@ -1045,6 +1047,15 @@ def persistent_forms_leg(dev):
                             c.n, c.n, fill_outputs=False)
     out.append({"solve": "bicgstab", "grid": 1024,
                 **both(A, lambda x: A.bicgstab(b, x, tol=1e-6, max_iter=40000), x)})
+    # an unstructured matrix: windows span the matrix, so the gather form
+    c = W.graph_laplacian(60000, 6.0, 3, shift=0.05)
+    x = torch.zeros(c.n, device=dev)
+    b = torch.from_numpy(W.rhs(c.n, 7)).to(dev)
+    A = mps.spmv.csr_tensor(torch.from_numpy(c.keys()), torch.from_numpy(c.vals), e, e, e,
+                            c.n, c.n, fill_outputs=False)
+    for solve in ("cgd", "bicgstab"):
+        out.append({"solve": solve, "grid": "random graph, 60,000 rows, mean degree 6",
+                    **both(A, lambda x: getattr(A, solve)(b, x, tol=1e-6, max_iter=40000), x)})
     return out
 
 

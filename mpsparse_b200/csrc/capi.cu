@@ -488,8 +488,8 @@ static mps_status solve_errors(mps_csr* h, const unsigned* e2, mps_status st, cu
 
 // Plain CG / Jacobi-PCG, or BiCGSTAB, as one persistent cooperative kernel
 // when A's rows (or, in the stream form, their vector windows) fit one CTA
-// per SM (fsai_persistent.cu; BiCGSTAB in the window and stream forms only);
-// *ran = false: not eligible, the graph form runs instead.  Same parameters,
+// per SM (fsai_persistent.cu); *ran = false: not eligible, the graph form
+// runs instead.  Same parameters,
 // result places and report as run_solve.
 static mps_status csr_persistent(SolverKind kind, mps_csr* h, const float* b, float* x,
                                  const mps_solve_opts& o, mps_solve_info* info, cudaStream_t s, bool* ran) {

@@ -875,9 +875,9 @@ out:
 // (bicg_stop_beta).  p and v are double-buffered by iteration parity: a CTA
 // writes its rows of the new ones while slower CTAs still gather the old.
 // s and t are never written to global memory: every CTA forms s over its
-// own window, and keeps its rows of t in shared memory.
-// Window or stream form (the plan's budget for them covers the own rows' x
-// and t kept here).  Buffers: P.r0 = r, P.r1 = r0 (the shadow residual),
+// own window (gather form: per gathered nonzero), and keeps its rows of t in
+// shared memory.  All three forms (the launch adds the own rows' x and t to
+// the gather form's footprint).  Buffers: P.r0 = r, P.r1 = r0 (the shadow residual),
 // P.p0 / P.p1 = p, P.q / P.z = v, P.b32 = b, P.x32 = x.
 template <int FORM>
 __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
@@ -889,12 +889,13 @@ __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
     const int a0 = P.a_rp[r0], na = P.a_rp[r1] - a0;
     // shared layout: arp[R+1] | [aci[na] | pad | av[na]] | pad to 8 (the
     // stream form reads its columns and values from global memory; columns
-    // 16-bit, window-relative in both forms) | xs[R] | ts[R] | win[hi - lo]
-    static_assert(FORM == kWindowForm || FORM == kStreamForm, "BiCGSTAB: window or stream form");
+    // 16-bit, window-relative in the window and stream forms) | xs[R] | ts[R]
+    // | (WIN: win[hi - lo])
+    constexpr bool WIN = FORM != kGatherForm;
     constexpr bool STREAM = FORM == kStreamForm;
-    using CI = ColIdx<true>;
-    const int wlo = P.win[2 * blockIdx.x], whi = P.win[2 * blockIdx.x + 1];
-    const int coff = wlo;   // global column = coff + stored index
+    using CI = ColIdx<WIN>;
+    const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
+    const int coff = wlo;   // global column = coff + stored index (wlo = 0 in the gather form)
     const int* arp;
     const CI* aci;
     const float* av;
@@ -966,12 +967,14 @@ __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
             auto dirp = [&](int c) {
                 return first ? ldv(r + c) : fmaf(beta, fmaf(-omega, ldv(vo + c), ldv(po + c)), ldv(r + c));
             };
-            fill_window(win, wlo, whi, dirp);
-            __syncthreads();
+            if constexpr (WIN) {
+                fill_window(win, wlo, whi, dirp);
+                __syncthreads();
+            }
             double acc[1] = {0.0};
             auto own = [&](int li, float s) {
                 const int i = r0 + li;
-                pn[i] = win[i - wlo];
+                pn[i] = WIN ? win[i - wlo] : dirp(i);
                 vn[i] = s;
                 acc[0] += (double)rh[i] * (double)s;
             };
@@ -979,7 +982,8 @@ __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
                 const int lj = li + kPNT;
                 const bool has1 = lj < R;
                 float s0, s1;
-                row_pair_f32<STREAM>(arp, aci, av, li, lj, has1, wg, s0, s1);
+                if constexpr (WIN) row_pair_f32<STREAM>(arp, aci, av, li, lj, has1, wg, s0, s1);
+                else row_pair_f32(arp, aci, av, li, lj, has1, dirp, s0, s1);
                 own(li, s0);
                 if (has1) own(lj, s1);
             }
@@ -1002,12 +1006,14 @@ __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
         const float af = (float)S.alpha;
         auto dirs = [&](int c) { return fmaf(-af, ldv(vn + c), ldv(r + c)); };
         {
-            fill_window(win, wlo, whi, dirs);
-            __syncthreads();
+            if constexpr (WIN) {
+                fill_window(win, wlo, whi, dirs);
+                __syncthreads();
+            }
             double acc[2] = {0.0, 0.0};
             auto own = [&](int li, float t) {
                 const int i = r0 + li;
-                const float sv = win[i - wlo];
+                const float sv = WIN ? win[i - wlo] : dirs(i);
                 ts[li] = t;
                 acc[0] += (double)t * (double)sv;
                 acc[1] += (double)t * (double)t;
@@ -1016,7 +1022,8 @@ __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
                 const int lj = li + kPNT;
                 const bool has1 = lj < R;
                 float s0, s1;
-                row_pair_f32<STREAM>(arp, aci, av, li, lj, has1, wg, s0, s1);
+                if constexpr (WIN) row_pair_f32<STREAM>(arp, aci, av, li, lj, has1, wg, s0, s1);
+                else row_pair_f32(arp, aci, av, li, lj, has1, dirs, s0, s1);
                 own(li, s0);
                 if (has1) own(lj, s1);
             }
@@ -1034,7 +1041,9 @@ __global__ void __launch_bounds__(kPNT, 1) bicg_persistent(PersistDev P) {
             double acc[2] = {0.0, 0.0};
             for (int li = tid; li < R; li += kPNT) {
                 const int i = r0 + li;
-                const float sv = win[i - wlo];
+                // s of the own row: from the window, or formed again from r
+                // and v (read before this thread overwrites r[i] below)
+                const float sv = WIN ? win[i - wlo] : dirs(i);
                 float xv = fmaf(af, ldv(pn + i), xs[li]);
                 xv = fmaf(w, sv, xv);
                 xs[li] = xv;
@@ -1192,9 +1201,11 @@ static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const C
     const int* win = start + grid + 1 + kBarWords;
     const int* cnt = win + 2 * grid;
     size_t worst = 0, worst_win = 0, worst_stream = 0;
+    int rows_max = 0;
     for (int c = 0; c < grid; ++c) {
         const int rows = start[c + 1] - start[c];
         if (rows < 0) return cudaSuccess;
+        rows_max = std::max(rows_max, rows);
         size_t b = 4 * (size_t)words * ((size_t)rows + 1) + 8 * (size_t)cnt[2 * c];
         if (M) b += 8 * (size_t)cnt[2 * c + 1];
         worst = std::max(worst, b);
@@ -1213,6 +1224,7 @@ static cudaError_t plan_rows(PersistPlan& pp, int n, const void* kernel, const C
         worst_stream = std::max(worst_stream, w > 65536 ? ~(size_t)0 : bs);
     }
     pp.grid = grid;
+    pp.rows_max = rows_max;
     // a footprint above the gather budget must still leave one CTA
     // resident per SM
     auto resident = [&](size_t need) {
@@ -1333,7 +1345,7 @@ cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s, const double* b64, doub
     return cudaLaunchCooperativeKernel(k, dim3(h->pp_a.grid), dim3(kPNT), args, h->pp_a.smem, s);
 }
 
-// BiCGSTAB as one cooperative launch (window or stream form): b is H.v(vB), x
+// BiCGSTAB as one cooperative launch (any form): b is H.v(vB), x
 // lands in H.v(vX) and the final scalars in H.ws.sc; the parameters must be
 // in H.ws.d_params.  cudaErrorNotSupported: not eligible (the graph form runs).
 cudaError_t persist_bicg_solve(mps_csr* h, cudaStream_t s) {
@@ -1341,7 +1353,23 @@ cudaError_t persist_bicg_solve(mps_csr* h, cudaStream_t s) {
         const cudaError_t e = persist_plan_build_a(h, s);
         if (e != cudaSuccess) return e;
     }
-    if (h->pp_a.state != 1 || h->pp_a.form == kGatherForm) return cudaErrorNotSupported;
+    if (h->pp_a.state != 1) return cudaErrorNotSupported;
+    const int f = h->pp_a.form;
+    size_t smem = h->pp_a.smem;
+    if (f == kGatherForm) {
+        // the gather form's footprint holds A's rows only: add the own rows'
+        // x and t (and 8 bytes of alignment); it must still fit one CTA per SM
+        smem = ((smem + 8 * (size_t)h->pp_a.rows_max + 8 + 15) / 16) * 16;
+        const void* kg = reinterpret_cast<const void*>(bicg_persistent<kGatherForm>);
+        int per = 0;
+        cudaError_t eg = smem <= kPSmemWinBudget ? cudaSuccess : cudaErrorInvalidValue;
+        if (eg == cudaSuccess) eg = cudaFuncSetAttribute(kg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (eg == cudaSuccess) eg = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kg, kPNT, smem);
+        if (eg != cudaSuccess || per < 1) {
+            cudaGetLastError();
+            return cudaErrorNotSupported;
+        }
+    }
     SolverHost& H = h->H;
     PersistDev P{};
     P.a_rp = h->A.rp;
@@ -1366,14 +1394,15 @@ cudaError_t persist_bicg_solve(mps_csr* h, cudaStream_t s) {
     P.b32 = H.v(vB);
     P.x32 = H.v(vX);
     P.a_c16 = h->pp_a.d_c16;
-    const void* k = h->pp_a.form == kStreamForm ? reinterpret_cast<const void*>(bicg_persistent<kStreamForm>)
-                                                : reinterpret_cast<const void*>(bicg_persistent<kWindowForm>);
+    const void* k = f == kStreamForm   ? reinterpret_cast<const void*>(bicg_persistent<kStreamForm>)
+                    : f == kWindowForm ? reinterpret_cast<const void*>(bicg_persistent<kWindowForm>)
+                                       : reinterpret_cast<const void*>(bicg_persistent<kGatherForm>);
     cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->pp_a.smem);
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     void* args[] = {&P};
-    return cudaLaunchCooperativeKernel(k, dim3(h->pp_a.grid), dim3(kPNT), args, h->pp_a.smem, s);
+    return cudaLaunchCooperativeKernel(k, dim3(h->pp_a.grid), dim3(kPNT), args, smem, s);
 }
 
 void persist_plan_free(mps_csr* h) {

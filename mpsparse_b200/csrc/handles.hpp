@@ -37,6 +37,7 @@ struct FsaiProduct {
 struct PersistPlan {
     int state = 0;                 // 0 not built, 1 eligible, -1 rows do not fit
     int grid = 0;
+    int rows_max = 0;              // most rows of one CTA
     size_t smem = 0;               // dynamic shared memory per CTA
     int form = 0;                  // 0 gather, 1 window (16-bit window-relative columns), 2 stream
     int* d_row_start = nullptr;    // grid + 1 row boundaries, the barrier's words, the windows

@@ -110,9 +110,8 @@ def test_persistent_forms_bit_identical(mps):
     """512^2 fits one CTA per SM in all three forms (window, gather,
     stream).  They share the row partition, each row's arithmetic and the
     order of every sum, so learned-FSAI MP-PCG, plain CG and BiCGSTAB return
-    bit-identical solutions and iteration counts in every form they run in;
-    BiCGSTAB has no gather form (the graph form runs), and an unknown form
-    is rejected."""
+    bit-identical solutions and iteration counts in every form; an unknown
+    form is rejected."""
     c, A = _learned(mps, 512, 512, 31)
     b = torch.from_numpy(W.rhs(c.n, 8).astype(np.float64)).cuda()
     forms = ("window", "gather", "stream")
@@ -128,7 +127,7 @@ def test_persistent_forms_bit_identical(mps):
         assert out[form][1:] == out["window"][1:], (form, out[form][1:], out["window"][1:])
     # plain CG needs ~19,000 iterations on this system: 500 of each solver
     b32 = b.float()
-    for solve, fs in (("cgd", forms), ("bicgstab", ("window", "stream"))):
+    for solve, fs in (("cgd", forms), ("bicgstab", forms)):
         xs = {}
         for form in fs:
             A.set_persistent(True, form=form)
@@ -138,10 +137,6 @@ def test_persistent_forms_bit_identical(mps):
             xs[form] = x
         for form in fs[1:]:
             assert torch.equal(xs[form], xs["window"]), (solve, form)
-    A.set_persistent(True, form="gather")
-    x = torch.zeros(c.n, device="cuda")
-    info = A.bicgstab(b32, x, tol=1e-300, max_iter=20)
-    assert not info["persistent"] and info["iters"] == 20
     with pytest.raises(ValueError):
         A.set_persistent(True, form="tiled")
     A.set_persistent(True)
@@ -158,7 +153,7 @@ def test_persistent_forms_bit_identical_edge_cases(mps, case):
     A = _cg_system(mps, c)
     b = torch.from_numpy(W.rhs(c.n, 2)).cuda()
     forms = ("window", "gather", "stream")
-    for solve, fs in (("cgd", forms), ("bicgstab", ("window", "stream"))):
+    for solve, fs in (("cgd", forms), ("bicgstab", forms)):
         xs = {}
         for form in fs:
             A.set_persistent(True, form=form)
@@ -368,6 +363,25 @@ def test_persistent_gather_form_on_random_graph(mps, oracle):
     x = torch.zeros(c.n, device="cuda")
     info = A.cgd(bt, x, tol=1e-6, max_iter=20000)
     assert info["persistent_form"] == "gather" and info["stop_rule_met"]
+    # BiCGSTAB in the gather form: the graph form's first iterates, and a
+    # converged solve; the window form does not fit here (graph form runs)
+    for k in (1, 5, 20):
+        xs = []
+        for persistent in (True, False):
+            A.set_persistent(persistent)
+            x = torch.zeros(c.n, device="cuda")
+            info = A.bicgstab(bt, x, tol=1e-300, max_iter=k)
+            assert info["iters"] == k and info["persistent_form"] == ("gather" if persistent else None)
+            xs.append(x)
+        assert float((xs[0] - xs[1]).norm() / xs[1].norm()) <= 1e-5, k
+    A.set_persistent(True)
+    x = torch.zeros(c.n, device="cuda")
+    info = A.bicgstab(bt, x, tol=1e-6, max_iter=20000)
+    assert info["persistent_form"] == "gather" and info["stop_rule_met"]
+    A.set_persistent(True, form="window")
+    info = A.bicgstab(bt, x, tol=1e-6, max_iter=20000)
+    assert not info["persistent"] and info["stop_rule_met"]
+    A.set_persistent(True)
     from mpsparse_b200.fsai import LearnedFsai
     LearnedFsai.load().attach(A)
     A.set_fsai_apply("product")
