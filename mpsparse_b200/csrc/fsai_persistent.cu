@@ -1,5 +1,6 @@
 // fsai_persistent.cu -- whole solves as one cooperative kernel, for matrices
-// whose rows fit the shared memory of one CTA per SM: reliable-update
+// whose share of one CTA per SM (its rows, their vector window, or both)
+// fits that CTA's shared memory: reliable-update
 // FSAI-PCG (product form: z = M r with M = G^T G; fsai_pcg_persistent),
 // plain CG / Jacobi-PCG, FP32 or with reliable updates (cg_persistent), and
 // BiCGSTAB (bicg_persistent).
@@ -8,9 +9,9 @@
 // grid-wide kernels per iteration; on an L2-resident system (512^2: 1.3 M
 // nonzeros in A, 1.8 M in M) each kernel is bound by its fixed latency --
 // launch, tile copies, the last-CTA reduction -- not by bytes.  Here one CTA
-// per SM keeps its block of rows of A and of M in shared memory for the whole
-// solve and the two dependent steps of an iteration are separated by grid
-// barriers instead of kernel boundaries:
+// per SM owns a block of rows of A and of M for the whole solve (held in its
+// shared memory, except in the stream form) and the two dependent steps of
+// an iteration are separated by grid barriers instead of kernel boundaries:
 //   step 1  p = z + beta p_old, q = A p, p.q                          -> alpha
 //   step 2  x += alpha p (FP64), r' = r - alpha q, z = M r',
 //           r'.r', r'.D^-1 r', r'.z                                  -> beta
@@ -21,11 +22,12 @@
 // (windows too large) the row sums gather the vector entries and form them
 // per nonzero; in the stream form (rows too large for shared memory, the
 // window not) the vector is staged as in the window form and the rows are
-// read from global memory (L2) in every step.  The arithmetic of every row is the graph form's (same products,
-// same order of additions, same FP32 / FP64 rounding points); only the FP64
-// sums of the per-CTA partials group differently.  Every CTA sums all
-// partials itself in one fixed order, so all CTAs take the same decisions
-// from the same bits and reach the same barriers.
+// read from global memory (L2) in every step. The arithmetic of every row is
+// the graph form's (same products, same order of additions, same FP32 / FP64
+// rounding points); only the FP64 sums of the per-CTA partials group
+// differently. Every CTA sums all partials itself in one fixed order, so all
+// CTAs take the same decisions from the same bits and reach the same
+// barriers.
 //
 // The host picks the window form when its footprint fits, else the gather
 // form, else the stream form (plan_rows).
