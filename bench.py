@@ -983,7 +983,8 @@ def persistent_forms_leg(dev):
     700^2 and up, whose rows of A and GᵀG no longer fit shared memory, in the
     stream form (rows read from L2 in every step); plain CG and BiCGSTAB on a
     random graph Laplacian (60,000 rows, mean degree 6, + 0.05 I) in the
-    gather form."""
+    gather form; Richardson (2,000 iterations) on that graph and on the
+    1024^2 Laplacian."""
     import torch
     import mpsparse_b200 as mps
     from mpsparse_b200.fsai import LearnedFsai
@@ -1056,6 +1057,16 @@ def persistent_forms_leg(dev):
     for solve in ("cgd", "bicgstab"):
         out.append({"solve": solve, "grid": "random graph, 60,000 rows, mean degree 6",
                     **both(A, lambda x: getattr(A, solve)(b, x, tol=1e-6, max_iter=40000), x)})
+    # Richardson, 2,000 iterations at omega 0.02 (below 2 / lambda_max)
+    out.append({"solve": "richardson", "grid": "random graph, 60,000 rows, mean degree 6",
+                **both(A, lambda x: A.richardson(b, x, omega=0.02, iters=2000), x)})
+    c = W.laplacian_2d(1024)
+    x = torch.zeros(c.n, device=dev)
+    b = torch.from_numpy(W.rhs(c.n, 1)).to(dev)
+    A = mps.spmv.csr_tensor(torch.from_numpy(c.keys()), torch.from_numpy(c.vals), e, e, e,
+                            c.n, c.n, fill_outputs=False)
+    out.append({"solve": "richardson", "grid": 1024,
+                **both(A, lambda x: A.richardson(b, x, omega=0.2, iters=2000), x)})
     return out
 
 

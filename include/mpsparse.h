@@ -229,8 +229,9 @@ typedef struct {
 } mps_ir_info;
 
 /* Reliable-update FSAI-PCG in product form (M = G^T G), plain CG /
- * Jacobi-PCG and BiCGSTAB (mps_csr_cg / mps_csr_bicgstab without
- * reference_compat or host_loop), run as ONE cooperative kernel -- one CTA
+ * Jacobi-PCG, BiCGSTAB and Richardson (mps_csr_cg / mps_csr_bicgstab /
+ * mps_csr_richardson without reference_compat or host_loop), run as ONE
+ * cooperative kernel -- one CTA
  * per SM, grid barriers between the steps of an iteration -- whenever the
  * CTA's share fits its shared memory (about 220 KB): its rows of A (and M)
  * with the vector window they reach (window form), its rows alone (gather

@@ -486,7 +486,7 @@ static mps_status solve_errors(mps_csr* h, const unsigned* e2, mps_status st, cu
     return MPS_OK;
 }
 
-// Plain CG / Jacobi-PCG, or BiCGSTAB, as one persistent cooperative kernel
+// Plain CG / Jacobi-PCG, BiCGSTAB or Richardson as one persistent cooperative kernel
 // when A's rows (or, in the stream form, their vector windows) fit one CTA
 // per SM (fsai_persistent.cu); *ran = false: not eligible, the graph form
 // runs instead.  Same parameters,
@@ -506,11 +506,24 @@ static mps_status csr_persistent(SolverKind kind, mps_csr* h, const float* b, fl
     P.stall_window = o.stall_window > 0 ? o.stall_window : 400;
     MPS_CUDA(cudaMemcpyAsync(H.ws.d_params, H.h_params, sizeof(SolveParams), cudaMemcpyHostToDevice, s));
     MPS_CUDA(cudaMemcpyAsync(H.v(vB), b, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
-    const cudaError_t pe = kind == kCG ? persist_cg_solve(h, s) : persist_bicg_solve(h, s);
+    const cudaError_t pe = kind == kCG     ? persist_cg_solve(h, s)
+                           : kind == kBiCG ? persist_bicg_solve(h, s)
+                                           : persist_rich_solve(h, s);
     if (pe == cudaErrorNotSupported) return MPS_OK;
-    if (pe != cudaSuccess) return cuda_fail(pe, kind == kCG ? "persistent CG" : "persistent BiCGSTAB");
+    if (pe != cudaSuccess)
+        return cuda_fail(pe, kind == kCG     ? "persistent CG"
+                             : kind == kBiCG ? "persistent BiCGSTAB"
+                                             : "persistent Richardson");
     *ran = true;
-    MPS_CUDA(cudaMemcpyAsync(x, H.v(vX), n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    if (kind == kRich) {   // x in vX or vXAlt by the final iteration's parity
+        const int nb = ((int)n + 255) / 256;
+        launch_k(copy_result, dim3(nb < 1184 ? (nb ? nb : 1) : 1184), dim3(256), 0, s, H.v(vX),
+                 static_cast<const float*>(H.v(vXAlt)), H.v(vXAlt), x, (int)n, (int)kResRich,
+                 static_cast<const DevScalars*>(H.ws.sc));
+        MPS_CUDA(cudaGetLastError());
+    } else {
+        MPS_CUDA(cudaMemcpyAsync(x, H.v(vX), n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    }
     const CsrOp op{&h->A, nullptr};
     MPS_CUDA(op.true_resid(x, H.v(vB), &H.ws.sc->true_rr, H.ws.counters + 11, H.ws.partials, s));
     MPS_CUDA(cudaMemcpyAsync(H.ws.h_sc, H.ws.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
@@ -537,7 +550,7 @@ static mps_status csr_solve(SolverKind kind, mps_csr* h, const float* b, float* 
     bool ran = false;
     if (h->persistent && !oo.reference_compat && !oo.host_loop &&
         ((kind == kCG && (oo.precond == MPS_PRECOND_NONE || oo.precond == MPS_PRECOND_JACOBI)) ||
-         kind == kBiCG))
+         kind == kBiCG || kind == kRich))
         st = csr_persistent(kind, h, b, x, oo, info, s, &ran);
     if (st != MPS_OK) return st;
     if (!ran) st = run_solve(kind, op, pc, h->H, b, x, o, info, s);

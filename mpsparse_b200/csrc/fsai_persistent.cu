@@ -1073,6 +1073,119 @@ out:
     }
 }
 
+// Richardson (the drop-in richardson, outside reference_compat) as one
+// cooperative kernel: per iteration the CTA stages x_in over its window (or
+// gathers it, gather form), forms its rows' x_out = x_in + (w b + (-w) A x_in)
+// with the graph form's arithmetic (rich_update) into the other x buffer,
+// and sums ||b - A x_in||^2 for the stop rule (rich_finalize): one grid sum
+// per iteration.  x is double-buffered by iteration parity (P.x32 even,
+// P.q odd, the graph form's vX / vXAlt), so a CTA writes its rows of x_out
+// while slower CTAs still read x_in; the grid sums alternate between slots
+// 0 and 1.  x itself does not depend on any sum, so for a given iteration
+// count every form returns the graph form's bits.
+template <int FORM>
+__global__ void __launch_bounds__(kPNT, 1) rich_persistent(PersistDev P) {
+    constexpr bool WIN = FORM != kGatherForm;
+    constexpr bool STREAM = FORM == kStreamForm;
+    extern __shared__ __align__(16) unsigned char psmem[];
+    __shared__ PersistShared sh;
+    const int tid = threadIdx.x;
+    const int r0 = P.row_start[blockIdx.x], r1 = P.row_start[blockIdx.x + 1];
+    const int R = r1 - r0;
+    const int a0 = P.a_rp[r0], na = P.a_rp[r1] - a0;
+    // shared layout: arp[R+1] | [aci[na] | pad | av[na]] | pad to 8 (the
+    // bracket not in the stream form) | (WIN: win[hi - lo]); columns 16-bit,
+    // window-relative in the window and stream forms
+    using CI = ColIdx<WIN>;
+    const int wlo = WIN ? P.win[2 * blockIdx.x] : 0, whi = WIN ? P.win[2 * blockIdx.x + 1] : 0;
+    const int coff = wlo;   // global column = coff + stored index (wlo = 0 in the gather form)
+    const int* arp;
+    const CI* aci;
+    const float* av;
+    size_t off_own = 0;
+    if constexpr (STREAM) {
+        int* arp_s = reinterpret_cast<int*>(psmem);
+        for (int i = tid; i <= R; i += kPNT) arp_s[i] = P.a_rp[r0 + i];
+        off_own = round_up(4 * (size_t)(R + 1), 8);
+        arp = arp_s;
+        aci = P.a_c16;
+        av = P.a_v;
+    } else {
+        int* arp_s = reinterpret_cast<int*>(psmem);
+        CI* aci_s = reinterpret_cast<CI*>(arp_s + (R + 1));
+        const size_t off_v = round_up(4 * (size_t)(R + 1) + sizeof(CI) * (size_t)na, 4);
+        float* av_s = reinterpret_cast<float*>(psmem + off_v);
+        off_own = round_up(off_v + 4 * (size_t)na, 8);
+        for (int i = tid; i <= R; i += kPNT) arp_s[i] = P.a_rp[r0 + i] - a0;
+        for (int k = tid; k < na; k += kPNT) {
+            aci_s[k] = (CI)(P.a_ci[a0 + k] - coff);
+            av_s[k] = P.a_v[a0 + k];
+        }
+        arp = arp_s;
+        aci = aci_s;
+        av = av_s;
+    }
+    float* win = reinterpret_cast<float*>(psmem + off_own);
+    auto wg = [&](int c) { return win[c]; };
+    if (tid == 0) {
+        sh.gen = 0;
+        sh.ok = 1;
+        sh.S = DevScalars{};
+    }
+    __syncthreads();
+    DevScalars& S = sh.S;
+    {
+        // x = 0; ||b||^2 (rich_init)
+        double acc[1] = {0.0};
+        for (int li = tid; li < R; li += kPNT) {
+            const int i = r0 + li;
+            const float bv = P.b32[i];
+            P.x32[i] = 0.f;
+            acc[0] += (double)bv * bv;
+        }
+        double tot[1];
+        if (!reduce_all<1>(P, sh, 3, acc, tot, [&](const double* t) { rich_init_scalars(&S, P.prm, P.n, t[0]); }))
+            goto out;
+    }
+    while (!S.done) {
+        const bool odd = S.iter & 1;
+        const float* xin = odd ? P.q : P.x32;
+        float* xout = odd ? P.x32 : P.q;
+        const float w = (float)S.omega_rich;
+        auto xg = [&](int c) { return ldv(xin + c); };
+        if constexpr (WIN) {
+            fill_window(win, wlo, whi, xg);
+            __syncthreads();
+        }
+        double acc[1] = {0.0};
+        auto own = [&](int li, float ax) {
+            const int i = r0 + li;
+            const float bv = P.b32[i];
+            const float xv = WIN ? win[i - wlo] : xg(i);
+            xout[i] = rich_update(xv, w, bv, ax);
+            const double res = (double)bv - (double)ax;
+            acc[0] += res * res;
+        };
+        for (int li = tid; li < R; li += 2 * kPNT) {
+            const int lj = li + kPNT;
+            const bool has1 = lj < R;
+            float s0, s1;
+            if constexpr (WIN) row_pair_f32<STREAM>(arp, aci, av, li, lj, has1, wg, s0, s1);
+            else row_pair_f32(arp, aci, av, li, lj, has1, xg, s0, s1);
+            own(li, s0);
+            if (has1) own(lj, s1);
+        }
+        double tot[1];
+        if (!reduce_all<1>(P, sh, odd ? 1 : 0, acc, tot, [&](const double* t) { rich_finalize(&S, t[0]); }))
+            goto out;
+    }
+out:
+    if (tid == 0 && blockIdx.x == 0) {
+        if (!sh.ok) S.err |= kErrTimeout;
+        *P.sc_out = S;
+    }
+}
+
 // Row blocks for `grid` CTAs balanced by their shared-memory bytes
 // (4 * words per row + 8 per nonzero of A, and of M when given): boundary c
 // is the first row whose prefix reaches c / grid of the total.  Each
@@ -1405,6 +1518,48 @@ cudaError_t persist_bicg_solve(mps_csr* h, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     void* args[] = {&P};
     return cudaLaunchCooperativeKernel(k, dim3(h->pp_a.grid), dim3(kPNT), args, smem, s);
+}
+
+// Richardson as one cooperative launch (any form; the CG plan, whose
+// own-row budget covers it): b is H.v(vB); x ends in H.v(vX) or H.v(vXAlt)
+// by the parity of the final iteration count (as in the graph form:
+// copy_result selects it); the final scalars in H.ws.sc, the parameters in
+// H.ws.d_params.  cudaErrorNotSupported: not eligible (the graph form runs).
+cudaError_t persist_rich_solve(mps_csr* h, cudaStream_t s) {
+    if (h->pp_a.state == 0) {
+        const cudaError_t e = persist_plan_build_a(h, s);
+        if (e != cudaSuccess) return e;
+    }
+    if (h->pp_a.state != 1) return cudaErrorNotSupported;
+    SolverHost& H = h->H;
+    PersistDev P{};
+    P.a_rp = h->A.rp;
+    P.a_ci = h->A.ci;
+    P.a_v = h->A.v;
+    P.row_start = h->pp_a.d_row_start;
+    P.win = h->pp_a.d_row_start + h->pp_a.grid + 1 + kBarWords;
+    P.a_c16 = h->pp_a.d_c16;
+    P.q = H.v(vXAlt);
+    P.part = H.ws.partials;
+    P.bar = reinterpret_cast<unsigned*>(h->pp_a.d_row_start + h->pp_a.grid + 1);
+    P.err = h->d_err;
+    P.sc_out = H.ws.sc;
+    P.prm = H.ws.d_params;
+    P.n = (int)h->A.n_rows;
+    P.spin_limit = h->test_spin_limit ? h->test_spin_limit : kGridSpinLimit;
+    P.silent_cta = h->test_silent_cta;
+    P.b32 = H.v(vB);
+    P.x32 = H.v(vX);
+    const int f = h->pp_a.form;
+    const void* k = f == kStreamForm   ? reinterpret_cast<const void*>(rich_persistent<kStreamForm>)
+                    : f == kWindowForm ? reinterpret_cast<const void*>(rich_persistent<kWindowForm>)
+                                       : reinterpret_cast<const void*>(rich_persistent<kGatherForm>);
+    cudaError_t e = cudaMemsetAsync(P.bar, 0, kBarWords * sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->pp_a.smem);
+    if (e != cudaSuccess) return e;
+    void* args[] = {&P};
+    return cudaLaunchCooperativeKernel(k, dim3(h->pp_a.grid), dim3(kPNT), args, h->pp_a.smem, s);
 }
 
 void persist_plan_free(mps_csr* h) {

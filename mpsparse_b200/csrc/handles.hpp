@@ -93,4 +93,5 @@ cudaError_t persist_solve(mps_csr* h, const double* b64, double* x64, cudaStream
 cudaError_t persist_cg_solve(mps_csr* h, cudaStream_t s, const double* b64 = nullptr,
                              double* x64 = nullptr);
 cudaError_t persist_bicg_solve(mps_csr* h, cudaStream_t s);
+cudaError_t persist_rich_solve(mps_csr* h, cudaStream_t s);
 }  // namespace mps

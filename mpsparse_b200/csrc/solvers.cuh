@@ -988,6 +988,28 @@ bicg_update_xr(float4* __restrict__ x, float4* __restrict__ r, const float4* __r
 
 // ============================ Richardson ===================================
 
+// The solver scalars at the start (x = 0, ||b||^2 = bb); shared by the graph
+// form (rich_init) and the persistent form.
+__device__ __forceinline__ void rich_init_scalars(DevScalars* s, const SolveParams* prm, int n, double bb);
+
+// One row of x_out = x_in + (w b + (-w) A x_in): iterative_step's spmv_op and
+// two weighted_adds (richardson/spmv.cpp:376-495), each product and sum
+// rounded to FP32 on its own (no contraction), in both forms.
+__device__ __forceinline__ float rich_update(float xin, float w, float bv, float ax) {
+    return __fadd_rn(xin, __fadd_rn(__fmul_rn(w, bv), __fmul_rn(-w, ax)));
+}
+
+// Iteration count and stop rule after ||b - A x_in||^2 = rr.
+__device__ __forceinline__ void rich_finalize(DevScalars* sc, double rr) {
+    const int it = ++sc->iter;
+    sc->rnorm2 = rr;
+    if (sc->tol2 > 0.0 && rr <= sc->tol2) {
+        sc->converged = 1;
+        sc->done = 1;
+    }
+    if (it >= sc->max_iter) sc->done = 1;
+}
+
 static __global__ void __launch_bounds__(kNT)
 rich_init(const float4* __restrict__ b, float4* __restrict__ x0, int n4, int n,
           const SolveParams* __restrict__ prm, Ctx c) {
@@ -1001,7 +1023,11 @@ rich_init(const float4* __restrict__ b, float4* __restrict__ x0, int n4, int n,
     double tot[1];
     if (!reduce_partials<1>(c, 8, acc, tot)) return;
     if (threadIdx.x != 0) return;
-    DevScalars* s = c.sc;
+    rich_init_scalars(c.sc, prm, n, tot[0]);
+    set_cond(c, !c.sc->done);
+}
+
+__device__ __forceinline__ void rich_init_scalars(DevScalars* s, const SolveParams* prm, int n, double bb) {
     s->n = n;
     s->compat = prm->compat;
     s->max_iter = prm->compat ? 1000 : prm->max_iter;        // richardson/spmv.cpp:402
@@ -1012,18 +1038,17 @@ rich_init(const float4* __restrict__ b, float4* __restrict__ x0, int n4, int n,
     s->breakdown = 0;
     s->snapshot = 0;
     s->err = 0;
-    s->bnorm2 = tot[0];
-    s->rnorm2 = tot[0];
-    s->tol2 = prm->compat ? 0.0 : prm->tol * prm->tol * tot[0];
+    s->bnorm2 = bb;
+    s->rnorm2 = bb;
+    s->tol2 = prm->compat ? 0.0 : prm->tol * prm->tol * bb;
     s->guard = 0;
     s->guard_limit = s->max_iter / 2 + 8;
-    if (!isfinite(tot[0])) {
+    if (!isfinite(bb)) {
         s->err = kErrNotFinite;
         s->done = 1;
     } else if (s->max_iter <= 0) {
         s->done = 1;
     }
-    set_cond(c, !s->done);
 }
 
 // x_out = x_in + (w b + (-w) A x_in)  (iterative_step's spmv_op + two
@@ -1048,19 +1073,12 @@ struct EpiRich {
     __device__ void row(int r, float s, double* acc) const {
         const float w = (float)__ldcg(&sc->omega_rich);
         const float bv = b[r];
-        const float s2 = w * bv + (-w) * s;
-        xout[r] = xin[r] + s2;
+        xout[r] = rich_update(xin[r], w, bv, s);
         const double res = (double)bv - (double)s;
         acc[0] += res * res;
     }
     __device__ void finalize(const double* tot) const {
-        const int it = ++sc->iter;
-        sc->rnorm2 = tot[0];
-        if (sc->tol2 > 0.0 && tot[0] <= sc->tol2) {
-            sc->converged = 1;
-            sc->done = 1;
-        }
-        if (it >= sc->max_iter) sc->done = 1;
+        rich_finalize(sc, tot[0]);
         if (last_in_body) set_cond(ctx, !sc->done);
     }
 };

@@ -163,6 +163,16 @@ def test_persistent_forms_bit_identical_edge_cases(mps, case):
             xs[form] = (x, info["iters"])
         for form in fs[1:]:
             assert torch.equal(xs[form][0], xs["window"][0]) and xs[form][1] == xs["window"][1], (solve, form)
+    omega = 0.2 if case == "one_cta" else 0.05   # below 2 / lambda_max of each system
+    xs = {}
+    for form in forms:
+        A.set_persistent(True, form=form)
+        x = torch.zeros(c.n, device="cuda")
+        info = A.richardson(b, x, omega=omega, iters=31)
+        assert info["persistent_form"] == form and info["iters"] == 31, (form, info)
+        xs[form] = x
+    for form in forms[1:]:
+        assert torch.equal(xs[form], xs["window"]), ("richardson", form)
     from mpsparse_b200.fsai import LearnedFsai
     LearnedFsai.load().attach(A)
     A.set_fsai_apply("product")
@@ -564,3 +574,48 @@ def test_persistent_barrier_timeout_returns_error_and_handle_stays_usable(mps, o
         assert np.linalg.norm(x.cpu().numpy() - xo) / np.linalg.norm(xo) <= 1e-5
     finally:
         L.mps_csr_destroy(h)
+
+
+def test_persistent_richardson_matches_graph_form_and_oracle(mps, oracle):
+    """Richardson (the drop-in richardson, outside reference_compat) as one
+    persistent kernel: x depends on no sum, so for a fixed iteration count
+    (odd and even: the result buffer alternates) it is bit-identical to the
+    graph form's, and within 1e-5 of the FP64 oracle's; with a tolerance
+    both forms stop within one iteration of each other (the stop test's sum
+    groups differently).  On a random graph the gather form runs."""
+    c = W.laplacian_2d(128)
+    A = _cg_system(mps, c)
+    Ao = oracle.Csr(*c.to_csr(), c.n)
+    b = W.rhs(c.n, 4)
+    bt = torch.from_numpy(b).cuda()
+    for iters in (1, 2, 301):
+        xs = []
+        for persistent in (True, False):
+            A.set_persistent(persistent)
+            x = torch.zeros(c.n, device="cuda")
+            info = A.richardson(bt, x, omega=0.2, iters=iters)
+            assert info["iters"] == iters
+            assert info["persistent_form"] == ("window" if persistent else None), info
+            xs.append(x)
+        assert torch.equal(xs[0], xs[1]), iters
+        xo, _ = oracle.richardson(Ao, b, compat=False, omega=0.2, iters=iters)
+        assert np.linalg.norm(xs[0].cpu().numpy() - xo) / np.linalg.norm(xo) <= 1e-5, iters
+    its = []
+    for persistent in (True, False):
+        A.set_persistent(persistent)
+        x = torch.zeros(c.n, device="cuda")
+        info = A.richardson(bt, x, omega=0.2, iters=20000, tol=0.3)
+        assert info["converged"] and info["persistent"] == persistent, info
+        its.append(info["iters"])
+    assert abs(its[0] - its[1]) <= 1, its
+    g = W.graph_laplacian(60000, 6.0, 3, shift=0.05)
+    G = _cg_system(mps, g)
+    bg = torch.from_numpy(W.rhs(g.n, 7)).cuda()
+    xs = []
+    for persistent in (True, False):
+        G.set_persistent(persistent)
+        x = torch.zeros(g.n, device="cuda")
+        info = G.richardson(bg, x, omega=0.02, iters=50)
+        assert info["persistent_form"] == ("gather" if persistent else None), info
+        xs.append(x)
+    assert torch.equal(xs[0], xs[1])
