@@ -236,10 +236,11 @@ typedef struct {
  * CTA's share fits its shared memory (about 220 KB): its rows of A (and M)
  * with the vector window they reach (window form), its rows alone (gather
  * form), or -- rows read from L2 in every step -- the window alone (stream
- * form; 2D 5-point systems up to about a million rows).  Otherwise, or with enable = 0, as the CUDA graph of two or
- * three kernels per iteration.  Default 1.  The forms compute the same
- * iterates up to the grouping of the FP64 partial sums.  No reference
- * counterpart. */
+ * form; 2D 5-point systems up to about a million rows).  Otherwise, or
+ * with enable = 0, as the CUDA graph of two or three kernels per
+ * iteration.  Default 1.  The two compute the same iterates up to the
+ * grouping of the FP64 partial sums (Richardson's x: the same bits).  No
+ * reference counterpart. */
 mps_status mps_csr_set_persistent(mps_csr* A, int32_t enable);
 
 /* Which persistent form the solves above may use: 0 (default) the first
